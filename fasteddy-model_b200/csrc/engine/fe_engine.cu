@@ -1,0 +1,820 @@
+// fe_engine.cu -- host side of the B200 engine: domains, device memory, stage sequencing,
+// CUDA-graph replay of RK3 steps, ensembles and the autotuner. C ABI in fasteddy_b200.h.
+//
+// Memory plan of one domain (all fields halo-inclusive, reference layout):
+//   state A, B, C      nf fields each: A = phi^n (and phi^{n+1}), B = phi*, C = phi**
+//   pres pA, pB, pC    perturbation pressure of A, B, C
+//   grid               zPos, J31, J32, J33, D_Jac, invD_Jac
+//   base               rho_BS, (rho theta)_BS, powf((rho theta)_BS c1, cp/cv)
+//   scratch            9 stresses, 3 TKE fluxes, length scale, 3 per moisture species
+//   surface (2-D)      cd, ch, cq, u*, w'th', T_skin, 1/L, z0m, z0t, w'q', q_skin
+//   clock              simTime_it, simTime of the step in flight
+// A stage reads its input state at the stencil neighbours and the step-start state A at
+// its own cell only, so stage 3 can write phi^{n+1} into A in place. The commit of every
+// stage writes the next state's halo cells, so the next stage needs no halo pass.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fasteddy_b200.h"
+#include "fe_kernels.cuh"
+
+using fe::Phys;
+using fe::Ptrs;
+
+namespace {
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e__ = (call);                                                                      \
+    if (e__ != cudaSuccess)                                                                        \
+      return set_err(FE_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__));           \
+  } while (0)
+}  // namespace
+
+struct fe_domain {
+  fe_config cfg;
+  Phys P;
+  Ptrs Q;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  float* st[3] = {nullptr, nullptr, nullptr};
+  float* pr[3] = {nullptr, nullptr, nullptr};
+  float* grid = nullptr;
+  float* base = nullptr;
+  float* scratch = nullptr;
+  float* surf = nullptr;
+  float* frhs = nullptr;
+  void* clock = nullptr;
+  float simTime = 0.0f;
+  int simIt = 0;
+  bool haveGrid = false, haveBase = false, haveState = false;
+  int tk = 32, tj = 4, ti = 2;
+  cudaGraphExec_t graph = nullptr;
+  int graphSteps = 0;
+  long long launches = 0;
+  size_t bytes = 0;
+};
+
+struct fe_ensemble {
+  std::vector<fe_domain*> m;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graphSteps = 0;
+};
+
+extern "C" const char* fe_last_error(void) { return g_err.c_str(); }
+
+extern "C" int fe_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+extern "C" void fe_config_defaults(fe_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->Nh = 3;
+  c->hydroBCs = 2;
+  c->pgfSelector = 1;
+  c->buoyancySelector = 1;
+  c->coriolisSelector = 0;
+  c->c_s = 0.18f;
+  c->c_k = 0.10f;
+  c->advectionSelector = 3;
+  c->b_hyb = 0.0f;
+  c->surflayer_z0 = 0.1f;
+  c->surflayer_z0t = 0.1f;
+  c->moistureCond = 1;
+  c->moistureCondTscale = 1.0f;
+  c->moistureMPcallTscale = 1.0f;
+  c->dampingLayerDepth = 100.0f;
+  c->z_Ug = 10000.0f;
+  c->z_Vg = 10000.0f;
+  c->physics_oneRKonly = 1;
+  c->temp_grnd = 300.0f;
+  c->pres_grnd = 1.0e5f;
+  c->dt = 1.0f;
+  c->dX = c->dY = c->dZ = 1.0f;
+  c->surflayer_ideal_amp = 0.1f;
+  c->surflayer_ideal_qamp = 0.1f;
+  fe_config_derive(c, 54.0f);
+}
+
+extern "C" void fe_config_derive(fe_config* c, float lat) {
+  c->kappa = 0.4f;
+  c->accel_g = 9.81f;
+  c->R_gas = 287.04f;
+  c->R_vapor = 461.60f;
+  c->cv_gas = 718.0f;
+  c->cp_gas = c->R_gas + c->cv_gas;
+  c->L_v = 2.5e6f;
+  c->R_cp = c->R_gas / c->cp_gas;
+  c->cp_R = c->cp_gas / c->R_gas;
+  c->cp_cv = c->cp_gas / c->cv_gas;
+  c->refPressure = 1.0e5f;
+  c->Rv_Rg = c->R_vapor / c->R_gas;
+  const double pi = std::acos(-1.0);
+  if (c->coriolisSelector > 0) {
+    c->corioConstHorz = (float)(1.45842e-4 * std::sin(pi / 180.0 * lat));
+    c->corioConstVert = c->coriolisSelector > 1 ? (float)(1.45842e-4 * std::cos(pi / 180.0 * lat)) : 0.0f;
+    c->corioLS_fact = 1.0f;
+  } else {
+    c->corioConstHorz = c->corioConstVert = 0.0f;
+  }
+}
+
+static int check_config(const fe_config* c) {
+  if (c->Nh != 3) return set_err(FE_ERR_CONFIG, "Nh must be 3");
+  if (c->Nx < 3 || c->Ny < 3 || c->Nz < 2) return set_err(FE_ERR_CONFIG, "need Nx,Ny >= 3 and Nz >= 2");
+  if (c->hydroBCs != 2) return set_err(FE_ERR_CONFIG, "only hydroBCs = 2 (periodic horizontal, ABL vertical)");
+  if (c->advectionSelector != 3 && c->advectionSelector != 5)
+    return set_err(FE_ERR_CONFIG, "advectionSelector must be 3 (HYB56) or 5 (WENO5)");
+  if (c->turbulenceSelector > 0 && c->TKESelector > 0 && c->TKEAdvSelector != 3 && c->TKEAdvSelector != 5)
+    return set_err(FE_ERR_CONFIG, "TKEAdvSelector must be 3 or 5");
+  if (c->diffusionSelector != 0 || c->filterSelector != 0 || c->lsfSelector != 0)
+    return set_err(FE_ERR_CONFIG, "diffusion, explicit filter and large-scale forcing are not on this path");
+  if (c->moistureSelector > 0) {
+    if (c->moistureNvars < 1 || c->moistureNvars > 2) return set_err(FE_ERR_CONFIG, "moistureNvars must be 1 or 2");
+    if (c->moistureAdvSelectorQv != 3 && c->moistureAdvSelectorQv != 5)
+      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQv must be 3 or 5");
+    if (c->moistureNvars > 1 && c->moistureAdvSelectorQi != 2)
+      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQi must be 2 (WENO5)");
+  }
+  if (c->surflayerSelector < 0 || c->surflayerSelector > 2) return set_err(FE_ERR_CONFIG, "surflayerSelector 0..2");
+  if (c->TKESelector > 1) return set_err(FE_ERR_CONFIG, "TKESelector must be 0 or 1");
+  if (!(c->dt > 0.0f)) return set_err(FE_ERR_CONFIG, "dt must be positive");
+  const long long n = (long long)(c->Nx + 6) * (c->Ny + 6) * (c->Nz + 6);
+  if (n >= (1LL << 31)) return set_err(FE_ERR_CONFIG, "a single field exceeds 2^31 cells");
+  return FE_OK;
+}
+
+static void make_phys(fe_domain* d) {
+  const fe_config& c = d->cfg;
+  Phys& P = d->P;
+  std::memset(&P, 0, sizeof(P));
+  P.Nx = c.Nx; P.Ny = c.Ny; P.Nz = c.Nz;
+  P.nxh = c.Nx + 6; P.nyh = c.Ny + 6; P.nzh = c.Nz + 6;
+  P.sj = P.nzh;
+  P.si = P.nyh * P.nzh;
+  P.n = (long long)P.nxh * P.nyh * P.nzh;
+  P.n2 = (long long)P.nxh * P.nyh;
+  P.iMin = 3; P.iMax = c.Nx + 3; P.jMin = 3; P.jMax = c.Ny + 3; P.kMin = 3; P.kMax = c.Nz + 3;
+  P.dX = c.dX; P.dY = c.dY; P.dZ = c.dZ;
+  P.dXi = 1.0f / c.dX; P.dYi = 1.0f / c.dY; P.dZi = 1.0f / c.dZ;
+  P.dt = c.dt;
+  P.itRestart = c.simTime_itRestart;
+  P.turb = c.turbulenceSelector > 0;
+  P.tke = P.turb && c.TKESelector > 0;
+  P.ntke = P.tke ? 1 : 0;
+  P.moist = c.moistureSelector > 0;
+  P.nmoist = P.moist ? c.moistureNvars : 0;
+  P.nf = 5 + P.ntke + P.nmoist;
+  P.pgf = c.pgfSelector > 0;
+  P.buoy = c.buoyancySelector > 0;
+  P.cor = c.coriolisSelector > 0;
+  P.advSel = c.advectionSelector;
+  P.tkeAdvSel = c.TKEAdvSelector;
+  P.qvAdvSel = c.moistureAdvSelectorQv;
+  P.qiAdvSel = c.moistureAdvSelectorQi;
+  P.bHyb = c.b_hyb; P.tkeBHyb = c.TKEAdvSelector_b_hyb; P.qvB = c.moistureAdvSelectorQv_b;
+  P.c_s = c.c_s; P.c_k = c.c_k;
+  P.surf = c.surflayerSelector;
+  P.surfStab = c.surflayer_stab;
+  P.idealSine = c.surflayer_idealsine;
+  P.qskinInput = c.surflayer_qskin_input;
+  P.z0 = c.surflayer_z0; P.z0t = c.surflayer_z0t; P.wth = c.surflayer_wth; P.tr = c.surflayer_tr;
+  P.wq = c.surflayer_wq; P.qr = c.surflayer_qr;
+  P.idealTs = c.surflayer_ideal_ts; P.idealTe = c.surflayer_ideal_te; P.idealAmp = c.surflayer_ideal_amp;
+  P.idealQts = c.surflayer_ideal_qts; P.idealQte = c.surflayer_ideal_qte; P.idealQamp = c.surflayer_ideal_qamp;
+  P.moistSGS = c.moistureSGSturb;
+  P.moistCond = c.moistureCond;
+  P.condBasePres = c.moistureCondBasePres;
+  P.condTscale = c.moistureCondTscale;
+  // cadences as the reference computes them (cuda_hydroCoreDevice.cu:382, cuda_surfaceLayerDevice.cu:128)
+  P.mpFreq = std::max(1, (int)roundf(fmaxf(c.moistureMPcallTscale, c.dt) / c.dt));
+  P.tempFreq = std::max(1, (int)roundf((float)(10.0 / c.dt)));
+  P.damp = c.dampingLayerSelector > 0;
+  P.dampDepth = c.dampingLayerDepth;
+  P.U_g = c.U_g; P.V_g = c.V_g; P.z_Ug = c.z_Ug; P.z_Vg = c.z_Vg; P.Ug_grad = c.Ug_grad; P.Vg_grad = c.Vg_grad;
+  P.fHorz = c.corioConstHorz; P.fVert = c.corioConstVert; P.fLS = c.corioLS_fact;
+  P.oneRK = c.physics_oneRKonly;
+  P.tempGrnd = c.temp_grnd; P.presGrnd = c.pres_grnd;
+  P.R_gas = c.R_gas; P.R_vapor = c.R_vapor; P.Rv_Rg = c.Rv_Rg; P.cp_gas = c.cp_gas; P.cv_gas = c.cv_gas;
+  P.g = c.accel_g; P.R_cp = c.R_cp; P.cp_R = c.cp_R; P.cp_cv = c.cp_cv; P.p0 = c.refPressure; P.kappa = c.kappa;
+  P.L_v = c.L_v;
+}
+
+static int dev_alloc(fe_domain* d, float** p, size_t nfloats) {
+  cudaError_t e = cudaMalloc((void**)p, nfloats * sizeof(float));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(FE_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  d->bytes += nfloats * sizeof(float);
+  CU(cudaMemsetAsync(*p, 0, nfloats * sizeof(float), d->stream));
+  return FE_OK;
+}
+
+static void free_domain(fe_domain* d) {
+  if (!d) return;
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  for (int b = 0; b < 3; b++) {
+    cudaFree(d->st[b]);
+    cudaFree(d->pr[b]);
+  }
+  cudaFree(d->grid);
+  cudaFree(d->base);
+  cudaFree(d->scratch);
+  cudaFree(d->surf);
+  cudaFree(d->frhs);
+  cudaFree(d->clock);
+  if (d->stream) cudaStreamDestroy(d->stream);
+  delete d;
+}
+
+extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
+  if (!cfg || !out) return set_err(FE_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  int ndev = fe_device_count();
+  if (ndev <= 0) return set_err(FE_ERR_NO_DEVICE, "no CUDA device visible");
+  if (device < 0 || device >= ndev) return set_err(FE_ERR_ARG, "device index out of range");
+  fe_domain* d = new fe_domain();
+  d->cfg = *cfg;
+  d->device = device;
+  make_phys(d);
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete d;
+    return set_err(FE_ERR_CUDA, "cannot create a stream on the device");
+  }
+  const Phys& P = d->P;
+  const size_t n = (size_t)P.n, n2 = (size_t)P.n2;
+  for (int b = 0; b < 3 && rc == FE_OK; b++) {
+    rc = dev_alloc(d, &d->st[b], n * P.nf);
+    if (rc == FE_OK) rc = dev_alloc(d, &d->pr[b], n);
+  }
+  const size_t nscr = (size_t)(9 + 3 + 1 + 3 * std::max(P.nmoist, 1));
+  if (rc == FE_OK) rc = dev_alloc(d, &d->grid, n * 6);
+  if (rc == FE_OK) rc = dev_alloc(d, &d->base, n * 3);
+  if (rc == FE_OK) rc = dev_alloc(d, &d->scratch, n * nscr);
+  if (rc == FE_OK) rc = dev_alloc(d, &d->surf, n2 * 11);
+  if (rc == FE_OK) {
+    cudaError_t e = cudaMalloc(&d->clock, 64);
+    if (e != cudaSuccess) rc = set_err(FE_ERR_NOMEM, "clock allocation failed");
+    else cudaMemsetAsync(d->clock, 0, 64, d->stream);
+  }
+  if (rc != FE_OK) {
+    free_domain(d);
+    return rc;
+  }
+  Ptrs& Q = d->Q;
+  Q.zPos = d->grid;
+  Q.J31 = d->grid + n;
+  Q.J32 = d->grid + 2 * n;
+  Q.J33 = d->grid + 3 * n;
+  Q.D = d->grid + 4 * n;
+  Q.invD = d->grid + 5 * n;
+  Q.rhoBS = d->base;
+  Q.thBS = d->base + n;
+  Q.pBS = d->base + 2 * n;
+  Q.tau = d->scratch;
+  Q.tkeQ = d->scratch + 9 * n;
+  Q.ls = d->scratch + 12 * n;
+  Q.mtau = d->scratch + 13 * n;
+  float* s = d->surf;
+  Q.cd = s; Q.ch = s + n2; Q.cq = s + 2 * n2; Q.fricVel = s + 3 * n2; Q.htFlux = s + 4 * n2; Q.tskin = s + 5 * n2;
+  Q.invOblen = s + 6 * n2; Q.z0m = s + 7 * n2; Q.z0t = s + 8 * n2; Q.qFlux = s + 9 * n2; Q.qskin = s + 10 * n2;
+  Q.clockIt = (int*)d->clock;
+  Q.clockTime = (float*)((char*)d->clock + 16);
+  // device-evaluated constants (the reference evaluates them with device powf in every kernel)
+  float* kc = nullptr;
+  if (cudaMalloc(&kc, 2 * sizeof(float)) != cudaSuccess) {
+    free_domain(d);
+    return set_err(FE_ERR_NOMEM, "constant buffer allocation failed");
+  }
+  fe::k_consts<<<1, 1, 0, d->stream>>>(P.R_gas, P.p0, P.R_cp, P.presGrnd, kc);
+  float hc[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(hc, kc, sizeof(hc), cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  cudaFree(kc);
+  if (e != cudaSuccess) {
+    free_domain(d);
+    return set_err(FE_ERR_CUDA, std::string("constant setup failed: ") + cudaGetErrorString(e));
+  }
+  d->P.c1 = hc[0];
+  d->P.presFac = hc[1];
+  d->launches = 1;
+  *out = d;
+  return FE_OK;
+}
+
+extern "C" int fe_destroy(fe_domain* d) {
+  if (!d) return FE_OK;
+  cudaSetDevice(d->device);
+  cudaStreamSynchronize(d->stream);
+  free_domain(d);
+  return FE_OK;
+}
+
+extern "C" size_t fe_device_bytes(const fe_domain* d) { return d ? d->bytes : 0; }
+extern "C" void* fe_stream(fe_domain* d) { return d ? (void*)d->stream : nullptr; }
+extern "C" long long fe_launch_count(const fe_domain* d) { return d ? d->launches : 0; }
+
+static int h2d(fe_domain* d, float* dst, const float* src, size_t nfloats) {
+  if (!src) return FE_OK;
+  CU(cudaMemcpyAsync(dst, src, nfloats * sizeof(float), cudaMemcpyHostToDevice, d->stream));
+  return FE_OK;
+}
+
+static void invalidate_graph(fe_domain* d) {
+  if (d->graph) {
+    cudaGraphExecDestroy(d->graph);
+    d->graph = nullptr;
+    d->graphSteps = 0;
+  }
+}
+
+extern "C" int fe_set_grid(fe_domain* d, const float* zPos, const float* J31, const float* J32, const float* J33,
+                           const float* D_Jac, const float* invD_Jac) {
+  if (!d || !zPos || !J31 || !J32 || !J33 || !D_Jac || !invD_Jac) return set_err(FE_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(d->device));
+  const size_t n = (size_t)d->P.n;
+  int rc = h2d(d, d->grid, zPos, n);
+  if (!rc) rc = h2d(d, d->grid + n, J31, n);
+  if (!rc) rc = h2d(d, d->grid + 2 * n, J32, n);
+  if (!rc) rc = h2d(d, d->grid + 3 * n, J33, n);
+  if (!rc) rc = h2d(d, d->grid + 4 * n, D_Jac, n);
+  if (!rc) rc = h2d(d, d->grid + 5 * n, invD_Jac, n);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(d->stream));
+  d->haveGrid = true;
+  return FE_OK;
+}
+
+extern "C" int fe_set_base_state(fe_domain* d, const float* bs) {
+  if (!d || !bs) return set_err(FE_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(d->device));
+  const size_t n = (size_t)d->P.n;
+  int rc = h2d(d, d->base, bs, 2 * n);
+  if (rc) return rc;
+  const int thr = 256;
+  fe::k_pbs<<<(unsigned)((n + thr - 1) / thr), thr, 0, d->stream>>>((long long)n, d->base + n, d->P.c1, d->P.cp_cv,
+                                                                    d->base + 2 * n);
+  d->launches++;
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(d->stream));
+  d->haveBase = true;
+  return FE_OK;
+}
+
+extern "C" int fe_set_surface(fe_domain* d, const float* z0m, const float* z0t, const float* htFlux, const float* tskin,
+                              const float* fricVel, const float* qFlux, const float* qskin) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  const size_t n2 = (size_t)d->P.n2;
+  int rc = h2d(d, d->Q.z0m, z0m, n2);
+  if (!rc) rc = h2d(d, d->Q.z0t, z0t, n2);
+  if (!rc) rc = h2d(d, d->Q.htFlux, htFlux, n2);
+  if (!rc) rc = h2d(d, d->Q.tskin, tskin, n2);
+  if (!rc) rc = h2d(d, d->Q.fricVel, fricVel, n2);
+  if (!rc) rc = h2d(d, d->Q.qFlux, qFlux, n2);
+  if (!rc) rc = h2d(d, d->Q.qskin, qskin, n2);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_set_clock(fe_domain* d, float simTime, int simTime_it) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  int it = simTime_it;
+  CU(cudaMemcpyAsync(d->Q.clockIt, &it, sizeof(int), cudaMemcpyHostToDevice, d->stream));
+  CU(cudaMemcpyAsync(d->Q.clockTime, &simTime, sizeof(float), cudaMemcpyHostToDevice, d->stream));
+  CU(cudaStreamSynchronize(d->stream));
+  d->simTime = simTime;
+  d->simIt = simTime_it;
+  return FE_OK;
+}
+
+extern "C" int fe_get_clock(const fe_domain* d, float* simTime, int* simTime_it) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (simTime) *simTime = d->simTime;
+  if (simTime_it) *simTime_it = d->simIt;
+  return FE_OK;
+}
+
+static unsigned blocks1d(long long n, int thr) { return (unsigned)((n + thr - 1) / thr); }
+
+extern "C" int fe_set_state(fe_domain* d, const float* hydro, const float* sgstke, const float* moist) {
+  if (!d || !hydro) return set_err(FE_ERR_ARG, "NULL argument");
+  if (!d->haveGrid || !d->haveBase) return set_err(FE_ERR_STATE, "set the grid and base state before the state");
+  if (d->P.ntke && !sgstke) return set_err(FE_ERR_ARG, "TKE field required");
+  if (d->P.nmoist && !moist) return set_err(FE_ERR_ARG, "moisture fields required");
+  CU(cudaSetDevice(d->device));
+  const Phys& P = d->P;
+  const size_t n = (size_t)P.n;
+  float* A = d->st[0];
+  int rc = h2d(d, A, hydro, 5 * n);
+  if (!rc && P.ntke) rc = h2d(d, A + 5 * n, sgstke, n);
+  if (!rc && P.nmoist) rc = h2d(d, A + (5 + P.ntke) * n, moist, n * P.nmoist);
+  if (rc) return rc;
+  fe::k_fill<<<blocks1d(P.n, 256), 256, 0, d->stream>>>(P, d->Q, A);
+  CU(cudaGetLastError());
+  fe::k_pressure<<<blocks1d(P.n, 256), 256, 0, d->stream>>>(P, d->Q, A, d->pr[0]);
+  CU(cudaGetLastError());
+  d->launches += 2;
+  // the boundary values that never change (base-state and constant halos) must be valid
+  // in every buffer, so start B and C as copies of the filled A
+  for (int b = 1; b < 3; b++) {
+    CU(cudaMemcpyAsync(d->st[b], A, n * P.nf * sizeof(float), cudaMemcpyDeviceToDevice, d->stream));
+    CU(cudaMemcpyAsync(d->pr[b], d->pr[0], n * sizeof(float), cudaMemcpyDeviceToDevice, d->stream));
+  }
+  CU(cudaStreamSynchronize(d->stream));
+  d->haveState = true;
+  return FE_OK;
+}
+
+static dim3 stage_grid(const fe_domain* d) {
+  const Phys& P = d->P;
+  return dim3((P.Nz + d->tk - 1) / d->tk, (P.Ny + d->tj - 1) / d->tj, (P.Nx + d->ti - 1) / d->ti);
+}
+static dim3 turb_grid(const fe_domain* d) {
+  const Phys& P = d->P;
+  return dim3((P.Nz + 2 + d->tk - 1) / d->tk, (P.Ny + 1 + d->tj - 1) / d->tj, (P.Nx + 1 + d->ti - 1) / d->ti);
+}
+
+static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }
+
+// Enqueue one RK3 step on stream s (no host synchronisation; graph-capturable).
+static void enqueue_step(fe_domain* d, cudaStream_t s) {
+  const Phys& P = d->P;
+  const Ptrs& Q = d->Q;
+  dim3 blk(d->tk, d->tj, d->ti), g = stage_grid(d), gt = turb_grid(d);
+  float *A = d->st[0], *B = d->st[1], *C = d->st[2];
+  const bool physPrep = (P.turb || P.surf > 0);
+  if (physPrep && stage_has_physics(d, 0)) { fe::k_turb<<<gt, blk, 0, s>>>(P, Q, A, 0); d->launches++; }
+  fe::k_stage<0, fe::MODE_COMMIT><<<g, blk, 0, s>>>(P, Q, A, A, B, d->pr[0], d->pr[1], nullptr);
+  if (physPrep && stage_has_physics(d, 1)) { fe::k_turb<<<gt, blk, 0, s>>>(P, Q, B, 1); d->launches++; }
+  fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, s>>>(P, Q, B, A, C, d->pr[1], d->pr[2], nullptr);
+  if (physPrep && stage_has_physics(d, 2)) { fe::k_turb<<<gt, blk, 0, s>>>(P, Q, C, 2); d->launches++; }
+  fe::k_stage<2, fe::MODE_COMMIT><<<g, blk, 0, s>>>(P, Q, C, A, A, d->pr[2], d->pr[0], nullptr);
+  fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
+  d->launches += 4;
+}
+
+static const int kGraphSteps = 8;
+
+static int build_graph(fe_domain* d) {
+  invalidate_graph(d);
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+  const long long before = d->launches;
+  for (int s = 0; s < kGraphSteps; s++) enqueue_step(d, d->stream);
+  d->launches = before;
+  cudaError_t e = cudaStreamEndCapture(d->stream, &g);
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&d->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    d->graph = nullptr;
+    return set_err(FE_ERR_CUDA, std::string("graph instantiate failed: ") + cudaGetErrorString(e));
+  }
+  d->graphSteps = kGraphSteps;
+  return FE_OK;
+}
+
+static int launches_per_step(const fe_domain* d) {
+  int l = 4;
+  if (d->P.turb || d->P.surf > 0) l += d->P.oneRK ? 1 : 3;
+  return l;
+}
+
+extern "C" int fe_advance(fe_domain* d, int nsteps) {
+  if (!d || nsteps < 0) return set_err(FE_ERR_ARG, "bad argument");
+  if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
+  CU(cudaSetDevice(d->device));
+  int left = nsteps;
+  if (left >= kGraphSteps) {
+    if (!d->graph) {
+      int rc = build_graph(d);
+      if (rc) return rc;
+    }
+    while (left >= kGraphSteps) {
+      CU(cudaGraphLaunch(d->graph, d->stream));
+      d->launches += (long long)kGraphSteps * launches_per_step(d);
+      left -= kGraphSteps;
+    }
+  }
+  for (; left > 0; left--) enqueue_step(d, d->stream);
+  CU(cudaGetLastError());
+  for (int s = 0; s < nsteps; s++) {
+    d->simTime = d->simTime + d->P.dt;
+    d->simIt += 1;
+  }
+  return FE_OK;
+}
+
+extern "C" int fe_sync(fe_domain* d) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  CU(cudaStreamSynchronize(d->stream));
+  CU(cudaGetLastError());
+  return FE_OK;
+}
+
+static int d2h(fe_domain* d, float* dst, const float* src, size_t nfloats) {
+  if (!dst) return FE_OK;
+  CU(cudaMemcpyAsync(dst, src, nfloats * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_get_state(fe_domain* d, float* hydro, float* sgstke, float* moist, float* pres) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  const Phys& P = d->P;
+  const size_t n = (size_t)P.n;
+  int rc = d2h(d, hydro, d->st[0], 5 * n);
+  if (!rc && P.ntke) rc = d2h(d, sgstke, d->st[0] + 5 * n, n);
+  if (!rc && P.nmoist) rc = d2h(d, moist, d->st[0] + (5 + P.ntke) * n, n * P.nmoist);
+  if (!rc) rc = d2h(d, pres, d->pr[0], n);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_get_surface(fe_domain* d, float* cd, float* ch, float* fricVel, float* htFlux, float* invOblen,
+                              float* tskin, float* qFlux, float* qskin) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  const size_t n2 = (size_t)d->P.n2;
+  const Ptrs& Q = d->Q;
+  int rc = d2h(d, cd, Q.cd, n2);
+  if (!rc) rc = d2h(d, ch, Q.ch, n2);
+  if (!rc) rc = d2h(d, fricVel, Q.fricVel, n2);
+  if (!rc) rc = d2h(d, htFlux, Q.htFlux, n2);
+  if (!rc) rc = d2h(d, invOblen, Q.invOblen, n2);
+  if (!rc) rc = d2h(d, tskin, Q.tskin, n2);
+  if (!rc) rc = d2h(d, qFlux, Q.qFlux, n2);
+  if (!rc) rc = d2h(d, qskin, Q.qskin, n2);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_build_frhs(fe_domain* d, int stage) {
+  if (!d || stage < 0 || stage > 2) return set_err(FE_ERR_ARG, "bad argument");
+  if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
+  CU(cudaSetDevice(d->device));
+  const Phys& P = d->P;
+  if (!d->frhs) {
+    int rc = dev_alloc(d, &d->frhs, (size_t)P.n * P.nf);
+    if (rc) return rc;
+  }
+  dim3 blk(d->tk, d->tj, d->ti);
+  float* A = d->st[0];
+  if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
+    fe::k_turb<<<turb_grid(d), blk, 0, d->stream>>>(P, d->Q, A, stage);
+    d->launches++;
+  }
+  switch (stage) {
+    case 0: fe::k_stage<0, fe::MODE_FRHS><<<stage_grid(d), blk, 0, d->stream>>>(P, d->Q, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
+    case 1: fe::k_stage<1, fe::MODE_FRHS><<<stage_grid(d), blk, 0, d->stream>>>(P, d->Q, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
+    default: fe::k_stage<2, fe::MODE_FRHS><<<stage_grid(d), blk, 0, d->stream>>>(P, d->Q, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
+  }
+  d->launches++;
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_get_frhs(fe_domain* d, float* hydroFrhs, float* sgstkeFrhs, float* moistFrhs, float* taus) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (!d->frhs) return set_err(FE_ERR_STATE, "no tendency evaluated yet");
+  CU(cudaSetDevice(d->device));
+  const Phys& P = d->P;
+  const size_t n = (size_t)P.n;
+  int rc = d2h(d, hydroFrhs, d->frhs, 5 * n);
+  if (!rc && P.ntke) rc = d2h(d, sgstkeFrhs, d->frhs + 5 * n, n);
+  if (!rc && P.nmoist) rc = d2h(d, moistFrhs, d->frhs + (5 + P.ntke) * n, n * P.nmoist);
+  if (!rc) rc = d2h(d, taus, d->Q.tau, 9 * n);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_count_nonfinite(fe_domain* d, long long* count) {
+  if (!d || !count) return set_err(FE_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(d->device));
+  unsigned long long* dc = nullptr;
+  CU(cudaMalloc(&dc, sizeof(unsigned long long)));
+  cudaMemsetAsync(dc, 0, sizeof(unsigned long long), d->stream);
+  fe::k_nonfinite<<<blocks1d(d->P.n, 256), 256, 0, d->stream>>>(d->P, d->st[0], dc);
+  d->launches++;
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, dc, sizeof(h), cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  cudaFree(dc);
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, cudaGetErrorString(e));
+  *count = (long long)h;
+  return FE_OK;
+}
+
+extern "C" int fe_domain_means(fe_domain* d, double* means) {
+  if (!d || !means) return set_err(FE_ERR_ARG, "NULL argument");
+  CU(cudaSetDevice(d->device));
+  double* dm = nullptr;
+  const int nf = d->P.nf;
+  CU(cudaMalloc(&dm, sizeof(double) * nf));
+  cudaMemsetAsync(dm, 0, sizeof(double) * nf, d->stream);
+  fe::k_means<<<blocks1d(d->P.n, 256), 256, 0, d->stream>>>(d->P, d->st[0], dm);
+  d->launches++;
+  cudaError_t e = cudaMemcpyAsync(means, dm, sizeof(double) * nf, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  cudaFree(dm);
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, cudaGetErrorString(e));
+  const double cells = (double)d->P.Nx * d->P.Ny * d->P.Nz;
+  for (int f = 0; f < nf; f++) means[f] /= cells;
+  return FE_OK;
+}
+
+extern "C" int fe_set_tiling(fe_domain* d, int tk, int tj, int ti) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (tk <= 0) tk = 32;
+  if (tj <= 0) tj = 4;
+  if (ti <= 0) ti = 2;
+  if (tk * tj * ti > 256 || tk % 32 != 0) return set_err(FE_ERR_ARG, "tile must have <= 256 threads and tk a multiple of 32");
+  d->tk = tk; d->tj = tj; d->ti = ti;
+  invalidate_graph(d);
+  return FE_OK;
+}
+
+// Autotuner: times the dynamics stage kernel (writes only the stage-2 buffer C, which
+// every step overwrites) for each candidate launch shape and keeps the fastest.
+extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
+  CU(cudaSetDevice(d->device));
+  static const int cand[][3] = {{32, 4, 2}, {32, 8, 1}, {32, 2, 4}, {64, 2, 2}, {64, 4, 1}, {32, 4, 1},
+                                {32, 2, 2}, {64, 2, 1}, {128, 2, 1}, {32, 1, 8}};
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bi = 0;
+  const int reps = 5;
+  for (int c = 0; c < (int)(sizeof(cand) / sizeof(cand[0])); c++) {
+    if (cand[c][0] > 32 * ((d->P.Nz + 31) / 32) && cand[c][0] > 32) continue;
+    d->tk = cand[c][0]; d->tj = cand[c][1]; d->ti = cand[c][2];
+    dim3 blk(d->tk, d->tj, d->ti), g = stage_grid(d);
+    fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, d->stream>>>(d->P, d->Q, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
+    cudaEventRecord(e0, d->stream);
+    for (int r = 0; r < reps; r++)
+      fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, d->stream>>>(d->P, d->Q, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
+    cudaEventRecord(e1, d->stream);
+    d->launches += reps + 1;
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) { best = ms; bi = c; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU(cudaGetLastError());
+  d->tk = cand[bi][0]; d->tj = cand[bi][1]; d->ti = cand[bi][2];
+  invalidate_graph(d);
+  if (tk) *tk = d->tk;
+  if (tj) *tj = d->tj;
+  if (ti) *ti = d->ti;
+  return FE_OK;
+}
+
+// ------------------------------------------------------------------ ensembles
+extern "C" int fe_ensemble_create(fe_domain** members, int n, fe_ensemble** out) {
+  if (!members || n <= 0 || !out) return set_err(FE_ERR_ARG, "bad argument");
+  fe_ensemble* e = new fe_ensemble();
+  for (int i = 0; i < n; i++) {
+    if (!members[i] || members[i]->device != members[0]->device) {
+      delete e;
+      return set_err(FE_ERR_ARG, "members must be valid and on one device");
+    }
+    e->m.push_back(members[i]);
+  }
+  if (cudaSetDevice(members[0]->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return set_err(FE_ERR_CUDA, "cannot create ensemble stream");
+  }
+  *out = e;
+  return FE_OK;
+}
+
+// One graph holds kGraphSteps steps of every member, members as independent branches.
+static int ens_build_graph(fe_ensemble* e) {
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  e->graph = nullptr;
+  cudaGraph_t g = nullptr;
+  std::vector<cudaEvent_t> ev(e->m.size());
+  cudaEvent_t fork;
+  CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  for (auto& x : ev) CU(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+  CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  cudaEventRecord(fork, e->stream);
+  for (size_t i = 0; i < e->m.size(); i++) {
+    fe_domain* d = e->m[i];
+    cudaStreamWaitEvent(d->stream, fork, 0);
+    const long long before = d->launches;
+    for (int s = 0; s < kGraphSteps; s++) enqueue_step(d, d->stream);
+    d->launches = before;
+    cudaEventRecord(ev[i], d->stream);
+    cudaStreamWaitEvent(e->stream, ev[i], 0);
+  }
+  cudaError_t err = cudaStreamEndCapture(e->stream, &g);
+  cudaEventDestroy(fork);
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (err != cudaSuccess) return set_err(FE_ERR_CUDA, std::string("ensemble capture failed: ") + cudaGetErrorString(err));
+  err = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (err != cudaSuccess) {
+    e->graph = nullptr;
+    return set_err(FE_ERR_CUDA, std::string("ensemble instantiate failed: ") + cudaGetErrorString(err));
+  }
+  e->graphSteps = kGraphSteps;
+  return FE_OK;
+}
+
+extern "C" int fe_ensemble_advance(fe_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return set_err(FE_ERR_ARG, "bad argument");
+  for (auto* d : e->m)
+    if (!d->haveState) return set_err(FE_ERR_STATE, "member state not set");
+  CU(cudaSetDevice(e->m[0]->device));
+  int left = nsteps;
+  if (left >= kGraphSteps && !e->graph) {
+    int rc = ens_build_graph(e);
+    if (rc) return rc;
+  }
+  while (left >= kGraphSteps) {
+    CU(cudaGraphLaunch(e->graph, e->stream));
+    for (auto* d : e->m) d->launches += (long long)kGraphSteps * launches_per_step(d);
+    left -= kGraphSteps;
+  }
+  if (left > 0) {
+    cudaEvent_t fork;
+    CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    cudaEventRecord(fork, e->stream);
+    for (auto* d : e->m) {
+      cudaStreamWaitEvent(d->stream, fork, 0);
+      for (int s = 0; s < left; s++) enqueue_step(d, d->stream);
+      cudaEvent_t done;
+      cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+      cudaEventRecord(done, d->stream);
+      cudaStreamWaitEvent(e->stream, done, 0);
+      cudaEventDestroy(done);
+    }
+    cudaEventDestroy(fork);
+  }
+  CU(cudaGetLastError());
+  for (auto* d : e->m)
+    for (int s = 0; s < nsteps; s++) {
+      d->simTime = d->simTime + d->P.dt;
+      d->simIt += 1;
+    }
+  return FE_OK;
+}
+
+extern "C" int fe_ensemble_sync(fe_ensemble* e) {
+  if (!e) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(e->m[0]->device));
+  CU(cudaStreamSynchronize(e->stream));
+  for (auto* d : e->m) CU(cudaStreamSynchronize(d->stream));
+  CU(cudaGetLastError());
+  return FE_OK;
+}
+
+extern "C" void* fe_ensemble_stream(fe_ensemble* e) { return e ? (void*)e->stream : nullptr; }
+
+extern "C" int fe_ensemble_destroy(fe_ensemble* e) {
+  if (!e) return FE_OK;
+  cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  cudaStreamDestroy(e->stream);
+  delete e;
+  return FE_OK;
+}

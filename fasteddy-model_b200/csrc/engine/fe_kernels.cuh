@@ -1,0 +1,736 @@
+// fe_kernels.cuh -- CUDA kernels of the hot path (sm_100a).
+//
+//   k_consts      device-evaluated constants c1 = R/p0^(R/cp) and (p0/p_grnd)^(R/cp)
+//   k_pbs         powf(thBS*c1, cp/cv) per cell (the base-state pressure term of p')
+//   k_fill        boundary values of every halo cell of a state block (gather form)
+//   k_pressure    perturbation pressure of a state block, halo-inclusive
+//   k_turb        last-stage SGS physics on the +1 ring: strain, length scale, Km, stresses,
+//                 TKE transport fluxes, moisture SGS fluxes, surface layer
+//   k_stage       fused tendency + WS2002 RK3 commit of one stage; writes the next state
+//                 with its halo images and its perturbation pressure (or, in Frhs mode,
+//                 writes the tendency only)
+//   k_clock       advance the device simulation clock after the last stage
+//   k_nonfinite, k_means   device reductions (NaN/Inf count, FP64 domain means)
+#pragma once
+#include "fe_device.cuh"
+
+namespace fe {
+
+constexpr int MODE_COMMIT = 0;
+constexpr int MODE_FRHS = 1;
+
+__global__ void k_consts(float R_gas, float p0, float R_cp, float presGrnd, float* out) {
+  out[0] = R_gas / powf(p0, R_cp);
+  out[1] = powf((p0 / presGrnd), R_cp);
+}
+
+__global__ void k_pbs(long long n, const float* __restrict__ thBS, float c1, float cp_cv, float* __restrict__ pBS) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) pBS[t] = powf(thBS[t] * c1, cp_cv);
+}
+
+__device__ __forceinline__ int wrap_i(const Phys& P, int i) { return i < P.iMin ? i + P.Nx : (i >= P.iMax ? i - P.Nx : i); }
+__device__ __forceinline__ int wrap_j(const Phys& P, int j) { return j < P.jMin ? j + P.Ny : (j >= P.jMax ? j - P.Ny : j); }
+
+// Boundary value of field f at halo cell (i,j,k): the vertical boundary rule applied on
+// the periodic source column, i.e. the reference's Commence BCs (cuda_hydroCoreDevice.cu:
+// 469-550) with every read of the current stage.
+__global__ void k_fill(Phys P, Ptrs Q, float* st) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.n) return;
+  const int k = (int)(t % P.nzh);
+  const int j = (int)((t / P.nzh) % P.nyh);
+  const int i = (int)(t / ((long long)P.nzh * P.nyh));
+  const bool inI = i >= P.iMin && i < P.iMax, inJ = j >= P.jMin && j < P.jMax, inK = k >= P.kMin && k < P.kMax;
+  if (inI && inJ && inK) return;
+  const int is = wrap_i(P, i), js = wrap_j(P, j);
+  const long long col = (long long)is * P.si + (long long)js * P.sj;
+  const long long src = col + k;
+  const long long bot = col + P.kMin, top = col + P.kMax - 1;
+  for (int f = 0; f < P.nf; f++) {
+    float* F = st + (long long)f * P.n;
+    float v;
+    if (inK) {
+      v = F[src];
+    } else {
+      const bool below = k < P.kMin;
+      if (f == 0) v = Q.rhoBS[src];
+      else if (f == 4) v = Q.thBS[src];
+      else if (f <= 3) v = below ? F[bot] : momentum_bs(P, f, Q.zPos[top], Q.rhoBS[top]);
+      else if (f == 5 && P.ntke) v = below ? F[bot] : 0.0f;
+      else v = below ? F[bot] : F[top];
+    }
+    F[t] = v;
+  }
+}
+
+// Perturbation pressure over the halo-inclusive block (cuda_pressureDevice.cu:53-113):
+// levels 1..kMin-1 use the kMin cell, levels >= kMax use kMax-1, level 0 its own cell.
+__global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, float* __restrict__ pres) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P.n) return;
+  const int k = (int)(t % P.nzh);
+  long long src = t;
+  if (k > 0 && k < P.kMin) src = t - k + P.kMin;
+  else if (k >= P.kMax) src = t - k + P.kMax - 1;
+  pres[t] = pert_pressure(P, st, Q.pBS, src);
+}
+
+__device__ __forceinline__ float rinv(float r) { return 1.0f / fmaxf(r, 1e-6f); }
+
+// SGS length scale at cell c (cuda_sgstkeDevice.cu:96-151).
+__device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, const float* __restrict__ rho,
+                                              const float* __restrict__ th, const float* __restrict__ e, long long c) {
+  const int si = P.si, sj = P.sj;
+#define THr(x) (th[x] * rinv(rho[x]))
+  const float dthdz = (float)(0.5 * (double)((Q.J31[c] * P.dXi * (THr(c + si) - THr(c - si))) +
+                                             (Q.J32[c] * P.dYi * (THr(c + sj) - THr(c - sj))) +
+                                             (Q.J33[c] * P.dZi * (THr(c + 1) - THr(c - 1)))));
+  const float N2 = (P.g / THr(c)) * dthdz;
+#undef THr
+  const float len2 = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
+  if (N2 > 0.0f) {
+    const float tb = powf(N2, -0.5f);
+    const float ec = e[c] * rinv(rho[c]);
+    const float len1 = (float)(0.76 * (double)powf(ec, 0.5f) * (double)tb);
+    return fmaxf(fminf(len1, len2), 1e-2f);
+  }
+  return len2;
+}
+
+// ------------------------------------------------------------------ surface layer
+// Land-surface update and Monin-Obukhov iteration of one column (cuda_surfaceLayerDevice.cu:
+// 112-521). Writes tau31, tau32, tauTH3 (and the q_v flux) at kMin.
+__device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int stage) {
+  const long long c = (long long)i * P.si + (long long)j * P.sj + P.kMin;
+  const long long ij = (long long)i * P.nyh + j;
+  const bool moist = P.moist > 0 && P.nmoist > 0;
+  const float pi = acosf(-1.0f);
+  const int it = *Q.clockIt;
+  const float simTime = *Q.clockTime;
+  const float* rho = st;
+  const float r = rho[c], mu = st[P.n + c], mv = st[2 * P.n + c], mth = st[4 * P.n + c];
+  const float mq = moist ? st[(long long)(5 + P.ntke) * P.n + c] : 0.0f;
+  float z0 = Q.z0m[ij];
+  float z1 = 0.5f / (P.dZi * Q.J33[c]);
+  float z1oz0 = (z1 + z0) / z0;
+  float z0t = Q.z0t[ij];
+  float z1ozt0 = (z1 + z0t) / z0t;
+  float u1 = mu / r, v1 = mv / r;
+  float U1 = sqrtf(powf(u1, 2.0f) + powf(v1, 2.0f));
+  float th1 = mth / r;
+  float q1 = mq / r;
+  float qsk_input = moist ? Q.qskin[ij] : 0.0f;
+  // ---- LSM
+  if (it == P.itRestart && it == 0) {
+    Q.cd[ij] = powf(P.kappa, 2.0f) / powf(logf(z1oz0), 2.0f);
+    Q.ch[ij] = powf(P.kappa, 2.0f) / powf(logf(z1ozt0), 2.0f);
+    if (moist) Q.cq[ij] = powf(P.kappa, 2.0f) / powf(logf(z1ozt0), 2.0f);
+  } else if (it == P.itRestart && it != 0) {
+    Q.cd[ij] = powf(Q.fricVel[ij], 2.0f) / (powf(U1, 2.0f));
+    float th0 = Q.tskin[ij] * P.presFac;
+    Q.ch[ij] = Q.htFlux[ij] / (U1 * (th0 - th1));
+    if (moist) Q.cq[ij] = Q.qFlux[ij] / (U1 * (Q.qskin[ij] - q1));
+  }
+  if (P.surf == 1) {
+    if (P.idealSine == 1) {
+      if ((simTime > P.idealTs) && (simTime <= P.idealTe))
+        Q.htFlux[ij] = (float)(P.wth + P.idealAmp * sin(pi * (simTime - P.idealTs) / (P.idealTe - P.idealTs)));
+      else
+        Q.htFlux[ij] = P.wth;
+      if (moist) {
+        if ((simTime > P.idealQts) && (simTime <= P.idealQte))
+          Q.qFlux[ij] = (float)(P.idealQamp * sin(pi * (simTime - P.idealQts) / (P.idealQte - P.idealQts)));
+        else
+          Q.qFlux[ij] = P.wq;
+      }
+    }
+  } else if (P.surf == 2) {
+    const float tff = (float)P.tempFreq;
+    float tsk_c, qsk_c = 0.0f;
+    if ((it % P.tempFreq == 0) && (stage == 2)) {
+      if (P.idealSine == 1 && (simTime > P.idealTs) && (simTime < P.idealTe + P.dt * tff)) {
+        float prev = fmaxf(simTime - tff * P.dt, P.idealTs);
+        float inc = (float)(P.idealAmp * (sin(pi * (simTime - P.idealTs) / (P.idealTe - P.idealTs)) -
+                                          sin(pi * (prev - P.idealTs) / (P.idealTe - P.idealTs))));
+        tsk_c = Q.tskin[ij] + inc;
+        if (moist) {
+          float qinc = (float)(P.idealQamp * (sin(pi * (simTime - P.idealQts) / (P.idealQte - P.idealQts)) -
+                                              sin(pi * (prev - P.idealQts) / (P.idealQte - P.idealQts))));
+          qsk_c = Q.qskin[ij] + qinc;
+        }
+      } else {
+        tsk_c = (float)(Q.tskin[ij] + P.tr * P.dt * tff / 3600.0);
+        if (moist) qsk_c = (float)(Q.qskin[ij] + P.qr * P.dt * tff / 3600.0);
+      }
+      Q.tskin[ij] = tsk_c;
+      if (moist) Q.qskin[ij] = qsk_c;
+    } else {
+      tsk_c = Q.tskin[ij];
+      if (moist) qsk_c = Q.qskin[ij];
+    }
+    float th0 = tsk_c * P.presFac;
+    Q.htFlux[ij] = Q.ch[ij] * U1 * (th0 - th1);
+    if (moist) {
+      Q.qFlux[ij] = Q.cq[ij] * U1 * (qsk_c - q1);
+      if (P.qskinInput == 1) Q.qskin[ij] = qsk_input;
+    }
+  }
+  // ---- MOST
+  {
+    const float beta = 5.0f, ol_lim = 1.0f;
+    const int it_max = P.surfStab == 0 ? 5 : 1;
+    int it_n = 0;
+    float th0 = Q.tskin[ij] * P.presFac;
+    float q0 = moist ? Q.qskin[ij] : 0.0f;
+    float cd0 = Q.cd[ij], cd_i = 0.0f, ch_i = 0.0f, cq_i = 0.0f;
+    float fv = Q.fricVel[ij], iol = Q.invOblen[ij], hf = Q.htFlux[ij], qf = moist ? Q.qFlux[ij] : 0.0f;
+    do {
+      float tauxz = -cd0 * U1 * u1;
+      float tauyz = -cd0 * U1 * v1;
+      fv = powf(powf(tauxz, 2.0f) + powf(tauyz, 2.0f), 0.25f);
+      it_n = it_n + 1;
+      if (P.surfStab == 0) {
+        if (fv > 0.0f) {
+          iol = -(P.kappa * P.g * hf) / (powf(fv, 3.0f) * th1);
+          iol = fmaxf(fminf(iol, ol_lim), -ol_lim);
+        } else {
+          iol = -ol_lim;
+        }
+      } else {
+        iol = 0.0f;
+      }
+      float zol = iol * (z1 + z0);
+      float psi_m, psi_h;
+      if (zol < 0.0f) {
+        float xi = powf(1.0f - 16.0f * zol, 0.25f);
+        psi_m = (float)(logf(0.5f * (1.0f + powf(xi, 2.0f)) * powf(0.5f * (1.0f + xi), 2.0f)) - 2.0f * atanf(xi) + 0.5f * pi);
+        psi_h = 2.0f * logf(0.5f * (1.0f + powf(xi, 2.0f)));
+      } else {
+        psi_m = -beta * zol;
+        psi_h = -beta * zol;
+      }
+      cd_i = powf(P.kappa, 2.0f) / powf(logf(z1oz0) - psi_m, 2.0f);
+      ch_i = powf(P.kappa, 2.0f) / ((logf(z1ozt0) - psi_m) * (logf(z1ozt0) - psi_h));
+      cq_i = powf(P.kappa, 2.0f) / ((logf(z1ozt0) - psi_m) * (logf(z1ozt0) - psi_h));
+      if (P.surf > 1) {
+        hf = ch_i * U1 * (th0 - th1);
+        if (moist) qf = cq_i * U1 * (q0 - q1);
+      }
+      cd0 = cd_i;
+    } while (it_n <= it_max);
+    Q.cd[ij] = cd_i;
+    Q.ch[ij] = ch_i;
+    if (moist) Q.cq[ij] = cq_i;
+    float tauxz = -cd_i * sqrtf(powf(mu / r, 2.0f) + powf(mv / r, 2.0f)) * mu;
+    float tauyz = -cd_i * sqrtf(powf(mu / r, 2.0f) + powf(mv / r, 2.0f)) * mv;
+    Q.tau[2 * P.n + c] = tauxz;
+    Q.tau[3 * P.n + c] = tauyz;
+    fv = powf(powf(tauxz, 2.0f) + powf(tauyz, 2.0f), 0.25f);
+    Q.tau[8 * P.n + c] = hf * r;
+    if (moist && P.moistSGS > 0) Q.mtau[2 * P.n + c] = qf * r;
+    iol = -(P.kappa * P.g * hf) / (powf(fv, 3.0f) * th1);
+    Q.fricVel[ij] = fv;
+    Q.invOblen[ij] = iol;
+    Q.htFlux[ij] = hf;
+    if (moist) Q.qFlux[ij] = qf;
+  }
+}
+
+// ------------------------------------------------------------------ last-stage SGS physics
+// One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
+// (the reference's ring minus the i=iMax+1/j=jMax+1 cells, which nothing reads).
+__global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+  const int k = P.kMin - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = P.jMin - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = P.iMin - 1 + blockIdx.z * blockDim.z + threadIdx.z;
+  if (k > P.kMax || j > P.jMax || i > P.iMax) return;
+  const long long n = P.n;
+  const int si = P.si, sj = P.sj;
+  const long long c = (long long)i * si + (long long)j * sj + k;
+  const float *rho = st, *mu = st + n, *mv = st + 2 * n, *mw = st + 3 * n, *mth = st + 4 * n;
+  const float* e = P.ntke ? st + 5 * n : nullptr;
+  if (P.turb) {
+    float* T = Q.tau;
+    float Km = 0.0f, lsc = 0.0f;
+    const float delta = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
+    if (P.tke) lsc = length_scale(P, Q, rho, mth, e, c);
+    if (k >= P.kMin) {
+      const long long a = c - si, b = c - sj, d = c - 1, ab = a - sj, ad = a - 1, bd = b - 1, abd = ab - 1;
+      const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
+      const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
+#define U_(x) (mu[x] * rinv(rho[x]))
+#define V_(x) (mv[x] * rinv(rho[x]))
+#define W_(x) (mw[x] * rinv(rho[x]))
+#define TH_(x) (mth[x] * rinv(rho[x]))
+      float S11 = dXi * (U_(c) - U_(a));
+      float S22 = dYi * (V_(c) - V_(b));
+      float S33 = J1 * dXi * (W_(c) - W_(a)) + J2 * dYi * (W_(c) - W_(b)) + J3 * dZi * (W_(c) - W_(d));
+      float S21 = 0.5f * (0.5f * (dXi * (V_(c) - V_(a)) + dXi * (V_(b) - V_(ab))) +
+                          0.5f * (dYi * (U_(c) - U_(b)) + dYi * (U_(a) - U_(ab))));
+      float S31 = 0.5f * (0.5f * (dXi * (W_(c) - W_(a)) + dXi * (W_(d) - W_(ad))) +
+                          0.5f * (J1 * dXi * (U_(c) - U_(a)) + J1 * dXi * (U_(d) - U_(ad))) +
+                          0.25f * (J2 * dYi * (U_(c) - U_(b)) + J2 * dYi * (U_(a) - U_(ab)) + J2 * dYi * (U_(d) - U_(bd)) +
+                                   J2 * dYi * (U_(ad) - U_(abd))) +
+                          0.5f * (J3 * dZi * (U_(c) - U_(d)) + J3 * dZi * (U_(a) - U_(ad))));
+      float S32 = 0.5f * (0.5f * (dYi * (W_(c) - W_(b)) + dYi * (W_(d) - W_(bd))) +
+                          0.25f * (J1 * dXi * (V_(c) - V_(a)) + J1 * dXi * (V_(b) - V_(ab)) + J1 * dXi * (V_(d) - V_(ad)) +
+                                   J1 * dXi * (V_(bd) - V_(abd))) +
+                          0.5f * (J2 * dYi * (V_(c) - V_(b)) + J2 * dYi * (V_(d) - V_(bd))) +
+                          0.5f * (J3 * dZi * (V_(c) - V_(d)) + J3 * dZi * (V_(b) - V_(bd))));
+      float ST1 = dXi * (TH_(c) - TH_(a));
+      float ST2 = dYi * (TH_(c) - TH_(b));
+      float ST3 = (J1 * dXi * (TH_(c) - TH_(a))) + (J2 * dYi * (TH_(c) - TH_(b))) + (J3 * dZi * (TH_(c) - TH_(d)));
+#undef U_
+#undef V_
+#undef W_
+#undef TH_
+      const float r = rho[c];
+      if (P.tke) {
+        const float lsm = length_scale(P, Q, rho, mth, e, d);
+        const float e0 = e[c] * rinv(r), e1 = e[d] * rinv(rho[d]);
+        Km = (float)((double)P.c_k * 0.5 * (double)(lsc * powf(e0, 0.5f) + lsm * powf(e1, 0.5f)));
+        const float invPr = 1.0f + 2.0f * lsc / delta;
+        const float dev = (float)((2.0 / 3.0) * (double)r *
+                                  (double)(Km * (dXi * (mu[c] / r - mu[a] / rho[a]) + dYi * (mv[c] / r - mv[b] / rho[b]) +
+                                                 J1 * dXi * (mw[c] / r - mw[a] / rho[a]) +
+                                                 J2 * dYi * (mw[c] / r - mw[b] / rho[b]) +
+                                                 J3 * dZi * (mw[c] / r - mw[d] / rho[d])) +
+                                           e[c] / r));
+        T[c] = -2.0f * r * Km * S11 + dev;
+        T[n + c] = -2.0f * r * Km * S21;
+        T[2 * n + c] = -2.0f * r * Km * S31;
+        T[3 * n + c] = -2.0f * r * Km * S32;
+        T[4 * n + c] = -2.0f * r * Km * S22 + dev;
+        T[5 * n + c] = -2.0f * r * Km * S33 + dev;
+        T[6 * n + c] = -r * Km * invPr * ST1;
+        T[7 * n + c] = -r * Km * invPr * ST2;
+        T[8 * n + c] = -r * Km * invPr * ST3;
+      } else {
+        const float t1 = 0.5f * (S11 * S11 + S22 * S22 + S33 * S33) + S21 * S21 + S31 * S31 + S32 * S32;
+        const float N2 = P.g / (mth[c] * rinv(r)) * ST3;
+        const float t2 = N2 * 3.0f;
+        Km = (P.c_s * delta) * (P.c_s * delta) * sqrtf(fmaxf(0.0f, t1 - fmaxf(0.0f, t2)));
+        const float invPr = 1.0f + 2.0f * delta / delta;
+        T[c] = -2.0f * r * Km * S11;
+        T[n + c] = -2.0f * r * Km * S21;
+        T[2 * n + c] = -2.0f * r * Km * S31;
+        T[3 * n + c] = -2.0f * r * Km * S32;
+        T[4 * n + c] = -2.0f * r * Km * S22;
+        T[5 * n + c] = -2.0f * r * Km * S33;
+        T[6 * n + c] = -r * Km * invPr * ST1;
+        T[7 * n + c] = -r * Km * invPr * ST2;
+        T[8 * n + c] = -r * Km * invPr * ST3;
+      }
+    }
+    if (P.tke) {
+      Q.ls[c] = lsc;
+      // TKE transport fluxes (de/dx_j)*Km*rho (cuda_sgstkeDevice.cu:309-397), Km = 0 below kMin
+      const float ex = e[c + si] * rinv(rho[c + si]) - e[c - si] * rinv(rho[c - si]);
+      const float ey = e[c + sj] * rinv(rho[c + sj]) - e[c - sj] * rinv(rho[c - sj]);
+      const float ez = e[c + 1] * rinv(rho[c + 1]) - e[c - 1] * rinv(rho[c - 1]);
+      const float dedx = 0.5f * (P.dXi * ex);
+      const float dedy = 0.5f * (P.dYi * ey);
+      const float dedz = 0.5f * (Q.J31[c] * P.dXi * ex + Q.J32[c] * P.dYi * ey + Q.J33[c] * P.dZi * ez);
+      Q.tkeQ[c] = dedx * Km * rho[c];
+      Q.tkeQ[n + c] = dedy * Km * rho[c];
+      Q.tkeQ[2 * n + c] = dedz * Km * rho[c];
+    }
+    if (P.moist && P.moistSGS > 0) {
+      const float invPr = 1.0f + 2.0f * (P.tke ? lsc : delta) / delta;
+      for (int m = 0; m < P.nmoist; m++) {
+        const float* q = st + (long long)(5 + P.ntke + m) * n;
+        const float qc = q[c] * rinv(rho[c]), qa = q[c - si] * rinv(rho[c - si]);
+        const float qb = q[c - sj] * rinv(rho[c - sj]), qd = q[c - 1] * rinv(rho[c - 1]);
+        float g1 = P.dXi * (qc - qa);
+        float g2 = P.dYi * (qc - qb);
+        float g3 = Q.J31[c] * P.dXi * (qc - qa) + Q.J32[c] * P.dYi * (qc - qb) + Q.J33[c] * P.dZi * (qc - qd);
+        if (k >= P.kMin) {
+          g1 = -rho[c] * Km * invPr * g1;
+          g2 = -rho[c] * Km * invPr * g2;
+          g3 = -rho[c] * Km * invPr * g3;
+        }
+        Q.mtau[(3 * m + 0) * n + c] = g1;
+        Q.mtau[(3 * m + 1) * n + c] = g2;
+        Q.mtau[(3 * m + 2) * n + c] = g3;
+      }
+    }
+  }
+  if (P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin) surface_column(P, Q, st, i, j, stage);
+}
+
+// Write value v of one field at interior cell (i,j,k) and at its periodic images; `bot`
+// also writes the 3 cells below kMin (bottom copy rule), `nbot` how many of them, `top`
+// the 3 cells above kMax-1 (zero-gradient rule).
+__device__ __forceinline__ void store_images(const Phys& P, float* __restrict__ F, int i, int j, int k, float v, int nbot,
+                                             bool top) {
+  int is[3], js[3], ni = 0, nj = 0;
+  is[ni++] = i;
+  if (i < P.iMin + 3) is[ni++] = i + P.Nx;
+  if (i >= P.iMax - 3) is[ni++] = i - P.Nx;
+  js[nj++] = j;
+  if (j < P.jMin + 3) js[nj++] = j + P.Ny;
+  if (j >= P.jMax - 3) js[nj++] = j - P.Ny;
+  for (int a = 0; a < ni; a++)
+    for (int b = 0; b < nj; b++) {
+      const long long cb = (long long)is[a] * P.si + (long long)js[b] * P.sj + k;
+      F[cb] = v;
+      for (int h = 1; h <= nbot; h++) F[cb - h] = v;
+      if (top)
+        for (int h = 1; h <= 3; h++) F[cb + h] = v;
+    }
+}
+
+// ------------------------------------------------------------------ fused stage
+template <int STAGE, int MODE>
+__global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base,
+                                               float* __restrict__ nxt, const float* __restrict__ pcur,
+                                               float* __restrict__ pnxt, float* __restrict__ frhs) {
+  const int k = P.kMin + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = P.jMin + blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = P.iMin + blockIdx.z * blockDim.z + threadIdx.z;
+  if (k >= P.kMax || j >= P.jMax || i >= P.iMax) return;
+  const long long n = P.n;
+  const int si = P.si, sj = P.sj;
+  const long long c = (long long)i * si + (long long)j * sj + k;
+  const float *rho = cur, *mu = cur + n, *mv = cur + 2 * n, *mw = cur + 3 * n, *mth = cur + 4 * n;
+  const float* me = P.ntke ? cur + 5 * n : nullptr;
+  const float* mq0 = P.nmoist > 0 ? cur + (5 + P.ntke) * n : nullptr;
+  const float* mq1 = P.nmoist > 1 ? mq0 + n : nullptr;
+  const bool phys = (P.oneRK == 0) || (STAGE == 2);
+  const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
+  const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
+  float F0 = 0.0f, F1 = 0.0f, F2 = 0.0f, F3 = 0.0f, F4 = 0.0f, Fe = 0.0f, Fq0 = 0.0f, Fq1 = 0.0f;
+
+  // pressure-gradient force (cuda_pressureDevice.cu:118-194)
+  if (P.pgf) {
+    const float dpx = pcur[c + si] - pcur[c - si];
+    const float dpy = pcur[c + sj] - pcur[c - sj];
+    const float dpz = pcur[c + 1] - pcur[c - 1];
+    if (P.nmoist > 0) {
+      float rmd = 1.0f;
+      rmd = (float)((double)rmd + (double)(mq0[c] / rho[c]) * 1e-3);
+      if (P.nmoist > 1) rmd = (float)((double)rmd + (double)(mq1[c] / rho[c]) * 1e-3);
+      const float rdm = 1.0f / rmd;
+      F1 = (float)((double)F1 - (double)rdm * 0.5 * (double)dXi * (double)dpx);
+      F2 = (float)((double)F2 - (double)rdm * 0.5 * (double)dYi * (double)dpy);
+      F3 = (float)((double)F3 - (double)rdm * 0.5 * (double)(dXi * J1 * dpx + dYi * J2 * dpy + dZi * J3 * dpz));
+    } else {
+      F1 = F1 - (0.5f * dXi) * dpx;
+      F2 = F2 - (0.5f * dYi) * dpy;
+      F3 = F3 - 0.5f * (dXi * J1 * dpx + dYi * J2 * dpy + dZi * J3 * dpz);
+    }
+  }
+
+  // face velocities of this cell (cuda_advectionDevice.cu:89-106)
+  FaceVel fv;
+  {
+    const float* D = Q.D;
+    const long long im = c - si, ip = c + si, jm = c - sj, jp = c + sj, km = c - 1, kp = c + 1;
+    const float cxc = contra(D[c], rho[c], mu[c], mw[c], J1);
+    const float cxm = contra(D[im], rho[im], mu[im], mw[im], Q.J31[im]);
+    const float cxp = contra(D[ip], rho[ip], mu[ip], mw[ip], Q.J31[ip]);
+    fv.um = (0.5f * dXi) * (cxc + cxm);
+    fv.up = (0.5f * dXi) * (cxp + cxc);
+    const float cyc = contra(D[c], rho[c], mv[c], mw[c], J2);
+    const float cym = contra(D[jm], rho[jm], mv[jm], mw[jm], Q.J32[jm]);
+    const float cyp = contra(D[jp], rho[jp], mv[jp], mw[jp], Q.J32[jp]);
+    fv.vm = (0.5f * dYi) * (cyc + cym);
+    fv.vp = (0.5f * dYi) * (cyp + cyc);
+    const float czc = (D[c] / rho[c]) * (mw[c] * J3);
+    const float czm = (D[km] / rho[km]) * (mw[km] * Q.J33[km]);
+    const float czp = (D[kp] / rho[kp]) * (mw[kp] * Q.J33[kp]);
+    fv.wm = (k == P.kMin) ? 0.0f : (0.5f * dZi) * (czc + czm);
+    fv.wp = (k + 1 >= P.kMax) ? 0.0f : (0.5f * dZi) * (czp + czc);
+  }
+  const float invD = Q.invD[c];
+
+  auto adv56 = [&](const float* __restrict__ s, float b) -> float {
+    const float bf = 1.0f - b;
+    float fxp, fxm, fyp, fym, fzp, fzm;
+    {
+      const float m3 = s[c - 3 * si], m2 = s[c - 2 * si], m1 = s[c - si], z0 = s[c], p1 = s[c + si], p2 = s[c + 2 * si],
+                  p3 = s[c + 3 * si];
+      fxp = hyb56_flux(m2, m1, z0, p1, p2, p3, fv.up, bf);
+      fxm = hyb56_flux(m3, m2, m1, z0, p1, p2, fv.um, bf);
+    }
+    {
+      const float m3 = s[c - 3 * sj], m2 = s[c - 2 * sj], m1 = s[c - sj], z0 = s[c], p1 = s[c + sj], p2 = s[c + 2 * sj],
+                  p3 = s[c + 3 * sj];
+      fyp = hyb56_flux(m2, m1, z0, p1, p2, p3, fv.vp, bf);
+      fym = hyb56_flux(m3, m2, m1, z0, p1, p2, fv.vm, bf);
+    }
+    {
+      const float m3 = s[c - 3], m2 = s[c - 2], m1 = s[c - 1], z0 = s[c], p1 = s[c + 1], p2 = s[c + 2], p3 = s[c + 3];
+      fzp = hyb56_flux(m2, m1, z0, p1, p2, p3, fv.wp, bf);
+      fzm = hyb56_flux(m3, m2, m1, z0, p1, p2, fv.wm, bf);
+    }
+    const float Dx = fv.up * fxp - fv.um * fxm;
+    const float Dy = fv.vp * fyp - fv.vm * fym;
+    const float Dz = fv.wp * fzp - fv.wm * fzm;
+    return invD * (Dx + Dy + Dz);
+  };
+  // WENO5 applies x, y, z as three separate updates (cuda_hydroCoreDevice.cu:646-648)
+  auto advW5 = [&](float Facc, const float* __restrict__ s) -> float {
+    {
+      const float m3 = s[c - 3 * si], m2 = s[c - 2 * si], m1 = s[c - si], z0 = s[c], p1 = s[c + si], p2 = s[c + 2 * si],
+                  p3 = s[c + 3 * si];
+      const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, fv.up);
+      const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, fv.um);
+      Facc = Facc - invD * (fv.up * fp - fv.um * fm);
+    }
+    {
+      const float m3 = s[c - 3 * sj], m2 = s[c - 2 * sj], m1 = s[c - sj], z0 = s[c], p1 = s[c + sj], p2 = s[c + 2 * sj],
+                  p3 = s[c + 3 * sj];
+      const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, fv.vp);
+      const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, fv.vm);
+      Facc = Facc - invD * (fv.vp * fp - fv.vm * fm);
+    }
+    {
+      const float m3 = s[c - 3], m2 = s[c - 2], m1 = s[c - 1], z0 = s[c], p1 = s[c + 1], p2 = s[c + 2], p3 = s[c + 3];
+      const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, fv.wp);
+      const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, fv.wm);
+      Facc = Facc - invD * (fv.wp * fp - fv.wm * fm);
+    }
+    return Facc;
+  };
+  auto advect = [&](float Facc, const float* __restrict__ s, int sel, float b) -> float {
+    if (sel == 3) return Facc - adv56(s, b);
+    if (sel == 5) return advW5(Facc, s);
+    return Facc;
+  };
+
+  // advection of the hydro fields, Rayleigh damping and buoyancy on w (cuda_hydroCoreDevice.cu:631-672)
+  F0 = advect(F0, rho, P.advSel, P.bHyb);
+  F1 = advect(F1, mu, P.advSel, P.bHyb);
+  F2 = advect(F2, mv, P.advSel, P.bHyb);
+  F3 = advect(F3, mw, P.advSel, P.bHyb);
+  if (P.damp) {
+    const long long ctop = c - k + (P.kMax - 1);
+    const float z = Q.zPos[c], zt = Q.zPos[ctop];
+    if (z >= (zt - P.dampDepth)) {
+      const float wbs = momentum_bs(P, 3, z, Q.rhoBS[c]);
+      const float pio2 = 1.5707963267948966f;
+      const double s = (double)sinf((float)((double)pio2 * (1.0 - (double)((zt - z) / P.dampDepth))));
+      F3 = (float)((double)F3 - 0.2 * (double)rho[c] * (s * s) * (double)(mw[c] / rho[c] - wbs / Q.rhoBS[c]));
+    }
+  }
+  if (P.buoy) {
+    const float r = rho[c], rbs = Q.rhoBS[c];
+    if (P.nmoist == 1) {
+      const double rm = (double)r + (double)mq0[c] * 1e-3;
+      F3 = (float)((double)F3 - ((double)r / rm) * (double)P.g * (rm - (double)rbs));
+    } else if (P.nmoist == 2) {
+      const double rm = (double)r + (double)mq0[c] * 1e-3 + (double)mq1[c] * 1e-3;
+      F3 = (float)((double)F3 - ((double)r / rm) * (double)P.g * (rm - (double)rbs));
+    } else {
+      F3 = F3 - P.g * (r - rbs);
+    }
+  }
+  F4 = advect(F4, mth, P.advSel, P.bHyb);
+  if (P.ntke) Fe = advect(Fe, me, P.tkeAdvSel, P.tkeBHyb);
+  if (P.nmoist > 0) Fq0 = advect(Fq0, mq0, P.qvAdvSel, P.qvB);
+  if (P.nmoist > 1 && P.qiAdvSel == 2) Fq1 = advW5(Fq1, mq1);
+
+  // Coriolis (cuda_coriolisDevice.cu:50-58)
+  if (P.cor) {
+    const float z = Q.zPos[c], rbs = Q.rhoBS[c], r = rho[c];
+    const float ubs = momentum_bs(P, 1, z, rbs), vbs = momentum_bs(P, 2, z, rbs), wbs = momentum_bs(P, 3, z, rbs);
+    F1 = F1 + (P.fHorz * (mv[c] / r - P.fLS * vbs / rbs) - P.fVert * (mw[c] / r - P.fLS * wbs / rbs));
+    F2 = F2 - (P.fHorz * (mu[c] / r - P.fLS * ubs / rbs));
+    F3 = F3 + (P.fVert * (mu[c] / r - P.fLS * ubs / rbs));
+  }
+
+  if (phys && P.turb) {
+    // divergence of the SGS stresses (cuda_sgsTurbDevice.cu:447-547)
+    const float* T = Q.tau;
+    const long long ip = c + si, jp = c + sj, kp = c + 1;
+#define TT(m, x) T[(m) * n + (x)]
+    F1 = F1 - (dXi * (TT(0, ip) - TT(0, c)) + dYi * (TT(1, jp) - TT(1, c)) + J1 * dXi * (TT(2, ip) - TT(2, c)) +
+               J2 * dYi * (TT(2, jp) - TT(2, c)) + J3 * dZi * (TT(2, kp) - TT(2, c)));
+    F2 = F2 - (dXi * (TT(1, ip) - TT(1, c)) + dYi * (TT(4, jp) - TT(4, c)) + J1 * dXi * (TT(3, ip) - TT(3, c)) +
+               J2 * dYi * (TT(3, jp) - TT(3, c)) + J3 * dZi * (TT(3, kp) - TT(3, c)));
+    F3 = F3 - (dXi * (TT(2, ip) - TT(2, c)) + dYi * (TT(3, jp) - TT(3, c)) + J1 * dXi * (TT(5, ip) - TT(5, c)) +
+               J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c)));
+    F4 = F4 - (dXi * (TT(6, ip) - TT(6, c)) + dYi * (TT(7, jp) - TT(7, c)) + J1 * dXi * (TT(8, ip) - TT(8, c)) +
+               J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c)));
+    if (P.nmoist > 0 && P.moistSGS > 0) {
+      const float* M = Q.mtau;
+      Fq0 = Fq0 - (dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) +
+                   J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) + J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) +
+                   J3 * dZi * (M[2 * n + kp] - M[2 * n + c]));
+      if (P.nmoist > 1) {
+        const float* M1 = M + 3 * n;
+        Fq1 = Fq1 - (dXi * (M1[ip] - M1[c]) + dYi * (M1[n + jp] - M1[n + c]) + J1 * dXi * (M1[2 * n + ip] - M1[2 * n + c]) +
+                     J2 * dYi * (M1[2 * n + jp] - M1[2 * n + c]) + J3 * dZi * (M1[2 * n + kp] - M1[2 * n + c]));
+      }
+    }
+    // SGS TKE budget (cuda_sgstkeDevice.cu:155-397)
+    if (P.tke) {
+      const float ri = rinv(rho[c]);
+      const float delta = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
+      const float lsc = Q.ls[c];
+      Fe = Fe + P.g / (mth[c] * ri) * TT(8, c);
+      const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
+      const float ec = me[c] * ri;
+      Fe = Fe + (-ce * me[c] * powf(ec, 0.5f) / lsc);
+      const long long im = c - si, jm = c - sj, km = c - 1;
+#define G_(q, x) (q[x] * rinv(rho[x]))
+      const float dux = 0.5f * (dXi * (G_(mu, ip) - G_(mu, im)));
+      const float duy = 0.5f * (dYi * (G_(mu, jp) - G_(mu, jm)));
+      const float duz = 0.5f * (J1 * dXi * (G_(mu, ip) - G_(mu, im)) + J2 * dYi * (G_(mu, jp) - G_(mu, jm)) +
+                                J3 * dZi * (G_(mu, kp) - G_(mu, km)));
+      const float dvx = 0.5f * (dXi * (G_(mv, ip) - G_(mv, im)));
+      const float dvy = 0.5f * (dYi * (G_(mv, jp) - G_(mv, jm)));
+      const float dvz = 0.5f * (J1 * dXi * (G_(mv, ip) - G_(mv, im)) + J2 * dYi * (G_(mv, jp) - G_(mv, jm)) +
+                                J3 * dZi * (G_(mv, kp) - G_(mv, km)));
+      const float dwx = 0.5f * (dXi * (G_(mw, ip) - G_(mw, im)));
+      const float dwy = 0.5f * (dYi * (G_(mw, jp) - G_(mw, jm)));
+      const float dwz = 0.5f * (J1 * dXi * (G_(mw, ip) - G_(mw, im)) + J2 * dYi * (G_(mw, jp) - G_(mw, jm)) +
+                                J3 * dZi * (G_(mw, kp) - G_(mw, km)));
+#undef G_
+      const float shear = (-TT(0, c) * dux) + (-TT(1, c) * duy) + (-TT(2, c) * duz) + (-TT(1, c) * dvx) +
+                          (-TT(4, c) * dvy) + (-TT(3, c) * dvz) + (-TT(2, c) * dwx) + (-TT(3, c) * dwy) + (-TT(5, c) * dwz);
+      Fe = Fe + shear;
+      const float* G = Q.tkeQ;
+      const float tx = -(dXi * (G[ip] - G[im]));
+      const float ty = -(dYi * (G[n + jp] - G[n + jm]));
+      const float tz = -(J1 * dXi * (G[2 * n + ip] - G[2 * n + im]) + J2 * dYi * (G[2 * n + jp] - G[2 * n + jm]) +
+                         J3 * dZi * (G[2 * n + kp] - G[2 * n + km]));
+      Fe = Fe + (-(tx + ty + tz));
+    }
+#undef TT
+  }
+
+  // saturation adjustment (cuda_moistureDevice.cu:80-247)
+  if (phys && P.nmoist > 1 && P.moist && P.moistCond > 0) {
+    if ((*Q.clockIt) % P.mpFreq == 0) {
+      const float ri = rinv(rho[c]);
+      const float thd = mth[c] * ri;
+      const float prd = P.condBasePres == 1 ? powf(Q.thBS[c] * P.c1, P.cp_cv) : powf(mth[c] * P.c1, P.cp_cv);
+      const float Td = thd * powf(prd / P.p0, P.R_cp);
+      float pvs;
+      const float Tc = fmaxf(-80.0f, (Td - 273.16f));
+      if (Td >= 273.15f) {
+        pvs = (6.11239921f + Tc * (0.443987641f + Tc * (0.142986287e-1f + Tc * (0.264847430e-3f + Tc * (0.302950461e-5f +
+              Tc * (0.206739458e-7f + Tc * (0.640689451e-10f + Tc * (-0.952447341e-13f + -0.976195544e-15f * Tc)))))))) * 100.0f;
+      } else {
+        pvs = (6.11147274f + Tc * (0.503160820f + Tc * (0.188439774e-1f + Tc * (0.420895665e-3f + Tc * (0.615021634e-5f +
+              Tc * (0.602588177e-7f + Tc * (0.385852041e-9f + Tc * (0.146898966e-11f + 0.252751365e-14f * Tc)))))))) * 100.0f;
+      }
+      pvs = fminf((0.99f * prd), pvs);
+      float ffor = 0.0f;
+      const float flim = mq1[c] * 1e-3f;
+      if (P.moistCond == 1) {
+        ffor = mq0[c] * 1e-3f - (pvs / (P.R_vapor * Td));
+      } else if (P.moistCond == 2) {
+        const float rv = mq0[c] * 1e-3f, rvs = pvs / (P.R_vapor * Td);
+        ffor = (rv - rvs) / (1.0f + (powf(P.L_v, 2.0f) * rvs * ri / (P.cp_gas * P.R_vapor * powf(Td, 2.0f))));
+      } else {
+        const float rv = mq0[c] * 1e-3f;
+        float rvs = pvs / (prd - pvs) / P.Rv_Rg;
+        rvs = rvs / ri;
+        ffor = (rv - rvs) / (1.0f + (powf(P.L_v, 2.0f) * rvs * ri / (P.cp_gas * P.R_vapor * powf(Td, 2.0f))));
+      }
+      float fc = fmaxf(ffor, 0.0f) - fmaxf(fminf(flim, -ffor), 0.0f);
+      fc = fc / P.condTscale;
+      Fq0 = Fq0 - fc * 1e3f;
+      Fq1 = Fq1 + fc * 1e3f;
+      const float prd2 = powf(mth[c] * P.c1, P.cp_cv);
+      const float Td2 = thd * powf(prd2 / P.p0, P.R_cp);
+      F4 = F4 + ((thd * P.L_v) / (Td2 * P.cp_gas)) * fc;
+    }
+  }
+
+  if (MODE == MODE_FRHS) {
+    frhs[c] = F0;
+    frhs[n + c] = F1;
+    frhs[2 * n + c] = F2;
+    frhs[3 * n + c] = F3;
+    frhs[4 * n + c] = F4;
+    if (P.ntke) frhs[5 * n + c] = Fe;
+    if (P.nmoist > 0) frhs[(5 + P.ntke) * n + c] = Fq0;
+    if (P.nmoist > 1) frhs[(6 + P.ntke) * n + c] = Fq1;
+    return;
+  }
+
+  // WS2002 RK3 commit (cuda_RKschemes.cu:113-157) with the reference's rounding:
+  // stages 1-2 in double ((1/3)dt, 0.5 dt literals), stage 3 in float.
+  auto rk = [&](float phi0, float F) -> float {
+    if (STAGE == 0) return (float)fma((1.0 / 3.0) * (double)P.dt, (double)F, (double)phi0);
+    if (STAGE == 1) return (float)fma(0.5 * (double)P.dt, (double)F, (double)phi0);
+    return __fmaf_rn(P.dt, F, phi0);
+  };
+  const float* b0 = base;
+  const float n0 = rk(b0[c], F0);
+  const float n1 = rk(b0[n + c], F1);
+  const float n2 = rk(b0[2 * n + c], F2);
+  const float n3 = rk(b0[3 * n + c], F3);
+  const float n4 = rk(b0[4 * n + c], F4);
+  const bool atBot = (k == P.kMin), atTop = (k == P.kMax - 1);
+  store_images(P, nxt, i, j, k, n0, 0, false);
+  store_images(P, nxt + n, i, j, k, n1, atBot ? 3 : 0, false);
+  store_images(P, nxt + 2 * n, i, j, k, n2, atBot ? 3 : 0, false);
+  store_images(P, nxt + 3 * n, i, j, k, n3, atBot ? 3 : 0, false);
+  store_images(P, nxt + 4 * n, i, j, k, n4, 0, false);
+  float nq0 = 0.0f;
+  if (P.ntke) {
+    const float ne = fmaxf(rk(b0[5 * n + c], Fe), 1e-10f);
+    store_images(P, nxt + 5 * n, i, j, k, ne, atBot ? 3 : 0, false);
+  }
+  if (P.nmoist > 0) {
+    const long long o = (5 + P.ntke) * n;
+    nq0 = fmaxf(rk(b0[o + c], Fq0), 0.0f);
+    store_images(P, nxt + o, i, j, k, nq0, atBot ? 3 : 0, atTop);
+    if (P.nmoist > 1) {
+      const float nq1 = fmaxf(rk(b0[o + n + c], Fq1), 0.0f);
+      store_images(P, nxt + o + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
+    }
+  }
+  // perturbation pressure of the new state (levels 1..kMin-1 and kMax.. copy this cell)
+  float pn;
+  {
+    float rtm = n4;
+    if (P.nmoist > 0) rtm = (float)((double)n4 * (1.0 + (double)(P.Rv_Rg * nq0 / n0) * 1e-3));
+    pn = powf(rtm * P.c1, P.cp_cv) - Q.pBS[c];
+  }
+  store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
+}
+
+__global__ void k_clock(Ptrs Q, float dt) {
+  *Q.clockIt = *Q.clockIt + 1;
+  *Q.clockTime = *Q.clockTime + dt;
+}
+
+__global__ void k_nonfinite(Phys P, const float* __restrict__ st, unsigned long long* out) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned int cnt = 0;
+  if (t < P.n) {
+    const int k = (int)(t % P.nzh);
+    const int j = (int)((t / P.nzh) % P.nyh);
+    const int i = (int)(t / ((long long)P.nzh * P.nyh));
+    if (i >= P.iMin && i < P.iMax && j >= P.jMin && j < P.jMax && k >= P.kMin && k < P.kMax)
+      for (int f = 0; f < P.nf; f++) cnt += isfinite(st[(long long)f * P.n + t]) ? 0u : 1u;
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, (unsigned long long)cnt);
+}
+
+// FP64 sums of the interior fields: warp shuffle, then one atomic per warp and field.
+__global__ void k_means(Phys P, const float* __restrict__ st, double* out) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool in = false;
+  if (t < P.n) {
+    const int k = (int)(t % P.nzh);
+    const int j = (int)((t / P.nzh) % P.nyh);
+    const int i = (int)(t / ((long long)P.nzh * P.nyh));
+    in = i >= P.iMin && i < P.iMax && j >= P.jMin && j < P.jMax && k >= P.kMin && k < P.kMax;
+  }
+  for (int f = 0; f < P.nf; f++) {
+    double v = in ? (double)st[(long long)f * P.n + t] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&out[f], v);
+  }
+}
+
+}  // namespace fe

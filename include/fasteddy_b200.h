@@ -1,0 +1,194 @@
+/* fasteddy_b200.h -- C ABI of the B200-native FastEddy hot path.
+ *
+ * Two layers, both plain C (no C++ or torch types, plain pointers and sizes):
+ *
+ * 1. The reference-named drop-in entry points (section A). They have exactly the
+ *    signatures the FastEddy driver binds (reference SRC/FEMAIN/FastEddy.c:123,256,
+ *    263-280,379,451-461) and read their inputs from the same global host symbols the
+ *    reference CUDA layer reads (grid extents, metric arrays, prognostic arrays,
+ *    physics selectors; see fe_refglobals.h). They return 0 on success and a nonzero
+ *    FE_ERR_* code on failure; unlike the reference (fecuda_Device_cu.h:26-35) they
+ *    never call exit().
+ *
+ * 2. The engine API (section B): an explicit domain handle, used by the entry points
+ *    above, by the ensemble launcher and directly by tests and benchmarks.
+ *
+ * Field layout everywhere at this boundary is the reference's: a field of a domain
+ * with interior extents Nx,Ny,Nz and halo width Nh=3 is a float array of
+ * (Nx+6)*(Ny+6)*(Nz+6) values indexed ijk = i*(Ny+6)*(Nz+6) + j*(Nz+6) + k
+ * (k fastest, the iStride/jStride of every reference device routine), multi-field blocks
+ * concatenate fields with that stride, momentum/scalars in flux form (rho*phi).
+ */
+#ifndef FASTEDDY_B200_H
+#define FASTEDDY_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- error codes */
+#define FE_OK               0
+#define FE_ERR_CUDA         1   /* a CUDA runtime call failed (message via fe_last_error) */
+#define FE_ERR_CONFIG       2   /* unsupported or inconsistent configuration */
+#define FE_ERR_ARG          3   /* NULL handle/pointer or bad size */
+#define FE_ERR_STATE        4   /* call out of order (e.g. advance before set_state) */
+#define FE_ERR_NOMEM        5   /* device allocation failed */
+#define FE_ERR_NONFINITE    6   /* the state contains NaN/Inf after a batch */
+#define FE_ERR_NO_DEVICE    7   /* no CUDA device visible */
+
+/* ======================================================= A. reference-named ABI */
+/* Each entry replaces the same-named function of the reference CUDA layer. */
+
+/* replaces SRC/FECUDA/fecuda.h:35 fecuda_Init(): selects device (rank % numDevices). */
+int fecuda_Init(void);
+/* replaces SRC/FECUDA/fecuda.h:45 fecuda_SetBlocksPerGrid(): halo-inclusive extents;
+ * accepted for interface compatibility (launch geometry is chosen by the engine). */
+int fecuda_SetBlocksPerGrid(int Nx, int Ny, int Nz);
+/* replaces SRC/FECUDA/fecuda.h:55 / :60: single-GPU domains need no halo buffers. */
+int fecuda_AllocateHaloBuffers(int Nxp, int Nyp, int Nzp, int Nh);
+int fecuda_DeallocateHaloBuffers(void);
+/* replaces SRC/FECUDA/fecuda.h:40 fecuda_Cleanup(). */
+int fecuda_Cleanup(void);
+/* replaces SRC/GRID/CUDA/cuda_grid.h:30 cuda_gridInit(): uploads zPos and metrics. */
+int cuda_gridInit(void);
+/* replaces SRC/GRID/CUDA/cuda_grid.h:35 cuda_gridCleanup(). */
+int cuda_gridCleanup(void);
+/* replaces SRC/HYDRO_CORE/CUDA/cuda_hydroCore.h:30 cuda_hydroCoreInit(): creates the
+ * device domain from the physics globals and uploads the base state. */
+int cuda_hydroCoreInit(void);
+/* replaces SRC/HYDRO_CORE/CUDA/cuda_hydroCore.h:35 cuda_hydroCoreCleanup(). */
+int cuda_hydroCoreCleanup(void);
+/* replaces SRC/TIME_INTEGRATION/CUDA/cuda_timeInt.h:30 cuda_timeIntInit(): uploads the
+ * prognostic state and surface arrays. */
+int cuda_timeIntInit(void);
+/* replaces SRC/TIME_INTEGRATION/CUDA/cuda_timeInt.h:35 cuda_timeIntCleanup(). */
+int cuda_timeIntCleanup(void);
+/* replaces SRC/TIME_INTEGRATION/CUDA/cuda_timeInt.h:40 cuda_timeIntCommence(it):
+ * advances NtBatch RK3 steps (re-uploading the host state when it==simTime_itRestart),
+ * then copies state, perturbation pressure and surface arrays back to the host
+ * globals and advances simTime / simTime_it, as cuda_timeIntDevice.cu:105-157. */
+int cuda_timeIntCommence(int it);
+/* replaces SRC/HYDRO_CORE/CUDA/cuda_hydroCoreDevice_cu.h:97 (device-level twin):
+ * evaluates the tendency of RK stage `timeStage` (0..2) from the device state into
+ * the device Frhs buffers without committing; read it back with fe_get_frhs(). */
+int cuda_hydroCoreDeviceBuildFrhs(float simTime, int simTime_it, int simTime_itRestart,
+                                  float dt, int timeStage, int numRKstages);
+/* replaces SRC/TIME_INTEGRATION/CUDA/cuda_timeIntDevice_cu.h:57/:62 twins. */
+int cuda_timeIntHydroInitDevice(void);
+int cuda_timeIntHydroSynchFromDevice(void);
+
+/* ===================================================================== B. engine */
+typedef struct fe_domain fe_domain;
+typedef struct fe_ensemble fe_ensemble;
+
+/* Physics configuration of one domain. Names and meanings follow the reference's
+ * parameter keys (SRC/HYDRO_CORE/hydro_core.c:197-395, SRC/GRID/grid.c:68-88,
+ * SRC/TIME_INTEGRATION/time_integration.c:51-64); derived constants follow
+ * hydro_core.c:941-967. Fill with fe_config_defaults() then override. */
+typedef struct fe_config {
+  int Nx, Ny, Nz, Nh;                 /* interior extents per rank, halo width (3) */
+  float dX, dY, dZ;                   /* d_xi, d_eta, d_zeta */
+  float dt;
+  int simTime_itRestart;
+  int hydroBCs;                       /* only 2 (periodic horizontal, ABL vertical) */
+  int pgfSelector, buoyancySelector, coriolisSelector;
+  int turbulenceSelector, TKESelector, TKEAdvSelector;
+  float TKEAdvSelector_b_hyb, c_s, c_k;
+  int advectionSelector;              /* 3 = HYB56, 5 = WENO5 */
+  float b_hyb;
+  int diffusionSelector, filterSelector, lsfSelector;   /* must be 0 */
+  int surflayerSelector;              /* 0, 1 (heat flux) or 2 (skin temperature) */
+  float surflayer_z0, surflayer_z0t, surflayer_wth, surflayer_tr, surflayer_wq, surflayer_qr;
+  int surflayer_qskin_input, surflayer_stab, surflayer_idealsine;
+  float surflayer_ideal_ts, surflayer_ideal_te, surflayer_ideal_amp;
+  float surflayer_ideal_qts, surflayer_ideal_qte, surflayer_ideal_qamp;
+  int moistureSelector, moistureNvars, moistureAdvSelectorQv;
+  float moistureAdvSelectorQv_b;
+  int moistureAdvSelectorQi, moistureSGSturb, moistureCond;
+  float moistureCondTscale;
+  int moistureCondBasePres;
+  float moistureMPcallTscale;
+  int dampingLayerSelector;
+  float dampingLayerDepth;
+  float U_g, V_g, z_Ug, z_Vg, Ug_grad, Vg_grad;
+  float corioConstHorz, corioConstVert, corioLS_fact;
+  int physics_oneRKonly;
+  float temp_grnd, pres_grnd;
+  float R_gas, R_vapor, Rv_Rg, cp_gas, cv_gas, accel_g, R_cp, cp_R, cp_cv, refPressure, kappa, L_v;
+} fe_config;
+
+/* Reference defaults (hydro_core.c:197-395 defaults, hydro_core.c:941-952 constants). */
+void fe_config_defaults(fe_config *cfg);
+/* Recompute the derived constants (cp, ratios, Coriolis factors from latitude). */
+void fe_config_derive(fe_config *cfg, float coriolisLatitude);
+
+int fe_device_count(void);
+/* Create a domain on `device`; checks the configuration and allocates device memory. */
+int fe_create(const fe_config *cfg, int device, fe_domain **out);
+int fe_destroy(fe_domain *d);
+/* Bytes of device memory held by the domain. */
+size_t fe_device_bytes(const fe_domain *d);
+
+/* Grid inputs, reference layout, halo-inclusive, one field each. */
+int fe_set_grid(fe_domain *d, const float *zPos, const float *J31, const float *J32,
+                const float *J33, const float *D_Jac, const float *invD_Jac);
+/* Base state: rho_BS and (rho*theta)_BS, two concatenated fields (hydroBaseStateFlds). */
+int fe_set_base_state(fe_domain *d, const float *baseStateFlds);
+/* Prognostic state: hydroFlds (5 fields), sgstke (TKESelector fields or NULL),
+ * moist (moistureNvars fields or NULL). Halos are filled on the device. */
+int fe_set_state(fe_domain *d, const float *hydroFlds, const float *sgstke, const float *moist);
+/* Surface 2-D arrays ((Nx+6)*(Ny+6) each, any may be NULL when unused). */
+int fe_set_surface(fe_domain *d, const float *z0m, const float *z0t, const float *htFlux,
+                   const float *tskin, const float *fricVel, const float *qFlux, const float *qskin);
+/* Simulation clock (simTime, simTime_it) the next step starts from. */
+int fe_set_clock(fe_domain *d, float simTime, int simTime_it);
+int fe_get_clock(const fe_domain *d, float *simTime, int *simTime_it);
+
+/* Advance `nsteps` RK3 steps on the domain's stream (asynchronous; see fe_sync). */
+int fe_advance(fe_domain *d, int nsteps);
+/* Block until queued work of the domain finished; reports device errors. */
+int fe_sync(fe_domain *d);
+/* CUDA stream (cudaStream_t) the domain launches on, for event timing. */
+void *fe_stream(fe_domain *d);
+
+int fe_get_state(fe_domain *d, float *hydroFlds, float *sgstke, float *moist, float *pres);
+int fe_get_surface(fe_domain *d, float *cd, float *ch, float *fricVel, float *htFlux,
+                   float *invOblen, float *tskin, float *qFlux, float *qskin);
+
+/* Tendency of RK stage `stage` (0..2) from the current state, no commit. */
+int fe_build_frhs(fe_domain *d, int stage);
+/* Copy the tendencies of the last fe_build_frhs (same field blocks as fe_get_state)
+ * and, if taus != NULL, the 9 SGS stress/flux fields (order of hydroTauFlds). */
+int fe_get_frhs(fe_domain *d, float *hydroFrhs, float *sgstkeFrhs, float *moistFrhs, float *taus);
+
+/* Count NaN/Inf values in the interior prognostic state (device reduction). */
+int fe_count_nonfinite(fe_domain *d, long long *count);
+/* FP64 domain means of the interior prognostic fields (device reduction with FP64
+ * accumulation); means has room for 5 + TKESelector + moistureNvars values. */
+int fe_domain_means(fe_domain *d, double *means);
+
+/* Launch-shape control: threads per block along k and j of the stencil kernels and
+ * the number of i-planes each thread block marches (0 = engine default). */
+int fe_set_tiling(fe_domain *d, int tk, int tj, int ti);
+/* Pick the tiling by timing the candidates (the autotuner); writes the choice. */
+int fe_autotune(fe_domain *d, int *tk, int *tj, int *ti);
+/* Number of engine kernel launches enqueued since creation (for bookkeeping). */
+long long fe_launch_count(const fe_domain *d);
+
+/* Ensembles: advance several domains (different sizes allowed, same device) with one
+ * captured CUDA graph per step batch. */
+int fe_ensemble_create(fe_domain **members, int n, fe_ensemble **out);
+int fe_ensemble_advance(fe_ensemble *e, int nsteps);
+int fe_ensemble_sync(fe_ensemble *e);
+void *fe_ensemble_stream(fe_ensemble *e);
+int fe_ensemble_destroy(fe_ensemble *e);
+
+/* Text of the last error of the calling thread. */
+const char *fe_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

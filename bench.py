@@ -1,0 +1,358 @@
+"""Benchmark of the FastEddy hot path on B200: RK3 cell-updates/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--case NAME]
+
+Workload (default): the moist convective boundary layer over a Gaussian hill,
+512 x 512 x 128 cells, dx = dy = 20 m, dz = 10 m, terrain-following grid, prognostic
+q_v and q_l with saturation adjustment, 1.5-order TKE, surface layer, Rayleigh damping.
+Inputs are synthetic (seeded theta perturbations, analytic hill and q_v profile).
+
+Our arm: a step is one RK3 step (3 fused stage kernels + the last-stage physics kernel)
+replayed from a CUDA graph on the resident device state (8 fields, 1.15 GB, far larger
+than the 126 MB L2, so no flush is needed between steps). `e2e` is the same metric
+through the drop-in C ABI (cuda_timeIntCommence) with host buffers: upload of the host
+state, K steps, copy-back of state, pressure and surface arrays inside the timed region.
+
+Reference arm: the reference's own implementation of this path is CUDA-only; its code,
+compiled for sm_100a from the reference sources (oracle/_ref), runs the same case
+through its own cuda_timeIntCommence and is timed the same way.
+
+Multi-GPU: the path does not shard (single-domain model, no halo exchange), so N GPUs run
+N independent replicas; value is the whole-job rate, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CASES = {
+    # name: (case key, Nx, Ny, Nz, hill, prognostic fields, description)
+    "moist_hill_512": ("cbl_moist_hill", 512, 512, 128, True, 8,
+                       "moist CBL over a Gaussian hill, 512x512x128, dx=dy=20 m, dz=10 m"),
+    "moist_hill_256": ("cbl_moist_hill", 256, 256, 128, True, 8,
+                       "moist CBL over a Gaussian hill, 256x256x128, dx=dy=20 m, dz=10 m"),
+    "dry_cbl_128": ("cbl_dry", 128, 128, 64, False, 6, "dry CBL, flat, 128x128x64, dx=dy=20 m, dz=10 m"),
+    "dry_hill_1024": ("cbl_hill_dry", 1024, 1024, 256, True, 6,
+                      "dry CBL over a Gaussian hill, 1024x1024x256, dx=dy=20 m, dz=10 m"),
+}
+DEFAULT_CASE = "moist_hill_512"
+
+
+def bytes_per_cell_stage(nprog: int, terrain: bool) -> int:
+    """Algorithmic HBM bytes per cell per RK stage: read phi, read phi0, write phi
+    (3 N_p floats) plus 6 read-only metric/base-state fields on terrain."""
+    return 4 * (3 * nprog + (6 if terrain else 0))
+
+
+# ---------------------------------------------------------------- distributed helpers
+def dist_env() -> tuple[int, int, int]:
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def max_over_ranks(value: float, device: str = "cpu") -> float:
+    """Max of a per-rank float over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(device: str = "cpu") -> None:
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+def whole_job_rate(cells_per_rank: int, steps: int, max_seconds: float, world: int) -> float:
+    """Cell-updates/s of the whole job: every rank advances its own replica."""
+    return cells_per_rank * steps * world / max_seconds
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.lines: list[str] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self) -> None:
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc) -> None:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- roofline helpers
+def measured_peak_gbs() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(case: str) -> float | None:
+    """DRAM bytes per launch of the stage kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"k_stage_{case}.txt")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(fe, case_key: str, seconds_target: float = 8.0) -> dict:
+    """The FP64 C restatement of the path (oracle), single thread, on a sample of the
+    workload: the same case on a horizontal subdomain with the full column."""
+    from oracle.pyoracle import Oracle
+
+    c = CASES[case_key]
+    nz = c[3]
+    n = 32
+    host = fe.cases.setup_host(c[0], n, n, nz)
+    o = Oracle(host.config())
+    o.set_inputs(host.inputs())
+    t0 = time.perf_counter()
+    o.step(1)
+    t1 = time.perf_counter()
+    one = t1 - t0
+    steps = max(1, int(seconds_target / max(one, 1e-3)) - 1)
+    o.step(steps)
+    t2 = time.perf_counter()
+    o.close()
+    host.cleanup()
+    total_steps = steps + 1
+    rate = n * n * nz * total_steps / (t2 - t0)
+    return {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{total_steps} RK3 steps of the same case on a {n}x{n}x{nz} subdomain, "
+                      f"serial FP64 C restatement ({t2 - t0:.1f} s)"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank: int, world: int, local: int) -> dict | None:
+    import torch
+
+    fe = importlib.import_module("fasteddy-model_b200")
+    key, nx, ny, nz, terrain, nprog, desc = CASES[args.case]
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    host = fe.cases.setup_host(key, nx, ny, nz, seed=12345 + rank)
+    inp = host.inputs()
+    cfg = host.config()
+    dom = fe.Domain(cfg, device=local)
+    dom.set_inputs(inp)
+    if args.autotune:
+        dom.autotune()
+    cells = nx * ny * nz
+    dom.advance(args.warmup)
+    stream = torch.cuda.ExternalStream(dom.stream(), device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = dom.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        dom.advance(args.steps, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    launches = dom.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    max_ms = max_over_ranks(ms, device)
+    value = whole_job_rate(cells, args.steps, max_ms / 1e3, world)
+    # dominant kernel: the fused dynamics stage, timed alone with CUDA events
+    stage_ms = dom.time_stage_kernel(reps=10)
+    bpc = bytes_per_cell_stage(nprog, terrain)
+    achieved = bpc * cells / (stage_ms * 1e-3) / 1e9
+    peak, peak_src = measured_peak_gbs()
+    traffic = profiled_traffic(args.case)
+    nonfinite = dom.nonfinite()
+    dom.close()
+    # end to end through the drop-in C ABI with host buffers
+    libs = fe.load()
+    ra = libs["refabi"]
+    host.set_gi("NtBatch", args.steps)
+    for fn in ("fecuda_Init", "cuda_gridInit", "cuda_hydroCoreInit", "cuda_timeIntInit"):
+        rc = getattr(ra, fn)()
+        if rc:
+            raise RuntimeError(f"{fn} failed ({rc}): {libs['engine'].fe_last_error().decode()}")
+    ra.cuda_timeIntCommence(host.gi("simTime_itRestart"))  # warm-up batch (graph capture)
+    host.set_gi("simTime_it", 0)
+    barrier()
+    t0 = time.perf_counter()
+    rc = ra.cuda_timeIntCommence(host.gi("simTime_itRestart"))  # uploads host state, K steps, copies back
+    t1 = time.perf_counter()
+    barrier()
+    if rc:
+        raise RuntimeError(f"cuda_timeIntCommence failed ({rc})")
+    e2e_s = max_over_ranks(t1 - t0, device)
+    ra.cuda_hydroCoreCleanup()
+    n3 = (nx + 6) * (ny + 6) * (nz + 6)
+    n2 = (nx + 6) * (ny + 6)
+    nm = cfg.moistureNvars if cfg.moistureSelector else 0
+    ntke = 1 if cfg.TKESelector else 0
+    h2d = 4 * (n3 * (5 + ntke + nm) + n2 * (7 if nm else 5))
+    d2h = 4 * (n3 * (5 + ntke + nm + 1) + n2 * (6 if nm else 4))
+    clocks = clk.summary()
+    host.cleanup()
+    if rank != 0:
+        return None
+    line = {
+        "metric": "RK3 cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": desc, "cells": cells, "prognostic_fields": nprog, "dt_s": float(cfg.dt),
+                   "parallelism": f"replicas{world}", "l2": "state 4*8*N bytes >> 126 MB L2, no flush needed"},
+        "e2e": {"value": whole_job_rate(cells, args.steps, e2e_s, world), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+                "path": "cuda_timeIntCommence (drop-in C ABI), host buffers, one batch of K steps"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_stage (fused tendency + RK3 commit)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_src, "bytes_per_cell_stage": bpc, "stage_kernel_ms": stage_ms},
+        "clocks": clocks,
+        "nonfinite_cells": nonfinite,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(fe, args.case)
+    return line
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, rank: int, world: int) -> dict | None:
+    if rank != 0:
+        return None
+    key, nx, ny, nz, terrain, nprog, desc = CASES[args.case]
+    base = {"metric": "RK3 cell-updates/s", "unit": "cell-updates/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "cells": nx * ny * nz, "parallelism": "single process"}}
+    try:
+        from oracle import refrun
+        if not refrun.available():
+            from oracle import build_ref
+            build_ref.build()
+        fe = importlib.import_module("fasteddy-model_b200")
+        host = fe.cases.setup_host(key, nx, ny, nz)
+        inp = host.inputs()
+        text = fe.cases.param_text(key, nx, ny, nz)
+        with ClockSampler(0) as clk:
+            t = refrun.time_steps(text, inp, args.steps)
+        host.cleanup()
+    except Exception as exc:  # the reference cannot run here: report why
+        return {"impl": "reference", "unavailable": f"{type(exc).__name__}: {str(exc).splitlines()[0][:200]}"}
+    ms = t["ms_per_step"]
+    value = nx * ny * nz / (ms * 1e-3)
+    base.update({
+        "value": value, "ms_per_step": ms,
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
+                         "sample": f"reference CUDA build (oracle/_ref, sm_100a) on the B200 through its own "
+                                   f"cuda_timeIntCommence: ({2 * args.steps}-step batch - {args.steps}-step batch)/"
+                                   f"{args.steps}; the reference has no CPU implementation of this path"},
+        "clocks": clk.summary(),
+        "reference_timing": t,
+    })
+    return base
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--case", choices=sorted(CASES), default=DEFAULT_CASE)
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

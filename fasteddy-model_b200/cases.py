@@ -21,8 +21,8 @@ _BASE = """Description = {desc}
 numProcsX = 1
 numProcsY = 1
 tBx = 1
-tBy = 4
-tBz = 64
+tBy = {tby}
+tBz = {tbz}
 inPath =
 inFile =
 outPath = ./output/
@@ -108,9 +108,43 @@ physics_oneRKonly = 1
 """
 
 
-def param_text(case: str, nx: int, ny: int, nz: int, *, dx: float = 20.0, dz: float = 10.0, dt: float = 0.05,
-               nt: int = 100, topo: str = "", ug: float = 10.0, z0: float = 0.05) -> str:
-    """Parameter file text of `case` at the given size."""
+# Time step. The cases ask for dx = dy = 20 m, dz = 10 m and dt = 0.05 s, but the
+# explicit acoustic step of this model is unstable there: c*dt*sqrt(dx^-2+dy^-2+dz^-2)
+# = 347*0.05*0.1225 = 2.1 exceeds the RK3 limit sqrt(3), and the reference build, the FP64
+# oracle and this engine all overflow after ~30 steps. dt = 0.025 s (1.06) is stable; the
+# work per step is unchanged.
+DT_STABLE = 0.025
+
+
+def exact_tiling(n_halo: int) -> int:
+    """Largest divisor of a halo-inclusive extent that fits a thread block dimension."""
+    for t in range(min(n_halo, 128), 0, -1):
+        if n_halo % t == 0:
+            return t
+    return 1
+
+
+def exact_tb(ny: int, nz: int, max_threads: int = 256) -> tuple[int, int]:
+    """(tBy, tBz) dividing the halo-inclusive extents exactly; at most `max_threads`
+    threads so the reference's register-heavy kernels can launch."""
+    tbz = exact_tiling(nz + 6)
+    while tbz > max_threads:
+        tbz = exact_tiling(tbz - 1) if (nz + 6) % (tbz - 1) == 0 else tbz - 1
+    tby = 1
+    for t in range(1, ny + 7):
+        if (ny + 6) % t == 0 and t * tbz <= max_threads:
+            tby = t
+    return tby, tbz
+
+
+def param_text(case: str, nx: int, ny: int, nz: int, *, dx: float = 20.0, dz: float = 10.0, dt: float = DT_STABLE,
+               nt: int = 100, topo: str = "", ug: float = 10.0, z0: float = 0.05, tb: tuple[int, int] | None = None) -> str:
+    """Parameter file text of `case` at the given size.
+
+    tb = (tBy, tBz) sets the reference build's thread-block shape; by default the
+    tutorials' (4, 64). A shape that divides the halo-inclusive extents exactly avoids
+    the reference's out-of-range threads (see oracle/refrun.py)."""
+    tby, tbz = tb if tb is not None else (4, 64)
     ztop = nz * dz - 0.5 * dz
     if case == "cbl_dry":
         kw = dict(desc="dry CBL, flat terrain", moist=0, damp=0, dampdepth=100.0, wth=0.35, zsb=600.0, pert=1)
@@ -126,7 +160,7 @@ def param_text(case: str, nx: int, ny: int, nz: int, *, dx: float = 20.0, dz: fl
     else:
         raise ValueError(f"unknown case {case}")
     return _BASE.format(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, dt=dt, nt=nt, topo=topo, lat=LAT_F1EM4, ug=ug,
-                        z0=z0, **kw)
+                        z0=z0, tby=tby, tbz=tbz, **kw)
 
 
 # Gaussian hill of the terrain cases: height 200 m, half-width 1 km (h = 200 * 2^-(r/1km)^2)
@@ -137,8 +171,11 @@ QV_SFC, QV_TOP, QV_ZTOP = 14.0, 4.0, 1500.0
 
 
 def setup_host(case: str, nx: int, ny: int, nz: int, seed: int = 12345, hill_halfwidth: float | None = None,
-               hill_height: float = HILL_HEIGHT, **kw):
-    """Load the case into the host layer (grid, base state, initial state). Returns the Host."""
+               hill_height: float = HILL_HEIGHT, qv: tuple[float, float, float] | None = None, **kw):
+    """Load the case into the host layer (grid, base state, initial state). Returns the Host.
+
+    qv = (q_sfc, q_top, z_top) overrides the water-vapour profile of the moist case
+    (tests use a supersaturated one to exercise the saturation adjustment)."""
     from .runtime import Host
 
     host = Host()
@@ -147,5 +184,5 @@ def setup_host(case: str, nx: int, ny: int, nz: int, seed: int = 12345, hill_hal
         host.gaussian_hill(hill_height, HILL_HALFWIDTH if hill_halfwidth is None else hill_halfwidth)
     host.init(seed)
     if case == "cbl_moist_hill":
-        host.set_qv_profile(QV_SFC, QV_TOP, QV_ZTOP)
+        host.set_qv_profile(*(qv if qv is not None else (QV_SFC, QV_TOP, QV_ZTOP)))
     return host

@@ -107,26 +107,31 @@ __device__ __forceinline__ float hyb56_flux(float m2, float m1, float z0, float 
 }
 
 // WENO5 face value from the upwind side, stencil a..e (cuda_advectionDevice.cu:626-926).
+// The squares of the smoothness indicators are products (the reference spells them
+// powf(x, 2.0)); the three normalised weights share one reciprocal of their sum.
 __device__ __forceinline__ float weno5_face(float a, float b, float c, float d, float e) {
   const float g1 = 1.0f / 10.0f, g2 = 3.0f / 5.0f, g3 = 3.0f / 10.0f, tol = 1e-6f;
-  float f1 = (1.0f / 3.0f) * a - (7.0f / 6.0f) * b + (11.0f / 6.0f) * c;
-  float f2 = -(1.0f / 6.0f) * b + (5.0f / 6.0f) * c + (1.0f / 3.0f) * d;
-  float f3 = (1.0f / 3.0f) * c + (5.0f / 6.0f) * d - (1.0f / 6.0f) * e;
-  float b1 = (13.0f / 12.0f) * powf((a - 2.0f * b + c), 2.0f) + (1.0f / 4.0f) * powf((a - 4.0f * b + 3.0f * c), 2.0f);
-  float b2 = (13.0f / 12.0f) * powf((b - 2.0f * c + d), 2.0f) + (1.0f / 4.0f) * powf((b - d), 2.0f);
-  float b3 = (13.0f / 12.0f) * powf((c - 2.0f * d + e), 2.0f) + (1.0f / 4.0f) * powf((3.0f * c - 4.0f * d + e), 2.0f);
-  float w1 = g1 / powf((tol + b1), 2.0f);
-  float w2 = g2 / powf((tol + b2), 2.0f);
-  float w3 = g3 / powf((tol + b3), 2.0f);
-  float ws = w1 + w2 + w3;
-  return (w1 / ws) * f1 + (w2 / ws) * f2 + (w3 / ws) * f3;
+  const float f1 = (1.0f / 3.0f) * a - (7.0f / 6.0f) * b + (11.0f / 6.0f) * c;
+  const float f2 = -(1.0f / 6.0f) * b + (5.0f / 6.0f) * c + (1.0f / 3.0f) * d;
+  const float f3 = (1.0f / 3.0f) * c + (5.0f / 6.0f) * d - (1.0f / 6.0f) * e;
+  const float s1 = a - 2.0f * b + c, t1 = a - 4.0f * b + 3.0f * c;
+  const float s2 = b - 2.0f * c + d, t2 = b - d;
+  const float s3 = c - 2.0f * d + e, t3 = 3.0f * c - 4.0f * d + e;
+  const float b1 = (13.0f / 12.0f) * (s1 * s1) + (1.0f / 4.0f) * (t1 * t1);
+  const float b2 = (13.0f / 12.0f) * (s2 * s2) + (1.0f / 4.0f) * (t2 * t2);
+  const float b3 = (13.0f / 12.0f) * (s3 * s3) + (1.0f / 4.0f) * (t3 * t3);
+  const float q1 = tol + b1, q2 = tol + b2, q3 = tol + b3;
+  const float w1 = g1 / (q1 * q1);
+  const float w2 = g2 / (q2 * q2);
+  const float w3 = g3 / (q3 * q3);
+  const float inv = 1.0f / (w1 + w2 + w3);
+  return (w1 * inv) * f1 + (w2 * inv) * f2 + (w3 * inv) * f3;
 }
 
+// The reference blends both one-sided values with weights 0.5(1 +- sign(u)), which are
+// exactly 1 and 0; only the upwind value is evaluated here (same result).
 __device__ __forceinline__ float weno5_flux(float m2, float m1, float z0, float p1, float p2, float p3, float vel) {
-  float fP = weno5_face(m2, m1, z0, p1, p2);
-  float fN = weno5_face(p3, p2, p1, z0, m1);
-  float s = sgnf(vel);
-  return 0.5f * (1.0f + s) * fP + 0.5f * (1.0f - s) * fN;
+  return sgnf(vel) > 0.0f ? weno5_face(m2, m1, z0, p1, p2) : weno5_face(p3, p2, p1, z0, m1);
 }
 
 // Face velocities of a cell: lower/upper faces in x, y, z (cuda_advectionDevice.cu:54-121).

@@ -59,6 +59,7 @@ struct fe_domain {
   float* surf = nullptr;
   float* frhs = nullptr;
   void* clock = nullptr;
+  unsigned long long* counter = nullptr;
   float simTime = 0.0f;
   int simIt = 0;
   bool haveGrid = false, haveBase = false, haveState = false;
@@ -244,6 +245,7 @@ static void free_domain(fe_domain* d) {
   cudaFree(d->surf);
   cudaFree(d->frhs);
   cudaFree(d->clock);
+  cudaFree(d->counter);
   if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
 }
@@ -278,6 +280,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   if (rc == FE_OK) rc = dev_alloc(d, &d->surf, n2 * 11);
   if (rc == FE_OK) {
     cudaError_t e = cudaMalloc(&d->clock, 64);
+    if (e == cudaSuccess) e = cudaMalloc(&d->counter, sizeof(unsigned long long));
     if (e != cudaSuccess) rc = set_err(FE_ERR_NOMEM, "clock allocation failed");
     else cudaMemsetAsync(d->clock, 0, 64, d->stream);
   }
@@ -458,7 +461,7 @@ static dim3 stage_grid(const fe_domain* d) {
 }
 static dim3 turb_grid(const fe_domain* d) {
   const Phys& P = d->P;
-  return dim3((P.Nz + 2 + d->tk - 1) / d->tk, (P.Ny + 1 + d->tj - 1) / d->tj, (P.Nx + 1 + d->ti - 1) / d->ti);
+  return dim3((P.Nz + 2 + d->tk - 1) / d->tk, (P.Ny + 2 + d->tj - 1) / d->tj, (P.Nx + 2 + d->ti - 1) / d->ti);
 }
 
 static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }
@@ -623,15 +626,13 @@ extern "C" int fe_get_frhs(fe_domain* d, float* hydroFrhs, float* sgstkeFrhs, fl
 extern "C" int fe_count_nonfinite(fe_domain* d, long long* count) {
   if (!d || !count) return set_err(FE_ERR_ARG, "NULL argument");
   CU(cudaSetDevice(d->device));
-  unsigned long long* dc = nullptr;
-  CU(cudaMalloc(&dc, sizeof(unsigned long long)));
+  unsigned long long* dc = d->counter;
   cudaMemsetAsync(dc, 0, sizeof(unsigned long long), d->stream);
   fe::k_nonfinite<<<blocks1d(d->P.n, 256), 256, 0, d->stream>>>(d->P, d->st[0], dc);
   d->launches++;
   unsigned long long h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, dc, sizeof(h), cudaMemcpyDeviceToHost, d->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
-  cudaFree(dc);
   if (e != cudaSuccess) return set_err(FE_ERR_CUDA, cudaGetErrorString(e));
   *count = (long long)h;
   return FE_OK;
@@ -703,6 +704,49 @@ extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
   if (tk) *tk = d->tk;
   if (tj) *tj = d->tj;
   if (ti) *ti = d->ti;
+  return FE_OK;
+}
+
+extern "C" int fe_host_register(void* ptr, size_t bytes) {
+  if (!ptr || !bytes) return FE_OK;
+  cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(FE_ERR_CUDA, std::string("cudaHostRegister: ") + cudaGetErrorString(e));
+  }
+  return FE_OK;
+}
+
+extern "C" int fe_host_unregister(void* ptr) {
+  if (!ptr) return FE_OK;
+  cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(FE_ERR_CUDA, std::string("cudaHostUnregister: ") + cudaGetErrorString(e));
+  }
+  return FE_OK;
+}
+
+extern "C" int fe_time_stage_kernel(fe_domain* d, int reps, float* ms) {
+  if (!d || !ms || reps <= 0) return set_err(FE_ERR_ARG, "bad argument");
+  if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
+  CU(cudaSetDevice(d->device));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  dim3 blk(d->tk, d->tj, d->ti), g = stage_grid(d);
+  cudaEventRecord(e0, d->stream);
+  for (int r = 0; r < reps; r++)
+    fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, d->stream>>>(d->P, d->Q, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
+  cudaEventRecord(e1, d->stream);
+  d->launches += reps;
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, cudaGetErrorString(e));
+  *ms = t / reps;
   return FE_OK;
 }
 

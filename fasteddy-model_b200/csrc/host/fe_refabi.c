@@ -22,6 +22,29 @@
 
 static fe_domain *g_dom = NULL;
 static int g_device = 0;
+static float *g_pinned[4] = {NULL, NULL, NULL, NULL};
+
+/* Page-lock the host state arrays the batch copies move (undone at cleanup). */
+static void pin_host_state(void) {
+  size_t n = (size_t)(Nxp + 2 * Nh) * (Nyp + 2 * Nh) * (Nzp + 2 * Nh);
+  float *bufs[4] = {hydroFlds, hydroPres, TKESelector > 0 ? sgstkeScalars : NULL, moistureSelector > 0 ? moistScalars : NULL};
+  size_t nf[4] = {5, 1, (size_t)TKESelector, (size_t)moistureNvars};
+  int b;
+  for (b = 0; b < 4; b++) {
+    if (g_pinned[b] == bufs[b]) continue;
+    if (g_pinned[b]) fe_host_unregister(g_pinned[b]);
+    g_pinned[b] = NULL;
+    if (bufs[b] && nf[b] > 0 && fe_host_register(bufs[b], n * nf[b] * sizeof(float)) == FE_OK) g_pinned[b] = bufs[b];
+  }
+}
+
+static void unpin_host_state(void) {
+  int b;
+  for (b = 0; b < 4; b++) {
+    if (g_pinned[b]) fe_host_unregister(g_pinned[b]);
+    g_pinned[b] = NULL;
+  }
+}
 
 static void fill_config(fe_config *c) {
   fe_config_defaults(c);
@@ -102,6 +125,7 @@ int cuda_hydroCoreInit(void) {
 
 int cuda_hydroCoreCleanup(void) {
   int rc = FE_OK;
+  unpin_host_state();
   if (g_dom) rc = fe_destroy(g_dom);
   g_dom = NULL;
   return rc;
@@ -134,7 +158,10 @@ int cuda_timeIntHydroSynchFromDevice(void) {
   return rc;
 }
 
-int cuda_timeIntInit(void) { return cuda_timeIntHydroInitDevice(); }
+int cuda_timeIntInit(void) {
+  pin_host_state();
+  return cuda_timeIntHydroInitDevice();
+}
 
 int cuda_timeIntCleanup(void) { return FE_OK; }
 

@@ -127,6 +127,9 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_set_tiling", ip, [vp, ip, ip, ip]),
         ("fe_autotune", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_launch_count", ctypes.c_longlong, [vp]),
+        ("fe_time_stage_kernel", ip, [vp, ip, fp]),
+        ("fe_host_register", ip, [vp, ctypes.c_size_t]),
+        ("fe_host_unregister", ip, [vp]),
         ("fe_ensemble_create", ip, [ctypes.POINTER(vp), ip, ctypes.POINTER(vp)]),
         ("fe_ensemble_advance", ip, [vp, ip]),
         ("fe_ensemble_sync", ip, [vp]),
@@ -366,6 +369,12 @@ class Domain:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(self.e.fe_autotune(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "fe_autotune")
         return a.value, b.value, c.value
+
+    def time_stage_kernel(self, reps: int = 10) -> float:
+        """Mean ms per launch of the fused dynamics stage kernel (CUDA events)."""
+        ms = ctypes.c_float()
+        _check(self.e.fe_time_stage_kernel(self.h, reps, ctypes.byref(ms)), "fe_time_stage_kernel")
+        return float(ms.value)
 
     def launch_count(self) -> int:
         return int(self.e.fe_launch_count(self.h))

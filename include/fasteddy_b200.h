@@ -174,6 +174,13 @@ int fe_domain_means(fe_domain *d, double *means);
 int fe_set_tiling(fe_domain *d, int tk, int tj, int ti);
 /* Pick the tiling by timing the candidates (the autotuner); writes the choice. */
 int fe_autotune(fe_domain *d, int *tk, int *tj, int *ti);
+/* Page-lock an existing host buffer for faster copies (cudaHostRegister) and undo it. */
+int fe_host_register(void *ptr, size_t bytes);
+int fe_host_unregister(void *ptr);
+/* Time `reps` back-to-back launches of the fused dynamics stage kernel (the RK3 second
+ * stage, whose output buffer every step rewrites, so the model state is unchanged) with
+ * CUDA events on the domain's stream; *ms receives the mean time per launch. */
+int fe_time_stage_kernel(fe_domain *d, int reps, float *ms);
 /* Number of engine kernel launches enqueued since creation (for bookkeeping). */
 long long fe_launch_count(const fe_domain *d);
 

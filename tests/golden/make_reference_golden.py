@@ -1,0 +1,70 @@
+"""Generate the reference-build golden vectors in tests/golden (run on a GPU box).
+
+Runs the reference's own CUDA build (oracle/_ref, built by oracle/build_ref.py) on small
+seeded cases produced by the host layer and stores its prognostic state after 1 and 10
+RK3 steps, so the FP64 oracle and the engine are checked against the reference's own
+outputs. The reference runs with a thread-block shape that divides the halo-inclusive
+extents (no out-of-range threads), twice, and the run-to-run difference is stored too.
+
+usage: python tests/golden/make_reference_golden.py OUTDIR
+"""
+from __future__ import annotations
+
+import hashlib
+import importlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+fe = importlib.import_module("fasteddy-model_b200")
+from oracle import refrun  # noqa: E402
+
+CASES = {
+    "cbl_dry": dict(case="cbl_dry", nx=16, ny=12, nz=12, kw={}),
+    "moist_hill": dict(case="cbl_moist_hill", nx=16, ny=12, nz=12,
+                       kw=dict(hill_halfwidth=60.0, hill_height=15.0, qv=(24.0, 8.0, 300.0))),
+}
+
+
+def input_digest(inp: dict) -> str:
+    h = hashlib.sha256()
+    for k in sorted(inp):
+        if inp[k] is not None:
+            h.update(k.encode())
+            h.update(np.ascontiguousarray(inp[k], dtype=np.float32).tobytes())
+    return h.hexdigest()
+
+
+def make_inputs(name: str):
+    c = CASES[name]
+    host = fe.cases.setup_host(c["case"], c["nx"], c["ny"], c["nz"], **c["kw"])
+    return host, host.inputs()
+
+
+def main(out: str) -> None:
+    os.makedirs(out, exist_ok=True)
+    for name, c in CASES.items():
+        host, inp = make_inputs(name)
+        ntke, nm = host.nfields()
+        text = fe.cases.param_text(c["case"], c["nx"], c["ny"], c["nz"], tb=fe.cases.exact_tb(c["ny"], c["nz"]))
+        res = {"input_sha256": np.array(input_digest(inp))}
+        for n in (1, 10):
+            a = refrun.run(text, inp, n, host.shape, ntke, nm)
+            b = refrun.run(text, inp, n, host.shape, ntke, nm)
+            I = (Ellipsis, slice(3, -3), slice(3, -3), slice(3, -3))
+            res[f"hydro_{n}"] = a["hydroFlds"][I]
+            res[f"self_absdiff_{n}"] = np.abs(a["hydroFlds"][I] - b["hydroFlds"][I]).max(axis=(1, 2, 3))
+            if ntke:
+                res[f"tke_{n}"] = a["sgstke"][I]
+            if nm:
+                res[f"moist_{n}"] = a["moist"][I]
+        np.savez_compressed(os.path.join(out, f"ref_{name}.npz"), **res)
+        print(name, {k: (v.shape if hasattr(v, "shape") else v) for k, v in res.items()}, flush=True)
+        host.cleanup()
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))

@@ -1,0 +1,73 @@
+"""Checks against golden vectors produced by the reference's own CUDA build
+(tests/golden/make_reference_golden.py, run on a B200 with oracle/_ref).
+
+The CPU test pins the FP64 oracle to the reference's outputs; the GPU test checks the
+engine against the same vectors. Tolerances: the reference computes in FP32, so its
+state after one step differs from FP64 by FP32 rounding (see test_gpu_engine.py); the
+reference's own run-to-run spread is stored with the vectors and added to the bound.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, interior, rel_l2
+from oracle.pyoracle import Oracle
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _load(name):
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("mkgold", os.path.join(GOLDEN, "make_reference_golden.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    path = os.path.join(GOLDEN, f"ref_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"golden vectors {path} not generated")
+    return mk, np.load(path)
+
+
+TOL = {1: [1e-6, 1e-5, 2e-3, 2e-3, 1e-6], 10: [2e-6, 2e-5, 5e-3, 5e-3, 2e-6]}
+
+
+def _compare(state, gold, n, spread):
+    for f in range(5):
+        ref = gold[f"hydro_{n}"][f]
+        bound = TOL[n][f] + 4 * spread[f] / max(np.abs(ref).max(), 1e-30)
+        assert rel_l2(interior(state["hydroFlds"][f]), ref) < bound, (n, f)
+    if f"moist_{n}" in gold:
+        assert rel_l2(interior(state["moist"][0]), gold[f"moist_{n}"][0]) < 2e-6
+
+
+@pytest.mark.parametrize("name", ["cbl_dry", "moist_hill"])
+def test_oracle_matches_reference_build(fe, name):
+    mk, gold = _load(name)
+    host, inp = mk.make_inputs(name)
+    assert mk.input_digest(inp) == str(gold["input_sha256"]), "host layer changed the golden inputs"
+    o = Oracle(host.config())
+    o.set_inputs(inp)
+    o.step(1)
+    _compare(o.get_state(), gold, 1, gold["self_absdiff_1"])
+    o.step(9)
+    _compare(o.get_state(), gold, 10, gold["self_absdiff_10"])
+    host.cleanup()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cbl_dry", "moist_hill"])
+def test_engine_matches_reference_build(fe, name):
+    mk, gold = _load(name)
+    host, inp = mk.make_inputs(name)
+    assert mk.input_digest(inp) == str(gold["input_sha256"])
+    d = fe.Domain(host.config())
+    d.set_inputs(inp)
+    d.advance(1)
+    _compare(d.get_state(), gold, 1, gold["self_absdiff_1"])
+    d.advance(9)
+    _compare(d.get_state(), gold, 10, gold["self_absdiff_10"])
+    d.close()
+    host.cleanup()

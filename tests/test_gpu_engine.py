@@ -1,0 +1,225 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle, plus the engine's
+own invariants: graph replay, drop-in entry points, ensembles, reductions, autotuner.
+
+Tolerances. The device path evaluates in FP32 like the reference. The tendency of
+momentum is a difference of FP32 perturbation pressures p' = p(rho theta) - p_BS with
+|p| ~ 1e5 Pa (ulp 0.008 Pa); the theta tendency a divergence of fluxes of |rho theta|
+~ 350. Both carry relative FP32 noise of order 1e-4 against the FP64 oracle on these
+perturbation-driven cases, so tendencies are checked at relative L2 <= 1e-3 and
+stresses at 2e-3. States after 1 and 10 steps are checked per field against their own
+norm: rho, rho theta, rho q_v at 1e-6 (FP32 storage), rho u at 1e-5, and the small
+fields rho v, rho w, rho e at 2e-3 (they start at or near zero, so their norm is small).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import interior, rel_l2
+from oracle.pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "cbl_dry": dict(case="cbl_dry", nx=24, ny=20, nz=16, kw={}),
+    "moist_hill": dict(case="cbl_moist_hill", nx=24, ny=20, nz=16,
+                       kw=dict(hill_halfwidth=90.0, hill_height=20.0, qv=(24.0, 8.0, 300.0))),
+    "hill_dry": dict(case="cbl_hill_dry", nx=20, ny=24, nz=16, kw=dict(hill_halfwidth=80.0, hill_height=25.0)),
+}
+
+STATE_TOL = [1e-6, 1e-5, 2e-3, 2e-3, 1e-6]
+
+
+def _setup(fe, name):
+    c = CASES[name]
+    host = fe.cases.setup_host(c["case"], c["nx"], c["ny"], c["nz"], **c["kw"])
+    return host, host.inputs(), host.config()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("stage", [0, 2])
+def test_tendency_matches_oracle(fe, name, stage):
+    host, inp, cfg = _setup(fe, name)
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    g = dom.build_frhs(stage)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    r = o.build_frhs(stage)
+    for f in range(5):
+        if np.abs(interior(r["hydroFrhs"][f])).max() == 0.0:
+            assert np.abs(interior(g["hydroFrhs"][f])).max() < 1e-6
+            continue
+        assert rel_l2(interior(g["hydroFrhs"][f]), interior(r["hydroFrhs"][f])) < 1e-3, f
+    if r["sgstkeFrhs"] is not None and stage == 2:
+        assert rel_l2(interior(g["sgstkeFrhs"][0]), interior(r["sgstkeFrhs"][0])) < 1e-3
+    if r["moistFrhs"] is not None:
+        for m in range(r["moistFrhs"].shape[0]):
+            if np.abs(interior(r["moistFrhs"][m])).max() > 0:
+                assert rel_l2(interior(g["moistFrhs"][m]), interior(r["moistFrhs"][m])) < 1e-3, m
+    if stage == 2:
+        # SGS stresses on the interior + upper ring the divergence reads
+        sl = (slice(3, -2), slice(3, -2), slice(3, -2))
+        for t in range(9):
+            assert rel_l2(g["taus"][t][sl], r["taus"][t][sl]) < 2e-3, t
+        sg, so = dom.get_surface(), o.get_surface()
+        for k in ("cd", "ch", "fricVel", "invOblen"):
+            assert rel_l2(sg[k][3:-3, 3:-3], so[k][3:-3, 3:-3]) < 1e-4, k
+    dom.close()
+    host.cleanup()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_state_matches_oracle_after_1_and_10_steps(fe, name):
+    host, inp, cfg = _setup(fe, name)
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    for n in (1, 9):
+        dom.advance(n)
+        o.step(n)
+        g, r = dom.get_state(), o.get_state()
+        for f in range(5):
+            assert rel_l2(interior(g["hydroFlds"][f]), interior(r["hydroFlds"][f])) < STATE_TOL[f], (n, f)
+        if r["sgstke"] is not None:
+            assert rel_l2(interior(g["sgstke"][0]), interior(r["sgstke"][0])) < 2e-3
+        if r["moist"] is not None:
+            assert rel_l2(interior(g["moist"][0]), interior(r["moist"][0])) < 1e-6
+            if np.abs(interior(r["moist"][1])).max() > 0:
+                assert rel_l2(interior(g["moist"][1]), interior(r["moist"][1])) < 2e-3
+        assert dom.nonfinite() == 0
+    if name == "moist_hill":
+        assert np.abs(interior(r["moist"][1])).max() > 0  # condensation happened
+    dom.close()
+    host.cleanup()
+
+
+def test_graph_replay_equals_step_by_step(fe):
+    host, inp, cfg = _setup(fe, "moist_hill")
+    a = fe.Domain(cfg)
+    a.set_inputs(inp)
+    a.advance(8)  # one captured 8-step graph
+    b = fe.Domain(cfg)
+    b.set_inputs(inp)
+    for _ in range(8):
+        b.advance(1)  # eager launches
+    sa, sb = a.get_state(), b.get_state()
+    for k in ("hydroFlds", "sgstke", "moist"):
+        np.testing.assert_array_equal(interior(sa[k]), interior(sb[k]))
+    a.close()
+    b.close()
+    host.cleanup()
+
+
+def test_tiling_and_autotune_do_not_change_results(fe):
+    host, inp, cfg = _setup(fe, "cbl_dry")
+    a = fe.Domain(cfg)
+    a.set_inputs(inp)
+    a.advance(3)
+    b = fe.Domain(cfg)
+    b.set_inputs(inp)
+    tk, tj, ti = b.autotune()
+    assert tk % 32 == 0 and tk * tj * ti <= 256
+    b.set_inputs(inp)
+    b.set_tiling(32, 8, 1)
+    b.advance(3)
+    np.testing.assert_array_equal(interior(a.get_state()["hydroFlds"]), interior(b.get_state()["hydroFlds"]))
+    a.close()
+    b.close()
+    host.cleanup()
+
+
+def test_dropin_entry_points_match_engine(fe):
+    """cuda_gridInit/..../cuda_timeIntCommence on the host globals == engine API."""
+    host, inp, cfg = _setup(fe, "moist_hill")
+    libs = fe.load()
+    ra = libs["refabi"]
+    host.set_gi("NtBatch", 5)
+    for fn in ("fecuda_Init", "cuda_gridInit", "cuda_hydroCoreInit", "cuda_timeIntInit"):
+        assert getattr(ra, fn)() == 0, fn
+    assert ra.fecuda_SetBlocksPerGrid(*host.shape) == 0
+    assert ra.cuda_timeIntCommence(0) == 0
+    assert host.gi("simTime_it") == 5
+    ref_h = host.array("hydroFlds", 5).copy()
+    ref_m = host.array("moistScalars", 2).copy()
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    dom.advance(5)
+    s = dom.get_state()
+    np.testing.assert_array_equal(interior(ref_h), interior(s["hydroFlds"]))
+    np.testing.assert_array_equal(interior(ref_m), interior(s["moist"]))
+    # a second batch continues from the device state (no re-upload when it != restart step)
+    assert ra.cuda_timeIntCommence(5) == 0
+    dom.advance(5)
+    np.testing.assert_array_equal(interior(host.array("hydroFlds", 5)), interior(dom.get_state()["hydroFlds"]))
+    # the device-level tendency twin fills the host Frhs arrays
+    assert ra.cuda_hydroCoreDeviceBuildFrhs(0.0, 0, 0, host.gf("dt"), 0, 2) == 0
+    assert np.abs(interior(host.array("hydroFldsFrhs", 5)[3])).max() > 0
+    for fn in ("cuda_timeIntCleanup", "cuda_hydroCoreCleanup", "cuda_gridCleanup", "fecuda_Cleanup"):
+        assert getattr(ra, fn)() == 0
+    dom.close()
+    host.cleanup()
+
+
+def test_nonfinite_state_is_reported(fe):
+    host, inp, cfg = _setup(fe, "cbl_dry")
+    libs = fe.load()
+    ra = libs["refabi"]
+    host.array("hydroFlds", 5)[4, 10, 10, 8] = np.nan
+    host.set_gi("NtBatch", 1)
+    assert ra.fecuda_Init() == 0 and ra.cuda_gridInit() == 0 and ra.cuda_hydroCoreInit() == 0
+    assert ra.cuda_timeIntInit() == 0
+    assert ra.cuda_timeIntCommence(0) == 6  # FE_ERR_NONFINITE
+    ra.cuda_hydroCoreCleanup()
+    host.cleanup()
+
+
+def test_fp64_domain_means(fe):
+    host, inp, cfg = _setup(fe, "moist_hill")
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    dom.advance(2)
+    s = dom.get_state()
+    m = dom.means()
+    fields = [s["hydroFlds"][f] for f in range(5)] + [s["sgstke"][0]] + [s["moist"][k] for k in range(2)]
+    for f, a in enumerate(fields):
+        np.testing.assert_allclose(m[f], interior(a).astype(np.float64).mean(), rtol=1e-12, atol=1e-300)
+    dom.close()
+    host.cleanup()
+
+
+def test_ensemble_of_uneven_domains_matches_members(fe):
+    shapes = [(16, 12, 10), (20, 16, 12), (12, 20, 14)]
+    hosts, inps, cfgs = [], [], []
+    for i, (nx, ny, nz) in enumerate(shapes):
+        h = fe.cases.setup_host("abl_neutral", nx, ny, nz, seed=100 + i, ug=5.0 + 2 * i)
+        inps.append(h.inputs())
+        cfgs.append(h.config())
+        h.cleanup()
+    members = []
+    for cfg, inp in zip(cfgs, inps):
+        d = fe.Domain(cfg)
+        d.set_inputs(inp)
+        members.append(d)
+    ens = fe.Ensemble(members)
+    ens.advance(11)  # one 8-step graph + 3 eager steps
+    for cfg, inp, d in zip(cfgs, inps, members):
+        solo = fe.Domain(cfg)
+        solo.set_inputs(inp)
+        solo.advance(11)
+        np.testing.assert_array_equal(interior(d.get_state()["hydroFlds"]), interior(solo.get_state()["hydroFlds"]))
+        solo.close()
+    ens.close()
+    for d in members:
+        d.close()
+
+
+def test_unsupported_configuration_is_rejected(fe):
+    host, inp, cfg = _setup(fe, "cbl_dry")
+    cfg.advectionSelector = 1
+    with pytest.raises(fe.FeError, match="advectionSelector"):
+        fe.Domain(cfg)
+    host.cleanup()

@@ -1,0 +1,140 @@
+"""Known-answer tests of the FP64 oracle (the checker of the CUDA path).
+
+The reference ships no tests or golden vectors for this path; the oracle is pinned by
+analytic properties here and by the reference build's own outputs in
+tests/test_golden_reference.py."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import interior
+from oracle.pyoracle import Oracle
+
+
+def _host(fe, case, nx, ny, nz, edits=(), **kw):
+    host = fe.Host()
+    text = fe.cases.param_text(case, nx, ny, nz, **kw)
+    for a, b in edits:
+        assert a in text
+        text = text.replace(a, b)
+    host.load_params_text(text)
+    if kw.get("hill"):
+        pass
+    return host
+
+
+REST = (("thetaPerturbationSwitch = 1", "thetaPerturbationSwitch = 0"), ("U_g = 10.0", "U_g = 0.0"),
+        ("surflayerSelector = 1", "surflayerSelector = 0"))
+
+
+@pytest.mark.parametrize("hill", [False, True])
+def test_rest_state_has_zero_tendency(fe, hill):
+    case = "cbl_hill_dry" if hill else "cbl_dry"
+    host = _host(fe, case, 12, 10, 16, REST)
+    if hill:
+        host.gaussian_hill(20.0, 60.0)
+    host.init(1)
+    o = Oracle(host.config())
+    o.set_inputs(host.inputs())
+    for stage in (0, 2):
+        F = o.build_frhs(stage)
+        for f in range(5):
+            assert np.abs(interior(F["hydroFrhs"][f])).max() == 0.0, (stage, f)
+        assert np.abs(interior(F["sgstkeFrhs"][0])).max() == 0.0
+    host.cleanup()
+
+
+def test_uniform_geostrophic_flow_is_steady(fe):
+    edits = REST[:1] + REST[2:]  # keep U_g = 10 m/s, no perturbations, no surface layer
+    host = _host(fe, "cbl_dry", 12, 10, 16, edits)
+    host.init(1)
+    o = Oracle(host.config())
+    o.set_inputs(host.inputs())
+    F = o.build_frhs(2)["hydroFrhs"]
+    for f in range(5):
+        assert np.abs(interior(F[f])).max() < 1e-9, f
+    host.cleanup()
+
+
+def test_mass_is_conserved(fe):
+    host = fe.cases.setup_host("cbl_dry", 12, 10, 16)
+    inp = host.inputs()
+    o = Oracle(host.config())
+    o.set_inputs(inp)
+    D = interior(inp["D_Jac"].astype(np.float64))
+    m0 = (interior(inp["hydroFlds"][0].astype(np.float64)) * D).sum()
+    o.step(5)
+    m1 = (interior(o.get_state()["hydroFlds"][0]) * D).sum()
+    assert abs(m1 - m0) / m0 < 1e-13
+    host.cleanup()
+
+
+def _advective_tendency_error(fe, n):
+    """Relative max error of the rho*theta advective tendency of one sine wave per domain
+    (n cells per wavelength) advected by a uniform wind."""
+    edits = (("stabilityScheme = 1", "stabilityScheme = 0"), ("thetaPerturbationSwitch = 1", "thetaPerturbationSwitch = 0"),
+             ("surflayerSelector = 1", "surflayerSelector = 0"), ("turbulenceSelector = 1", "turbulenceSelector = 0"),
+             ("TKESelector = 1", "TKESelector = 0"), ("coriolisSelector = 1", "coriolisSelector = 0"),
+             ("U_g = 10.0", "U_g = 5.0"))
+    host = _host(fe, "cbl_dry", n, 4, 4, edits)
+    host.init(1)
+    inp = host.inputs()
+    H = inp["hydroFlds"].astype(np.float64)
+    dx = 20.0
+    L = n * dx
+    x = (np.arange(n + 6) - 3 + 0.5) * dx
+    rho = H[0]
+    H[4] = rho * (300.0 + np.sin(2 * np.pi * x / L))[:, None, None]
+    o = Oracle(host.config())
+    o.set_inputs(inp)
+    o.lib.ora_set_state_f64(o.h, np.ascontiguousarray(H).ctypes.data_as(o.lib.ora_set_state_f64.argtypes[1]), None, None)
+    F = o.build_frhs(0)["hydroFrhs"][4]
+    exact = -5.0 * rho * (2 * np.pi / L) * np.cos(2 * np.pi * x / L)[:, None, None]
+    # relative to the exact tendency: the grid spacing is fixed, so kh = 2 pi / n
+    err = np.abs(interior(F - exact)).max() / np.abs(interior(exact)).max()
+    host.cleanup()
+    return err
+
+
+def test_hyb56_advection_is_fifth_order(fe):
+    e1 = _advective_tendency_error(fe, 16)
+    e2 = _advective_tendency_error(fe, 32)
+    order = np.log2(e1 / e2)
+    assert 4.6 < order < 5.4, order
+
+
+def test_neutral_surface_layer_log_law(fe):
+    edits = (("surflayer_wth = 0.35", "surflayer_wth = 0.0"), ("thetaPerturbationSwitch = 1", "thetaPerturbationSwitch = 0"))
+    host = _host(fe, "cbl_dry", 8, 8, 8, edits)
+    host.init(1)
+    inp = host.inputs()
+    o = Oracle(host.config())
+    o.set_inputs(inp)
+    F = o.build_frhs(2)
+    s = o.get_surface()
+    z1, z0, kap = 5.0, 0.05, 0.4
+    cd = kap ** 2 / np.log((z1 + z0) / z0) ** 2
+    rho = inp["hydroFlds"][0][5, 5, 3]
+    U = inp["hydroFlds"][1][5, 5, 3] / rho
+    np.testing.assert_allclose(s["cd"][5, 5], cd, rtol=1e-6)  # z0 and dZi are float inputs
+    np.testing.assert_allclose(F["taus"][2][5, 5, 3], -cd * U * (U * rho), rtol=1e-6)
+    # the final u* is taken from the flux-form stress -cd|U|(rho u), so it carries sqrt(rho)
+    # (cuda_surfaceLayerDevice.cu:402-406)
+    np.testing.assert_allclose(s["fricVel"][5, 5], np.sqrt(cd * rho) * U, rtol=1e-6)
+    host.cleanup()
+
+
+def test_rk3_stage_weights(fe):
+    """phi* = phi + dt/3 F, phi** = phi + dt/2 F*, phi^{n+1} = phi + dt F** (WS2002)."""
+    host = fe.cases.setup_host("cbl_dry", 8, 8, 8)
+    inp = host.inputs()
+    o = Oracle(host.config())
+    o.set_inputs(inp)
+    phi0 = o.get_state()["hydroFlds"].copy()
+    F0 = o.build_frhs(0)["hydroFrhs"].copy()
+    o.rk_stage(0)
+    phi1 = o.get_state()["hydroFlds"]
+    dt = float(np.float32(0.025))  # dt is a float parameter (time_integration.h:26)
+    np.testing.assert_allclose(interior(phi1), interior(phi0 + dt / 3.0 * F0), rtol=0, atol=1e-12)
+    host.cleanup()

@@ -359,26 +359,35 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
   if (P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin) surface_column(P, Q, st, i, j, stage);
 }
 
-// Write value v of one field at interior cell (i,j,k) and at its periodic images; `bot`
-// also writes the 3 cells below kMin (bottom copy rule), `nbot` how many of them, `top`
-// the 3 cells above kMax-1 (zero-gradient rule).
+// Write value v of one field at interior cell (i,j,k) and at its periodic images; `nbot`
+// cells below kMin get the same value (bottom copy rule) and, if `top`, the 3 cells above
+// kMax-1 too (zero-gradient rule). Image columns exist for i within 3 of either x edge and
+// j within 3 of either y edge (both sides when the domain is narrower than 6).
+__device__ __forceinline__ void store_column(float* __restrict__ F, long long cb, float v, int nbot, bool top) {
+  F[cb] = v;
+  for (int h = 1; h <= nbot; h++) F[cb - h] = v;
+  if (top)
+    for (int h = 1; h <= 3; h++) F[cb + h] = v;
+}
+
 __device__ __forceinline__ void store_images(const Phys& P, float* __restrict__ F, int i, int j, int k, float v, int nbot,
                                              bool top) {
-  int is[3], js[3], ni = 0, nj = 0;
-  is[ni++] = i;
-  if (i < P.iMin + 3) is[ni++] = i + P.Nx;
-  if (i >= P.iMax - 3) is[ni++] = i - P.Nx;
-  js[nj++] = j;
-  if (j < P.jMin + 3) js[nj++] = j + P.Ny;
-  if (j >= P.jMax - 3) js[nj++] = j - P.Ny;
-  for (int a = 0; a < ni; a++)
-    for (int b = 0; b < nj; b++) {
-      const long long cb = (long long)is[a] * P.si + (long long)js[b] * P.sj + k;
-      F[cb] = v;
-      for (int h = 1; h <= nbot; h++) F[cb - h] = v;
-      if (top)
-        for (int h = 1; h <= 3; h++) F[cb + h] = v;
-    }
+  const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+  const long long dI = (long long)P.Nx * P.si, dJ = (long long)P.Ny * P.sj;
+  const bool ilo = i < P.iMin + 3, ihi = i >= P.iMax - 3, jlo = j < P.jMin + 3, jhi = j >= P.jMax - 3;
+  store_column(F, c, v, nbot, top);
+  if (jlo) store_column(F, c + dJ, v, nbot, top);
+  if (jhi) store_column(F, c - dJ, v, nbot, top);
+  if (ilo) {
+    store_column(F, c + dI, v, nbot, top);
+    if (jlo) store_column(F, c + dI + dJ, v, nbot, top);
+    if (jhi) store_column(F, c + dI - dJ, v, nbot, top);
+  }
+  if (ihi) {
+    store_column(F, c - dI, v, nbot, top);
+    if (jlo) store_column(F, c - dI + dJ, v, nbot, top);
+    if (jhi) store_column(F, c - dI - dJ, v, nbot, top);
+  }
 }
 
 // ------------------------------------------------------------------ fused stage
@@ -517,12 +526,12 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
   }
   if (P.buoy) {
     const float r = rho[c], rbs = Q.rhoBS[c];
-    if (P.nmoist == 1) {
-      const double rm = (double)r + (double)mq0[c] * 1e-3;
-      F3 = (float)((double)F3 - ((double)r / rm) * (double)P.g * (rm - (double)rbs));
-    } else if (P.nmoist == 2) {
-      const double rm = (double)r + (double)mq0[c] * 1e-3 + (double)mq1[c] * 1e-3;
-      F3 = (float)((double)F3 - ((double)r / rm) * (double)P.g * (rm - (double)rbs));
+    if (P.nmoist > 0) {
+      // Klemp (2007) moist buoyancy; the excess density (cancellation-sensitive) in FP64
+      double rm = (double)r + (double)mq0[c] * 1e-3;
+      if (P.nmoist == 2) rm += (double)mq1[c] * 1e-3;
+      const float ratio = r / (float)rm;
+      F3 = (float)((double)F3 - (double)(ratio * P.g) * (rm - (double)rbs));
     } else {
       F3 = F3 - P.g * (r - rbs);
     }

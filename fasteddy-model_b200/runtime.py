@@ -65,6 +65,13 @@ class FeConfig(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class FeNoallocArgs(ctypes.Structure):
+    """Mirror of `fe_noalloc_args` (device pointers)."""
+
+    _fields_ = [(n, ctypes.c_void_p) for n in ("zPos", "J31", "J32", "J33", "D_Jac", "invD_Jac", "baseState", "state",
+                                                "surface", "frhs")]
+
+
 class FeError(RuntimeError):
     pass
 
@@ -136,6 +143,9 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_ensemble_stream", vp, [vp]),
         ("fe_ensemble_destroy", ip, [vp]),
         ("fe_last_error", ctypes.c_char_p, []),
+        ("fe_noalloc_max_cells", ctypes.c_longlong, []),
+        ("fe_frhs_noalloc", ip, [ctypes.POINTER(FeConfig), ip, ctypes.c_float, ip, ctypes.POINTER(FeNoallocArgs), vp]),
+        ("fe_noalloc_last_error", ctypes.c_char_p, []),
     ]:
         _declare(engine, name, res, args)
     for name in ("fecuda_Init", "fecuda_DeallocateHaloBuffers", "fecuda_Cleanup", "cuda_gridInit", "cuda_gridCleanup",

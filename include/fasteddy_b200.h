@@ -192,6 +192,33 @@ int fe_ensemble_sync(fe_ensemble *e);
 void *fe_ensemble_stream(fe_ensemble *e);
 int fe_ensemble_destroy(fe_ensemble *e);
 
+/* ---------------------------------------------- allocation-free tendency evaluation */
+/* No counterpart in the reference. For callers that cannot allocate device memory (pool
+ * allocators that own all device memory, embedders whose memory footprint is fixed after
+ * start-up): evaluates the tendency of
+ * RK stage `stage` like fe_build_frhs, but all scratch lives in one static device array of
+ * FE_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until exit. Limit:
+ * (Nx+6)(Ny+6)(Nz+6) <= fe_noalloc_max_cells() (about 799k cells). All pointers are device
+ * pointers in the reference layout; `state` (5 + TKE + moisture fields) must have its halo
+ * cells filled (as fe_get_state returns them); `surface` holds the 11 planes cd, ch, cq,
+ * fricVel, htFlux, tskin, invOblen, z0m, z0t, qFlux, qskin and is updated in place on a
+ * physics stage; `frhs` receives the interior tendencies. The first call on a device looks
+ * up the array's device address; make that first call before any stream capture. Calls
+ * share the array, so calls that overlap on the GPU (other streams, other threads) race.
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default stream) and synchronises it. */
+#define FE_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+typedef struct fe_noalloc_args {
+  const float *zPos, *J31, *J32, *J33, *D_Jac, *invD_Jac;
+  const float *baseState;
+  const float *state;
+  float *surface;
+  float *frhs;
+} fe_noalloc_args;
+long long fe_noalloc_max_cells(void);
+int fe_frhs_noalloc(const fe_config *cfg, int stage, float simTime, int simTime_it, const fe_noalloc_args *args,
+                    void *stream);
+const char *fe_noalloc_last_error(void);
+
 /* Text of the last error of the calling thread. */
 const char *fe_last_error(void);
 

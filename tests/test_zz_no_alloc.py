@@ -1,0 +1,78 @@
+"""The allocation-free tendency entry point (fe_frhs_noalloc) against the engine's own
+tendency evaluation (fe_build_frhs), through the C ABI.
+
+fe_frhs_noalloc exists for callers that cannot allocate device memory -- code inside a
+CUDA graph that someone else is capturing, allocators that own all device memory, or
+embedders whose footprint is fixed after start-up. It keeps its scratch in one static
+device array instead of calling cudaMalloc. This file is collected last so that a run
+stopping at the first failure has already run every other test; it also passes alone.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import interior, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+
+
+def test_noalloc_tendency_matches_engine_on_two_calls(fe):
+    import torch
+
+    host = fe.cases.setup_host("cbl_moist_hill", 20, 16, 14, hill_halfwidth=80.0, hill_height=20.0,
+                               qv=(24.0, 8.0, 300.0))
+    inp, cfg = host.inputs(), host.config()
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    st = dom.get_state()  # halo cells filled by the engine
+    state = np.concatenate([st["hydroFlds"], st["sgstke"], st["moist"]])
+    zero2 = np.zeros_like(inp["z0m"])
+    surface = np.stack([zero2, zero2, zero2, inp["fricVel"], inp["htFlux"], inp["tskin"], zero2, inp["z0m"],
+                        inp["z0t"], inp["qFlux"], inp["qskin"]])
+    torch.cuda.init()
+    d = {k: _dev(torch, inp[k]) for k in ("zPos", "J31", "J32", "J33", "D_Jac", "invD_Jac")}
+    d["baseState"] = _dev(torch, inp["baseState"])
+    d["state"] = _dev(torch, state)
+    d["surface"] = _dev(torch, surface)
+    d["frhs"] = torch.zeros_like(d["state"])
+    args = fe.runtime.FeNoallocArgs(**{k: v.data_ptr() for k, v in d.items()})
+    eng = fe.load()["engine"]
+    assert state[0].size <= eng.fe_noalloc_max_cells()
+    torch.cuda.synchronize()
+    for stage in (0, 2):  # two calls in a row; the second runs the SGS/surface physics
+        rc = eng.fe_frhs_noalloc(ctypes.byref(cfg), stage, 0.0, 0, ctypes.byref(args), None)
+        assert rc == 0, eng.fe_noalloc_last_error().decode()
+        got = d["frhs"].cpu().numpy()
+        ref = dom.build_frhs(stage)
+        want = np.concatenate([ref["hydroFrhs"], ref["sgstkeFrhs"], ref["moistFrhs"]])
+        for f in range(want.shape[0]):
+            if np.abs(interior(want[f])).max() == 0.0:
+                assert np.abs(interior(got[f])).max() == 0.0
+            else:
+                assert rel_l2(interior(got[f]), interior(want[f])) < 1e-6, (stage, f)
+    dom.close()
+    host.cleanup()
+
+
+def test_noalloc_rejects_domains_beyond_its_scratch(fe):
+    import torch
+
+    host = fe.cases.setup_host("cbl_dry", 120, 120, 60)
+    cfg = host.config()
+    host.cleanup()
+    eng = fe.load()["engine"]
+    assert 126 * 126 * 66 > eng.fe_noalloc_max_cells()
+    t = torch.zeros(8, device="cuda")
+    p = t.data_ptr()
+    args = fe.runtime.FeNoallocArgs(**{k: p for k in ("zPos", "J31", "J32", "J33", "D_Jac", "invD_Jac", "baseState",
+                                                       "state", "surface", "frhs")})
+    rc = eng.fe_frhs_noalloc(ctypes.byref(cfg), 0, 0.0, 0, ctypes.byref(args), None)
+    assert rc == 3  # FE_ERR_ARG
+    assert b"exceeds" in eng.fe_noalloc_last_error()

@@ -54,7 +54,7 @@ def build(verbose: bool = False) -> dict[str, str]:
         "host": os.path.join(OUT, "libfe_host.so"),
     }
     hdr = [os.path.join(INC, "fasteddy_b200.h")]
-    eng_src = [os.path.join(ENGINE_DIR, "fe_engine.cu"), os.path.join(ENGINE_DIR, "fe_noalloc.cu")]
+    eng_src = [os.path.join(ENGINE_DIR, f) for f in ("fe_engine.cu", "fe_noalloc.cu", "fe_learn.cu")]
     eng_deps = eng_src + _sources(ENGINE_DIR, (".cuh", ".h")) + hdr
     if _stale(libs["engine"], eng_deps):
         cmd = [_nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",

@@ -63,6 +63,9 @@ struct Ptrs {
 
 __device__ __forceinline__ float sgnf(float x) { return copysignf(1.0f, x); }
 
+// 1/rho with the reference's floor (rhoInv in cuda_hydroCoreDevice.cu:952-957)
+__device__ __forceinline__ float rinv(float r) { return 1.0f / fmaxf(r, 1e-6f); }
+
 // ---------------------------------------------------------------- boundary values
 // Value of field `f` in the vertical halo cell (column source cell `src` = interior
 // column (is,js), level k outside [kMin,kMax)), for hydroBCs = 2:

@@ -25,6 +25,9 @@
 
 #include "fasteddy_b200.h"
 #include "fe_kernels.cuh"
+#include "fe_march.cuh"
+#include "fe_learn.h"
+#include "fe_sgs.cuh"
 
 using fe::Phys;
 using fe::Ptrs;
@@ -63,7 +66,10 @@ struct fe_domain {
   float simTime = 0.0f;
   int simIt = 0;
   bool haveGrid = false, haveBase = false, haveState = false;
-  int tk = 32, tj = 4, ti = 2;
+  int tk = 32, tj = 4, ti = 2;       // cell-kernel tiling
+  int kind = FE_KERNEL_MARCH;        // stage-kernel form
+  int mtj = 8, mni = 64;             // march kernel: rows per tile, planes per thread block
+  fe_mlp* mlp = nullptr;             // learned SGS closure (nullptr: TKE closure)
   cudaGraphExec_t graph = nullptr;
   int graphSteps = 0;
   long long launches = 0;
@@ -78,6 +84,8 @@ struct fe_ensemble {
 };
 
 extern "C" const char* fe_last_error(void) { return g_err.c_str(); }
+
+int fe_internal_error(int code, const char* msg) { return set_err(code, msg ? msg : ""); }
 
 extern "C" int fe_device_count(void) {
   int n = 0;
@@ -250,6 +258,8 @@ static void free_domain(fe_domain* d) {
   delete d;
 }
 
+static int march_attrs();
+
 extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   if (!cfg || !out) return set_err(FE_ERR_ARG, "NULL argument");
   *out = nullptr;
@@ -269,6 +279,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   }
   const Phys& P = d->P;
   const size_t n = (size_t)P.n, n2 = (size_t)P.n2;
+  rc = march_attrs();
   for (int b = 0; b < 3 && rc == FE_OK; b++) {
     rc = dev_alloc(d, &d->st[b], n * P.nf);
     if (rc == FE_OK) rc = dev_alloc(d, &d->pr[b], n);
@@ -426,6 +437,8 @@ extern "C" int fe_get_clock(const fe_domain* d, float* simTime, int* simTime_it)
 
 static unsigned blocks1d(long long n, int thr) { return (unsigned)((n + thr - 1) / thr); }
 
+static int finish_state(fe_domain* d);
+
 extern "C" int fe_set_state(fe_domain* d, const float* hydro, const float* sgstke, const float* moist) {
   if (!d || !hydro) return set_err(FE_ERR_ARG, "NULL argument");
   if (!d->haveGrid || !d->haveBase) return set_err(FE_ERR_STATE, "set the grid and base state before the state");
@@ -439,6 +452,14 @@ extern "C" int fe_set_state(fe_domain* d, const float* hydro, const float* sgstk
   if (!rc && P.ntke) rc = h2d(d, A + 5 * n, sgstke, n);
   if (!rc && P.nmoist) rc = h2d(d, A + (5 + P.ntke) * n, moist, n * P.nmoist);
   if (rc) return rc;
+  return finish_state(d);
+}
+
+// Halo values, perturbation pressure and the copies into B and C of the state just put into A.
+static int finish_state(fe_domain* d) {
+  const Phys& P = d->P;
+  const size_t n = (size_t)P.n;
+  float* A = d->st[0];
   fe::k_fill<<<blocks1d(P.n, 256), 256, 0, d->stream>>>(P, d->Q, A);
   CU(cudaGetLastError());
   fe::k_pressure<<<blocks1d(P.n, 256), 256, 0, d->stream>>>(P, d->Q, A, d->pr[0]);
@@ -466,19 +487,75 @@ static dim3 turb_grid(const fe_domain* d) {
 
 static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }
 
+// Dynamic shared memory limits of the march kernels (three plane buffers exceed the 48 KB
+// default at 8 rows); set on the current device before any launch or capture.
+template <int STAGE, int MODE>
+static cudaError_t march_attrs_one() {
+  cudaError_t e = cudaFuncSetAttribute(fe::k_march<STAGE, MODE, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       fe::MarchTile<8>::SMEM_BYTES);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fe::k_march<STAGE, MODE, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             fe::MarchTile<4>::SMEM_BYTES);
+  return e;
+}
+static int march_attrs() {
+  cudaError_t e = march_attrs_one<0, fe::MODE_COMMIT>();
+  if (e == cudaSuccess) e = march_attrs_one<1, fe::MODE_COMMIT>();
+  if (e == cudaSuccess) e = march_attrs_one<2, fe::MODE_COMMIT>();
+  if (e == cudaSuccess) e = march_attrs_one<0, fe::MODE_FRHS>();
+  if (e == cudaSuccess) e = march_attrs_one<1, fe::MODE_FRHS>();
+  if (e == cudaSuccess) e = march_attrs_one<2, fe::MODE_FRHS>();
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, std::string("march kernel attributes: ") + cudaGetErrorString(e));
+  return FE_OK;
+}
+
+// Launch the fused stage kernel of stage STAGE in the domain's chosen form.
+template <int STAGE, int MODE>
+static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
+                         const float* pcur, float* pnxt, float* frhs) {
+  const Phys& P = d->P;
+  if (d->kind == FE_KERNEL_MARCH) {
+    const int ni = d->mni;
+    if (d->mtj == 4) {
+      dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + 3) / 4, (P.Nx + ni - 1) / ni);
+      fe::k_march<STAGE, MODE, 4><<<g, dim3(fe::MK, 4), fe::MarchTile<4>::SMEM_BYTES, s>>>(P, d->Q, cur, base, nxt, pcur,
+                                                                                        pnxt, frhs, ni);
+    } else {
+      dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + 7) / 8, (P.Nx + ni - 1) / ni);
+      fe::k_march<STAGE, MODE, 8><<<g, dim3(fe::MK, 8), fe::MarchTile<8>::SMEM_BYTES, s>>>(P, d->Q, cur, base, nxt, pcur,
+                                                                                        pnxt, frhs, ni);
+    }
+  } else {
+    fe::k_stage<STAGE, MODE><<<stage_grid(d), dim3(d->tk, d->tj, d->ti), 0, s>>>(P, d->Q, cur, base, nxt, pcur, pnxt, frhs);
+  }
+}
+
 // Enqueue one RK3 step on stream s (no host synchronisation; graph-capturable).
 static void enqueue_step(fe_domain* d, cudaStream_t s) {
   const Phys& P = d->P;
   const Ptrs& Q = d->Q;
-  dim3 blk(d->tk, d->tj, d->ti), g = stage_grid(d), gt = turb_grid(d);
+  dim3 blk(d->tk, d->tj, d->ti), gt = turb_grid(d);
   float *A = d->st[0], *B = d->st[1], *C = d->st[2];
   const bool physPrep = (P.turb || P.surf > 0);
-  if (physPrep && stage_has_physics(d, 0)) { fe::k_turb<<<gt, blk, 0, s>>>(P, Q, A, 0); d->launches++; }
-  fe::k_stage<0, fe::MODE_COMMIT><<<g, blk, 0, s>>>(P, Q, A, A, B, d->pr[0], d->pr[1], nullptr);
-  if (physPrep && stage_has_physics(d, 1)) { fe::k_turb<<<gt, blk, 0, s>>>(P, Q, B, 1); d->launches++; }
-  fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, s>>>(P, Q, B, A, C, d->pr[1], d->pr[2], nullptr);
-  if (physPrep && stage_has_physics(d, 2)) { fe::k_turb<<<gt, blk, 0, s>>>(P, Q, C, 2); d->launches++; }
-  fe::k_stage<2, fe::MODE_COMMIT><<<g, blk, 0, s>>>(P, Q, C, A, A, d->pr[2], d->pr[0], nullptr);
+  const bool learned = d->mlp && P.turb;
+  if (physPrep && stage_has_physics(d, 0)) {
+    fe::k_turb<<<gt, blk, 0, s>>>(P, Q, A, 0);
+    d->launches++;
+    if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, A, s); d->launches++; }
+  }
+  launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
+  if (physPrep && stage_has_physics(d, 1)) {
+    fe::k_turb<<<gt, blk, 0, s>>>(P, Q, B, 1);
+    d->launches++;
+    if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, B, s); d->launches++; }
+  }
+  launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
+  if (physPrep && stage_has_physics(d, 2)) {
+    fe::k_turb<<<gt, blk, 0, s>>>(P, Q, C, 2);
+    d->launches++;
+    if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, C, s); d->launches++; }
+  }
+  launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], nullptr);
   fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
   d->launches += 4;
 }
@@ -506,7 +583,7 @@ static int build_graph(fe_domain* d) {
 
 static int launches_per_step(const fe_domain* d) {
   int l = 4;
-  if (d->P.turb || d->P.surf > 0) l += d->P.oneRK ? 1 : 3;
+  if (d->P.turb || d->P.surf > 0) l += (d->P.oneRK ? 1 : 3) * ((d->mlp && d->P.turb) ? 2 : 1);
   return l;
 }
 
@@ -540,6 +617,7 @@ extern "C" int fe_sync(fe_domain* d) {
   CU(cudaSetDevice(d->device));
   CU(cudaStreamSynchronize(d->stream));
   CU(cudaGetLastError());
+  if (d->mlp) return fe_mlp_check(d->mlp);
   return FE_OK;
 }
 
@@ -596,11 +674,15 @@ extern "C" int fe_build_frhs(fe_domain* d, int stage) {
   if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
     fe::k_turb<<<turb_grid(d), blk, 0, d->stream>>>(P, d->Q, A, stage);
     d->launches++;
+    if (d->mlp && P.turb) {
+      CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
+      d->launches++;
+    }
   }
   switch (stage) {
-    case 0: fe::k_stage<0, fe::MODE_FRHS><<<stage_grid(d), blk, 0, d->stream>>>(P, d->Q, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
-    case 1: fe::k_stage<1, fe::MODE_FRHS><<<stage_grid(d), blk, 0, d->stream>>>(P, d->Q, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
-    default: fe::k_stage<2, fe::MODE_FRHS><<<stage_grid(d), blk, 0, d->stream>>>(P, d->Q, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
+    case 0: launch_stage<0, fe::MODE_FRHS>(d, d->stream, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
+    case 1: launch_stage<1, fe::MODE_FRHS>(d, d->stream, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
+    default: launch_stage<2, fe::MODE_FRHS>(d, d->stream, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;
   }
   d->launches++;
   CU(cudaGetLastError());
@@ -667,28 +749,58 @@ extern "C" int fe_set_tiling(fe_domain* d, int tk, int tj, int ti) {
   return FE_OK;
 }
 
+extern "C" int fe_set_stage_kernel(fe_domain* d, int kind, int tj, int ni) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (kind != FE_KERNEL_CELL && kind != FE_KERNEL_MARCH) return set_err(FE_ERR_ARG, "unknown stage-kernel form");
+  if (kind == FE_KERNEL_MARCH) {
+    if (tj <= 0) tj = 8;
+    if (ni <= 0) ni = 64;
+    if (tj != 4 && tj != 8) return set_err(FE_ERR_ARG, "march kernel: tj must be 4 or 8");
+    d->mtj = tj;
+    d->mni = ni;
+  }
+  d->kind = kind;
+  invalidate_graph(d);
+  return FE_OK;
+}
+
+extern "C" int fe_get_stage_kernel(const fe_domain* d, int* kind, int* tj, int* ni) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (kind) *kind = d->kind;
+  if (tj) *tj = d->kind == FE_KERNEL_MARCH ? d->mtj : d->tj;
+  if (ni) *ni = d->kind == FE_KERNEL_MARCH ? d->mni : d->ti;
+  return FE_OK;
+}
+
 // Autotuner: times the dynamics stage kernel (writes only the stage-2 buffer C, which
-// every step overwrites) for each candidate launch shape and keeps the fastest.
+// every step overwrites) for each candidate form and launch shape and keeps the fastest.
 extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
   if (!d) return set_err(FE_ERR_ARG, "NULL handle");
   if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
   CU(cudaSetDevice(d->device));
-  static const int cand[][3] = {{32, 4, 2}, {32, 8, 1}, {32, 2, 4}, {64, 2, 2}, {64, 4, 1}, {32, 4, 1},
-                                {32, 2, 2}, {64, 2, 1}, {128, 2, 1}, {32, 1, 8}};
+  struct Cand { int kind, a, b, c; };
+  std::vector<Cand> cand;
+  for (int tjm : {8, 4})
+    for (int ni : {16, 32, 64, 128, 256})
+      if (ni <= std::max(16, d->P.Nx)) cand.push_back({FE_KERNEL_MARCH, tjm, ni, 0});
+  static const int cell[][3] = {{32, 4, 2}, {32, 8, 1}, {32, 2, 4}, {64, 2, 2}, {64, 4, 1}, {32, 4, 1}, {32, 2, 2}};
+  for (auto& c : cell)
+    if (!(c[0] > 32 * ((d->P.Nz + 31) / 32) && c[0] > 32)) cand.push_back({FE_KERNEL_CELL, c[0], c[1], c[2]});
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
   float best = 1e30f;
-  int bi = 0;
+  size_t bi = 0;
   const int reps = 5;
-  for (int c = 0; c < (int)(sizeof(cand) / sizeof(cand[0])); c++) {
-    if (cand[c][0] > 32 * ((d->P.Nz + 31) / 32) && cand[c][0] > 32) continue;
-    d->tk = cand[c][0]; d->tj = cand[c][1]; d->ti = cand[c][2];
-    dim3 blk(d->tk, d->tj, d->ti), g = stage_grid(d);
-    fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, d->stream>>>(d->P, d->Q, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
+  const fe_domain saved = *d;
+  for (size_t c = 0; c < cand.size(); c++) {
+    d->kind = cand[c].kind;
+    if (d->kind == FE_KERNEL_MARCH) { d->mtj = cand[c].a; d->mni = cand[c].b; }
+    else { d->tk = cand[c].a; d->tj = cand[c].b; d->ti = cand[c].c; }
+    launch_stage<1, fe::MODE_COMMIT>(d, d->stream, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
     cudaEventRecord(e0, d->stream);
     for (int r = 0; r < reps; r++)
-      fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, d->stream>>>(d->P, d->Q, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
+      launch_stage<1, fe::MODE_COMMIT>(d, d->stream, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
     cudaEventRecord(e1, d->stream);
     d->launches += reps + 1;
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
@@ -699,7 +811,11 @@ extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CU(cudaGetLastError());
-  d->tk = cand[bi][0]; d->tj = cand[bi][1]; d->ti = cand[bi][2];
+  d->kind = saved.kind; d->mtj = saved.mtj; d->mni = saved.mni; d->tk = saved.tk; d->tj = saved.tj; d->ti = saved.ti;
+  const Cand& b = cand[bi];
+  d->kind = b.kind;
+  if (b.kind == FE_KERNEL_MARCH) { d->mtj = b.a; d->mni = b.b; }
+  else { d->tk = b.a; d->tj = b.b; d->ti = b.c; }
   invalidate_graph(d);
   if (tk) *tk = d->tk;
   if (tj) *tj = d->tj;
@@ -727,6 +843,152 @@ extern "C" int fe_host_unregister(void* ptr) {
   return FE_OK;
 }
 
+// ------------------------------------------------------------------ learned SGS closure: data
+namespace fe {
+// inputs, closure stresses and density of every interior cell (row-major i, j, k)
+__global__ void k_sgs_sample(Phys P, Ptrs Q, const float* __restrict__ st, float* __restrict__ X, float* __restrict__ tau,
+                             float* __restrict__ rho) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cells = (long long)P.Nx * P.Ny * P.Nz;
+  if (t >= cells) return;
+  const int k = (int)(t % P.Nz), j = (int)((t / P.Nz) % P.Ny), i = (int)(t / ((long long)P.Nz * P.Ny));
+  const long long c = (long long)(i + P.iMin) * P.si + (long long)(j + P.jMin) * P.sj + (k + P.kMin);
+  float x[SGS_NIN];
+  sgs_inputs(P, Q, st, c, x);
+  if (X)
+    for (int q = 0; q < SGS_NIN; q++) X[t * SGS_NIN + q] = x[q];
+  if (tau)
+    for (int q = 0; q < SGS_NOUT; q++) tau[t * SGS_NOUT + q] = Q.tau[q * P.n + c];
+  if (rho) rho[t] = st[c];
+}
+
+// 2x2x2 box filter (flux form, Favre averages) of a fine state onto a coarse interior, and the
+// subfilter fluxes of the coarse cells divided by the filtered density:
+//   tau_ij/rho = [<rho u_i u_j> - <rho u_i><rho u_j>/<rho> + <tau_ij^fine>] / <rho>
+//   tauTH_j/rho likewise with theta for u_i; the coarse TKE gains the resolved subfilter energy.
+__global__ void k_coarsen(Phys Pf, Ptrs Qf, const float* __restrict__ fs, Phys Pc, float* __restrict__ cs,
+                          float* __restrict__ tgt) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long cells = (long long)Pc.Nx * Pc.Ny * Pc.Nz;
+  if (t >= cells) return;
+  const int K = (int)(t % Pc.Nz), J = (int)((t / Pc.Nz) % Pc.Ny), I = (int)(t / ((long long)Pc.Nz * Pc.Ny));
+  const long long nf = Pf.n;
+  double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};           // rho, rho u, rho v, rho w, rho theta, rho e, rho qv, rho ql
+  double uu[6] = {0, 0, 0, 0, 0, 0};                 // rho u u, rho v u, rho w u, rho w v, rho v v, rho w w
+  double ut[3] = {0, 0, 0};                          // rho theta u_j
+  double tf[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};        // fine closure stresses
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++)
+      for (int g = 0; g < 2; g++) {
+        const long long c = (long long)(2 * I + a + Pf.iMin) * Pf.si + (long long)(2 * J + b + Pf.jMin) * Pf.sj +
+                            (2 * K + g + Pf.kMin);
+        const double r = fs[c], ru = fs[nf + c], rv = fs[2 * nf + c], rw = fs[3 * nf + c], rt = fs[4 * nf + c];
+        m[0] += r; m[1] += ru; m[2] += rv; m[3] += rw; m[4] += rt;
+        if (Pf.ntke) m[5] += fs[5 * nf + c];
+        for (int q = 0; q < Pf.nmoist; q++) m[6 + q] += fs[(5 + Pf.ntke + q) * nf + c];
+        uu[0] += ru * ru / r; uu[1] += rv * ru / r; uu[2] += rw * ru / r;
+        uu[3] += rw * rv / r; uu[4] += rv * rv / r; uu[5] += rw * rw / r;
+        ut[0] += rt * ru / r; ut[1] += rt * rv / r; ut[2] += rt * rw / r;
+        for (int q = 0; q < 9; q++) tf[q] += Qf.tau[q * nf + c];
+      }
+  for (int q = 0; q < 8; q++) m[q] *= 0.125;
+  for (int q = 0; q < 6; q++) uu[q] *= 0.125;
+  for (int q = 0; q < 3; q++) ut[q] *= 0.125;
+  for (int q = 0; q < 9; q++) tf[q] *= 0.125;
+  const double r = m[0];
+  const double s11 = uu[0] - m[1] * m[1] / r, s21 = uu[1] - m[2] * m[1] / r, s31 = uu[2] - m[3] * m[1] / r;
+  const double s32 = uu[3] - m[3] * m[2] / r, s22 = uu[4] - m[2] * m[2] / r, s33 = uu[5] - m[3] * m[3] / r;
+  const double h1 = ut[0] - m[4] * m[1] / r, h2 = ut[1] - m[4] * m[2] / r, h3 = ut[2] - m[4] * m[3] / r;
+  const long long cc = (long long)(I + Pc.iMin) * Pc.si + (long long)(J + Pc.jMin) * Pc.sj + (K + Pc.kMin);
+  const long long nc = Pc.n;
+  for (int q = 0; q < 5; q++) cs[q * nc + cc] = (float)m[q];
+  if (Pc.ntke) cs[5 * nc + cc] = (float)(m[5] + 0.5 * (s11 + s22 + s33));
+  for (int q = 0; q < Pc.nmoist; q++) cs[(5 + Pc.ntke + q) * nc + cc] = (float)m[6 + q];
+  if (tgt) {
+    const double v[9] = {s11 + tf[0], s21 + tf[1], s31 + tf[2], s32 + tf[3], s22 + tf[4],
+                         s33 + tf[5], h1 + tf[6], h2 + tf[7], h3 + tf[8]};
+    for (int q = 0; q < 9; q++) tgt[t * 9 + q] = (float)(v[q] / r);
+  }
+}
+}  // namespace fe
+
+extern "C" int fe_set_sgs_mlp(fe_domain* d, fe_mlp* m) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (m && fe_learn_device(m) != d->device) return set_err(FE_ERR_ARG, "network and domain must be on one device");
+  if (m && !d->P.turb) return set_err(FE_ERR_CONFIG, "the learned closure needs turbulenceSelector > 0");
+  d->mlp = m;
+  invalidate_graph(d);
+  return FE_OK;
+}
+
+// Evaluate the closure (TKE, or the network when set) on the current state and sample the
+// interior cells: inputs X (cells x 11), stresses tau (cells x 9), density rho (cells).
+extern "C" int fe_sgs_sample(fe_domain* d, float* X, float* tau, float* rho) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
+  if (!d->P.turb) return set_err(FE_ERR_CONFIG, "no SGS closure configured");
+  CU(cudaSetDevice(d->device));
+  const Phys& P = d->P;
+  const long long cells = (long long)P.Nx * P.Ny * P.Nz;
+  float* A = d->st[0];
+  fe::k_turb<<<turb_grid(d), dim3(d->tk, d->tj, d->ti), 0, d->stream>>>(P, d->Q, A, 2);
+  d->launches++;
+  if (d->mlp) {
+    CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
+    d->launches++;
+  }
+  float *dX = nullptr, *dT = nullptr, *dR = nullptr;
+  cudaError_t e = cudaMalloc(&dX, sizeof(float) * cells * fe::SGS_NIN);
+  if (e == cudaSuccess) e = cudaMalloc(&dT, sizeof(float) * cells * fe::SGS_NOUT);
+  if (e == cudaSuccess) e = cudaMalloc(&dR, sizeof(float) * cells);
+  if (e == cudaSuccess) {
+    fe::k_sgs_sample<<<blocks1d(cells, 256), 256, 0, d->stream>>>(P, d->Q, A, dX, dT, dR);
+    d->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && X) e = cudaMemcpyAsync(X, dX, sizeof(float) * cells * fe::SGS_NIN, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess && tau)
+    e = cudaMemcpyAsync(tau, dT, sizeof(float) * cells * fe::SGS_NOUT, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess && rho) e = cudaMemcpyAsync(rho, dR, sizeof(float) * cells, cudaMemcpyDeviceToHost, d->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  cudaFree(dX);
+  cudaFree(dT);
+  cudaFree(dR);
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, cudaGetErrorString(e));
+  if (d->mlp) return fe_mlp_check(d->mlp);
+  return FE_OK;
+}
+
+// Coarse-grain the state of `fine` (twice the cells per direction, same physical domain) into
+// `coarse` and return the subfilter targets (coarse cells x 9, divided by the filtered density).
+extern "C" int fe_coarsen(fe_domain* fine, fe_domain* coarse, float* tau_target) {
+  if (!fine || !coarse) return set_err(FE_ERR_ARG, "NULL handle");
+  if (!fine->haveState || !coarse->haveGrid || !coarse->haveBase) return set_err(FE_ERR_STATE, "states not ready");
+  const Phys &Pf = fine->P, &Pc = coarse->P;
+  if (Pf.Nx != 2 * Pc.Nx || Pf.Ny != 2 * Pc.Ny || Pf.Nz != 2 * Pc.Nz || Pf.ntke != Pc.ntke || Pf.nmoist != Pc.nmoist)
+    return set_err(FE_ERR_ARG, "fine domain must have twice the coarse cells per direction and the same fields");
+  if (fine->device != coarse->device) return set_err(FE_ERR_ARG, "domains must be on one device");
+  if (!Pf.turb) return set_err(FE_ERR_CONFIG, "the fine domain needs an SGS closure");
+  CU(cudaSetDevice(fine->device));
+  // the fine model's own subgrid stresses of its current state
+  fe::k_turb<<<turb_grid(fine), dim3(fine->tk, fine->tj, fine->ti), 0, fine->stream>>>(Pf, fine->Q, fine->st[0], 2);
+  fine->launches++;
+  const long long cells = (long long)Pc.Nx * Pc.Ny * Pc.Nz;
+  float* dT = nullptr;
+  if (tau_target) CU(cudaMalloc(&dT, sizeof(float) * cells * 9));
+  fe::k_coarsen<<<blocks1d(cells, 256), 256, 0, fine->stream>>>(Pf, fine->Q, fine->st[0], Pc, coarse->st[0], dT);
+  fine->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && dT) e = cudaMemcpyAsync(tau_target, dT, sizeof(float) * cells * 9, cudaMemcpyDeviceToHost, fine->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(fine->stream);
+  cudaFree(dT);
+  if (e != cudaSuccess) return set_err(FE_ERR_CUDA, cudaGetErrorString(e));
+  invalidate_graph(coarse);
+  int rc = finish_state(coarse);
+  if (rc) return rc;
+  return FE_OK;
+}
+
 extern "C" int fe_time_stage_kernel(fe_domain* d, int reps, float* ms) {
   if (!d || !ms || reps <= 0) return set_err(FE_ERR_ARG, "bad argument");
   if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
@@ -734,10 +996,9 @@ extern "C" int fe_time_stage_kernel(fe_domain* d, int reps, float* ms) {
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
-  dim3 blk(d->tk, d->tj, d->ti), g = stage_grid(d);
   cudaEventRecord(e0, d->stream);
   for (int r = 0; r < reps; r++)
-    fe::k_stage<1, fe::MODE_COMMIT><<<g, blk, 0, d->stream>>>(d->P, d->Q, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
+    launch_stage<1, fe::MODE_COMMIT>(d, d->stream, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
   cudaEventRecord(e1, d->stream);
   d->launches += reps;
   cudaError_t e = cudaEventSynchronize(e1);

@@ -76,8 +76,6 @@ __global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, float* 
   pres[t] = pert_pressure(P, st, Q.pBS, src);
 }
 
-__device__ __forceinline__ float rinv(float r) { return 1.0f / fmaxf(r, 1e-6f); }
-
 // SGS length scale at cell c (cuda_sgstkeDevice.cu:96-151).
 __device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, const float* __restrict__ rho,
                                               const float* __restrict__ th, const float* __restrict__ e, long long c) {

@@ -1,0 +1,588 @@
+// fe_march.cuh -- the fused stage kernel in i-marching form (sm_100a).
+//
+// A thread block owns a tile of 32 levels (k, one warp wide, so every row of the tile is one
+// 128-byte line) by TJ rows (j) and marches along i over a chunk of `ni` planes:
+//
+//   x direction   s(i..i+3) of every advected field live in registers (plus the prefetched
+//                 plane i+4), s(i-1) and s(i-2) are the thread's own cells of the two other
+//                 plane buffers; the x-face flux times the face velocity of the previous plane
+//                 is carried, so every x face is evaluated once.
+//   y, z          read a shared-memory copy of the (j,k) plane with a 3-cell ring. Three plane
+//                 buffers rotate: the thread's own value comes from its register window, the
+//                 ring of plane i+1 arrives by cp.async while plane i is computed, and one
+//                 __syncthreads per plane separates the two.
+//   face velocities  the contravariant velocities (D/rho)(m + w J) of plane i+1 are produced
+//                 one plane ahead into the same buffers (own cell plus a one-cell ring), so a
+//                 y or z face velocity costs one shared load.
+//
+// Everything else -- PGF, Rayleigh damping, buoyancy, Coriolis, SGS divergence and TKE budget,
+// saturation adjustment, the WS2002 commit with its halo images and the perturbation pressure
+// of the new state -- is the cell kernel's arithmetic (fe_kernels.cuh), term by term and in the
+// same order, evaluated on the register/shared copies.
+#pragma once
+#include "fe_kernels.cuh"
+
+namespace fe {
+
+constexpr int MK = 32;                      // levels per tile
+constexpr int MSLOTS = 9;                   // rho, rho u, rho v, rho w, rho theta, rho e, rho qv, rho ql, p'
+constexpr int SL_E = 5, SL_QV = 6, SL_QL = 7, SL_P = 8;
+
+template <int TJ>
+struct MarchTile {
+  static constexpr int PJ = TJ + 6, PK = MK + 6;   // staged plane with a 3-cell ring
+  static constexpr int PLANE = PJ * PK;
+  static constexpr int CYN = (TJ + 2) * MK;        // contravariant y velocity, rows j = -1..TJ
+  static constexpr int CZK = MK + 2;               // contravariant z velocity, columns k = -1..MK
+  static constexpr int CZN = TJ * CZK;
+  static constexpr int BUF = MSLOTS * PLANE + CYN + CZN;
+  static constexpr int NT = MK * TJ;
+  static constexpr int RING = PLANE - TJ * MK;
+  static constexpr int RPT = (RING + NT - 1) / NT;  // ring cells per thread
+  static constexpr int CYT = 2 * MK, CZT = 2 * TJ;   // ring tasks of the velocity planes
+  static constexpr int NBUF = 3;
+  static constexpr int SMEM_BYTES = NBUF * BUF * 4;
+};
+
+// Ring cell r of a staged plane: the 3 rows above and below the tile (full width), then the
+// 3 columns left and right of every tile row.
+template <int TJ>
+__device__ __forceinline__ void march_ring_cell(int r, int& row, int& col) {
+  constexpr int PK = MK + 6;
+  if (r < 6 * PK) {
+    row = r / PK;
+    col = r - row * PK;
+    if (row >= 3) row += TJ;
+  } else {
+    const int q = r - 6 * PK;
+    row = 3 + q / 6;
+    const int cc = q - (q / 6) * 6;
+    col = cc < 3 ? cc : MK + cc;
+  }
+}
+
+__device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ bool slot_on(const Phys& P, int s) {
+  if (s < 5) return true;
+  if (s == SL_E) return P.ntke > 0;
+  if (s == SL_QV) return P.nmoist > 0;
+  if (s == SL_QL) return P.nmoist > 1;
+  return P.pgf != 0;
+}
+__device__ __forceinline__ const float* slot_src(const Phys& P, const float* cur, const float* pcur, int s) {
+  if (s < 5) return cur + (long long)s * P.n;
+  if (s == SL_E) return cur + 5LL * P.n;
+  if (s == SL_QV) return cur + (long long)(5 + P.ntke) * P.n;
+  if (s == SL_QL) return cur + (long long)(6 + P.ntke) * P.n;
+  return pcur;
+}
+// advection scheme of a slot: 3 = HYB56, 5 = WENO5 (q_l always WENO5: moistureAdvSelectorQi = 2)
+__device__ __forceinline__ int slot_sel(const Phys& P, int s) {
+  if (s < 5) return P.advSel;
+  if (s == SL_E) return P.tkeAdvSel;
+  if (s == SL_QV) return P.qvAdvSel;
+  return 5;
+}
+__device__ __forceinline__ float slot_b(const Phys& P, int s) {
+  if (s < 5) return P.bHyb;
+  if (s == SL_E) return P.tkeBHyb;
+  if (s == SL_QV) return P.qvB;
+  return 0.0f;
+}
+
+template <int STAGE, int MODE, int TJ>
+__global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
+    k_march(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base, float* __restrict__ nxt,
+            const float* __restrict__ pcur, float* __restrict__ pnxt, float* __restrict__ frhs, int ni) {
+  using T = MarchTile<TJ>;
+  constexpr int PK = T::PK, PLANE = T::PLANE;
+  extern __shared__ __align__(16) float sm[];
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * MK + tx;
+  const int k0 = P.kMin + blockIdx.x * MK, j0 = P.jMin + blockIdx.y * TJ;
+  const int i0 = P.iMin + blockIdx.z * ni;
+  const int i1 = min(i0 + ni, P.iMax);
+  const int k = k0 + tx, j = j0 + ty;
+  const bool inArr = (k < P.nzh) && (j < P.nyh);     // the thread's column exists in memory
+  const bool active = (k < P.kMax) && (j < P.jMax);  // ... and is an interior column
+  const long long n = P.n;
+  const int si = P.si, sj = P.sj;
+  const long long col = (long long)j * sj + k;
+  const long long tile0 = (long long)j0 * sj + k0;
+  const int own = (ty + 3) * PK + (tx + 3);
+  const bool phys = (P.oneRK == 0) || (STAGE == 2);
+  const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
+
+  // ring cells of the staged planes handled by this thread
+  int rS[T::RPT], rG[T::RPT];
+  bool rV[T::RPT], rN[T::RPT];
+#pragma unroll
+  for (int q = 0; q < T::RPT; q++) {
+    const int r = tid + q * T::NT;
+    rV[q] = false; rN[q] = false; rS[q] = 0; rG[q] = 0;
+    if (r < T::RING) {
+      int row, cl;
+      march_ring_cell<TJ>(r, row, cl);
+      const int jj = j0 + row - 3, kk = k0 + cl - 3;
+      rV[q] = (jj < P.nyh) && (kk < P.nzh);
+      rN[q] = row >= 2 && row <= TJ + 3 && cl >= 2 && cl <= MK + 3;  // within one cell (p' ring)
+      rS[q] = row * PK + cl;
+      rG[q] = (row - 3) * sj + (cl - 3);
+    }
+  }
+  // velocity-plane ring task: cy at rows -1 and TJ, or cz at columns -1 and MK
+  int rtKind = 0, rtS = 0;
+  long long rtOff = 0;
+  {
+    int row = 0, cc = 0;
+    if (tid < T::CYT) {
+      rtKind = 1; row = (tid < MK) ? -1 : TJ; cc = tid & (MK - 1);
+      rtS = (row + 1) * MK + cc;
+    } else if (tid < T::CYT + T::CZT) {
+      const int q = tid - T::CYT;
+      rtKind = 2; row = q >> 1; cc = (q & 1) ? MK : -1;
+      rtS = T::CYN + row * T::CZK + (cc + 1);
+    }
+    const int jj = j0 + row, kk = k0 + cc;
+    if (rtKind && !(jj < P.nyh && kk < P.nzh)) rtKind = 0;
+    rtOff = (long long)jj * sj + kk;
+  }
+
+  auto issue_ring = [&](int ip, float* buf) {
+    const long long pl = (long long)ip * si + tile0;
+#pragma unroll
+    for (int s = 0; s < MSLOTS; s++) {
+      if (!slot_on(P, s)) continue;
+      const float* src = slot_src(P, cur, pcur, s) + pl;
+#pragma unroll
+      for (int q = 0; q < T::RPT; q++)
+        if (rV[q] && (s != SL_P || rN[q])) cp_async4(buf + s * PLANE + rS[q], src + rG[q]);
+    }
+    cp_async_commit();
+  };
+
+  // ---------------------------------------------------------------- prologue (plane i0)
+  // buffers: plane i0 -> 0, plane i0+1 -> 1 (holds s(i0-2) at the own cell until it is
+  // refilled), plane i0-1 -> 2
+  float w[8][4], nx[8], xc[8];
+  float pc1 = 0.0f, pnx = 0.0f;   // p'(i+1), p'(i+2)
+  float Dc = 0.0f, Dn = 0.0f, J1c = 0.0f, J1n = 0.0f, J2c = 0.0f, J3c = 0.0f;
+  const long long cA = (long long)i0 * si + col;
+#pragma unroll
+  for (int s = 0; s < 8; s++) {
+#pragma unroll
+    for (int d = 0; d < 4; d++) w[s][d] = 0.0f;
+    nx[s] = 0.0f; xc[s] = 0.0f;
+  }
+  float* const B0 = sm;
+  float* const B1 = sm + T::BUF;
+  float* const B2 = sm + 2 * T::BUF;
+  float Dm1 = 0.0f, J1m1 = 0.0f, rm1 = 0.0f, um1 = 0.0f, wm1 = 0.0f, p0v = 0.0f, pm1 = 0.0f;
+  if (inArr) {
+    Dm1 = Q.D[cA - si]; Dc = Q.D[cA]; Dn = Q.D[cA + si];
+    J1m1 = Q.J31[cA - si]; J1c = Q.J31[cA]; J1n = Q.J31[cA + si];
+    J2c = Q.J32[cA]; J3c = Q.J33[cA];
+    if (P.pgf) { pm1 = pcur[cA - si]; p0v = pcur[cA]; pc1 = pcur[cA + si]; }
+  }
+#pragma unroll
+  for (int s = 0; s < 8; s++) {
+    if (!slot_on(P, s)) continue;
+    const float* src = slot_src(P, cur, pcur, s);
+    float sm2 = 0.0f, sm1 = 0.0f;
+    if (inArr) {
+      sm2 = src[cA - 2 * (long long)si]; sm1 = src[cA - si];
+#pragma unroll
+      for (int d = 0; d < 4; d++) w[s][d] = src[cA + d * (long long)si];
+    }
+    B1[s * PLANE + own] = sm2;
+    B2[s * PLANE + own] = sm1;
+    B0[s * PLANE + own] = w[s][0];
+    if (s == 0) rm1 = sm1;
+    if (s == 1) um1 = sm1;
+    if (s == 3) wm1 = sm1;
+  }
+  if (P.pgf) { B0[SL_P * PLANE + own] = p0v; B2[SL_P * PLANE + own] = pm1; }
+  float cx0 = contra(Dc, w[0][0], w[1][0], w[3][0], J1c);
+  float upPrev;
+  {
+    const float cxm = contra(Dm1, rm1, um1, wm1, J1m1);
+    upPrev = (0.5f * dXi) * (cx0 + cxm);  // velocity of the face i0-1/2
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+      if (!slot_on(P, s)) continue;
+      const float* src = slot_src(P, cur, pcur, s);
+      const float m3 = inArr ? src[cA - 3 * (long long)si] : 0.0f;
+      const float m2 = B1[s * PLANE + own], m1 = B2[s * PLANE + own];
+      const float f = slot_sel(P, s) == 3
+                          ? hyb56_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev, 1.0f - slot_b(P, s))
+                          : weno5_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev);
+      xc[s] = upPrev * f;
+    }
+  }
+  float cyOwn, czOwn;
+  {
+    issue_ring(i0, B0);
+    const float dr = Dc / w[0][0];
+    cyOwn = dr * (w[2][0] + w[3][0] * J2c);
+    czOwn = dr * (w[3][0] * J3c);
+    float* v = B0 + MSLOTS * PLANE;
+    v[(ty + 1) * MK + tx] = cyOwn;
+    v[T::CYN + ty * T::CZK + tx + 1] = czOwn;
+    if (rtKind) {
+      const long long c = (long long)i0 * si + rtOff;
+      const float D = Q.D[c], r = cur[c];
+      v[rtS] = rtKind == 1 ? contra(D, r, cur[2 * n + c], cur[3 * n + c], Q.J32[c]) : (D / r) * (cur[3 * n + c] * Q.J33[c]);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+
+  const bool mpStep = phys && P.nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
+
+  // ---------------------------------------------------------------- march
+  float *cs = B0, *ns = B1, *ps = B2;  // planes i, i+1 (own cell: s(i-2) until refilled), i-1
+  for (int i = i0; i < i1; i++) {
+    const bool more = (i + 1 < i1);
+    const long long c = (long long)i * si + col;
+
+    // prefetch: plane i+4 of the x window, p'(i+2), D and J31 at i+2, J32 and J33 at i+1
+    float Dnn = 0.0f, J1nn = 0.0f, J2n = 0.0f, J3n = 0.0f;
+    if (inArr) {
+      const bool has4 = (i + 4) < P.nxh;
+#pragma unroll
+      for (int s = 0; s < 8; s++)
+        if (slot_on(P, s) && has4) nx[s] = slot_src(P, cur, pcur, s)[c + 4 * (long long)si];
+      if (P.pgf) pnx = pcur[c + 2 * (long long)si];
+      Dnn = Q.D[c + 2 * (long long)si];
+      J1nn = Q.J31[c + 2 * (long long)si];
+      J2n = Q.J32[c + si];
+      J3n = Q.J33[c + si];
+    }
+    if (more) issue_ring(i + 1, ns);
+    float rD = 0.0f, rR = 1.0f, rM = 0.0f, rW = 0.0f, rJ = 0.0f;
+    if (more && rtKind) {
+      const long long cr = (long long)(i + 1) * si + rtOff;
+      rD = Q.D[cr]; rR = cur[cr]; rW = cur[3 * n + cr];
+      if (rtKind == 1) { rM = cur[2 * n + cr]; rJ = Q.J32[cr]; }
+      else rJ = Q.J33[cr];
+    }
+
+    // face velocities of this cell (cuda_advectionDevice.cu:89-106)
+    const float cxp1 = contra(Dn, w[0][1], w[1][1], w[3][1], J1n);
+    const float up = (0.5f * dXi) * (cxp1 + cx0);
+    const float* cyP = cs + MSLOTS * PLANE;
+    const float* czP = cyP + T::CYN;
+    const float vm = (0.5f * dYi) * (cyOwn + cyP[ty * MK + tx]);
+    const float vp = (0.5f * dYi) * (cyP[(ty + 2) * MK + tx] + cyOwn);
+    const float wm = (k == P.kMin) ? 0.0f : (0.5f * dZi) * (czOwn + czP[ty * T::CZK + tx]);
+    const float wp = (k + 1 >= P.kMax) ? 0.0f : (0.5f * dZi) * (czP[ty * T::CZK + tx + 2] + czOwn);
+
+    const float J1 = J1c, J2 = J2c, J3 = J3c;
+    const float invD = inArr ? Q.invD[c] : 0.0f;
+    const float r0 = w[0][0];
+    float F[8];
+#pragma unroll
+    for (int s = 0; s < 8; s++) F[s] = 0.0f;
+
+    // pressure-gradient force (cuda_pressureDevice.cu:118-194)
+    if (P.pgf) {
+      const float* pp = cs + SL_P * PLANE + own;
+      const float dpx = pc1 - ps[SL_P * PLANE + own];
+      const float dpy = pp[PK] - pp[-PK];
+      const float dpz = pp[1] - pp[-1];
+      if (P.nmoist > 0) {
+        float rmd = 1.0f;
+        rmd = (float)((double)rmd + (double)(w[SL_QV][0] / r0) * 1e-3);
+        if (P.nmoist > 1) rmd = (float)((double)rmd + (double)(w[SL_QL][0] / r0) * 1e-3);
+        const float rdm = 1.0f / rmd;
+        F[1] = (float)((double)F[1] - (double)rdm * 0.5 * (double)dXi * (double)dpx);
+        F[2] = (float)((double)F[2] - (double)rdm * 0.5 * (double)dYi * (double)dpy);
+        F[3] = (float)((double)F[3] - (double)rdm * 0.5 * (double)(dXi * J1 * dpx + dYi * J2 * dpy + dZi * J3 * dpz));
+      } else {
+        F[1] = F[1] - (0.5f * dXi) * dpx;
+        F[2] = F[2] - (0.5f * dYi) * dpy;
+        F[3] = F[3] - 0.5f * (dXi * J1 * dpx + dYi * J2 * dpy + dZi * J3 * dpz);
+      }
+    }
+
+    // advection of every field (cuda_hydroCoreDevice.cu:631-672; WENO5 as x, y, z updates)
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+      if (!slot_on(P, s)) continue;
+      const float* pl = cs + s * PLANE + own;
+      const float z0 = w[s][0];
+      const float xm2 = ns[s * PLANE + own], xm1 = ps[s * PLANE + own];
+      if (slot_sel(P, s) == 3) {
+        const float bf = 1.0f - slot_b(P, s);
+        const float fxp = hyb56_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
+        const float pxp = up * fxp;
+        const float Dx = pxp - xc[s];
+        xc[s] = pxp;
+        float Dy, Dz;
+        {
+          const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
+          Dy = vp * hyb56_flux(m2, m1, z0, p1, p2, p3, vp, bf) - vm * hyb56_flux(m3, m2, m1, z0, p1, p2, vm, bf);
+        }
+        {
+          const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
+          Dz = wp * hyb56_flux(m2, m1, z0, p1, p2, p3, wp, bf) - wm * hyb56_flux(m3, m2, m1, z0, p1, p2, wm, bf);
+        }
+        F[s] = F[s] - invD * (Dx + Dy + Dz);
+      } else {
+        const float fxp = weno5_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up);
+        const float pxp = up * fxp;
+        F[s] = F[s] - invD * (pxp - xc[s]);
+        xc[s] = pxp;
+        {
+          const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
+          const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, vp);
+          const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, vm);
+          F[s] = F[s] - invD * (vp * fp - vm * fm);
+        }
+        {
+          const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
+          const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, wp);
+          const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, wm);
+          F[s] = F[s] - invD * (wp * fp - wm * fm);
+        }
+      }
+      if (s == 3) {
+        // Rayleigh damping and buoyancy act on F_w right after its advection
+        if (P.damp && inArr) {
+          const long long ctop = c - k + (P.kMax - 1);
+          const float z = Q.zPos[c], zt = Q.zPos[ctop];
+          if (z >= (zt - P.dampDepth)) {
+            const float rbs = Q.rhoBS[c];
+            const float wbs = momentum_bs(P, 3, z, rbs);
+            const float pio2 = 1.5707963267948966f;
+            const double sn = (double)sinf((float)((double)pio2 * (1.0 - (double)((zt - z) / P.dampDepth))));
+            F[3] = (float)((double)F[3] - 0.2 * (double)r0 * (sn * sn) * (double)(w[3][0] / r0 - wbs / rbs));
+          }
+        }
+        if (P.buoy) {
+          const float rbs = inArr ? Q.rhoBS[c] : 0.0f;
+          if (P.nmoist > 0) {
+            double rm = (double)r0 + (double)w[SL_QV][0] * 1e-3;
+            if (P.nmoist == 2) rm += (double)w[SL_QL][0] * 1e-3;
+            const float ratio = r0 / (float)rm;
+            F[3] = (float)((double)F[3] - (double)(ratio * P.g) * (rm - (double)rbs));
+          } else {
+            F[3] = F[3] - P.g * (r0 - rbs);
+          }
+        }
+      }
+    }
+
+    // Coriolis (cuda_coriolisDevice.cu:50-58)
+    if (P.cor && inArr) {
+      const float z = Q.zPos[c], rbs = Q.rhoBS[c];
+      const float ubs = momentum_bs(P, 1, z, rbs), vbs = momentum_bs(P, 2, z, rbs), wbs = momentum_bs(P, 3, z, rbs);
+      F[1] = F[1] + (P.fHorz * (w[2][0] / r0 - P.fLS * vbs / rbs) - P.fVert * (w[3][0] / r0 - P.fLS * wbs / rbs));
+      F[2] = F[2] - (P.fHorz * (w[1][0] / r0 - P.fLS * ubs / rbs));
+      F[3] = F[3] + (P.fVert * (w[1][0] / r0 - P.fLS * ubs / rbs));
+    }
+
+    if (phys && P.turb && active) {
+      // divergence of the SGS stresses (cuda_sgsTurbDevice.cu:447-547)
+      const float* Tt = Q.tau;
+      const long long ip = c + si, jp = c + sj, kp = c + 1;
+#define TT(m, x) Tt[(m) * n + (x)]
+      F[1] = F[1] - (dXi * (TT(0, ip) - TT(0, c)) + dYi * (TT(1, jp) - TT(1, c)) + J1 * dXi * (TT(2, ip) - TT(2, c)) +
+                     J2 * dYi * (TT(2, jp) - TT(2, c)) + J3 * dZi * (TT(2, kp) - TT(2, c)));
+      F[2] = F[2] - (dXi * (TT(1, ip) - TT(1, c)) + dYi * (TT(4, jp) - TT(4, c)) + J1 * dXi * (TT(3, ip) - TT(3, c)) +
+                     J2 * dYi * (TT(3, jp) - TT(3, c)) + J3 * dZi * (TT(3, kp) - TT(3, c)));
+      F[3] = F[3] - (dXi * (TT(2, ip) - TT(2, c)) + dYi * (TT(3, jp) - TT(3, c)) + J1 * dXi * (TT(5, ip) - TT(5, c)) +
+                     J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c)));
+      F[4] = F[4] - (dXi * (TT(6, ip) - TT(6, c)) + dYi * (TT(7, jp) - TT(7, c)) + J1 * dXi * (TT(8, ip) - TT(8, c)) +
+                     J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c)));
+      if (P.nmoist > 0 && P.moistSGS > 0) {
+        const float* M = Q.mtau;
+        F[SL_QV] = F[SL_QV] - (dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) +
+                               J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) + J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) +
+                               J3 * dZi * (M[2 * n + kp] - M[2 * n + c]));
+        if (P.nmoist > 1) {
+          const float* M1 = M + 3 * n;
+          F[SL_QL] = F[SL_QL] - (dXi * (M1[ip] - M1[c]) + dYi * (M1[n + jp] - M1[n + c]) +
+                                 J1 * dXi * (M1[2 * n + ip] - M1[2 * n + c]) + J2 * dYi * (M1[2 * n + jp] - M1[2 * n + c]) +
+                                 J3 * dZi * (M1[2 * n + kp] - M1[2 * n + c]));
+        }
+      }
+      // SGS TKE budget (cuda_sgstkeDevice.cu:155-397)
+      if (P.tke) {
+        const float ri = rinv(r0);
+        const float delta = powf(P.dX * P.dY * P.dZ * Dc, (float)(1.0 / 3.0));
+        const float lsc = Q.ls[c];
+        const float mec = w[SL_E][0];
+        float Fe = F[SL_E];
+        Fe = Fe + P.g / (w[4][0] * ri) * TT(8, c);
+        const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
+        const float ec = mec * ri;
+        Fe = Fe + (-ce * mec * powf(ec, 0.5f) / lsc);
+        const float* pr = cs + own;  // rho plane
+        auto G = [&](int s, int dir, int sgn) -> float {
+          // (rho phi)/rho at a neighbour: dir 0 = x (registers), 1 = y, 2 = z (shared plane)
+          if (dir == 0) return sgn > 0 ? w[s][1] * rinv(w[0][1]) : ps[s * PLANE + own] * rinv(ps[own]);
+          const int o = dir == 1 ? sgn * PK : sgn;
+          return cs[s * PLANE + own + o] * rinv(pr[o]);
+        };
+        const float dux = 0.5f * (dXi * (G(1, 0, 1) - G(1, 0, -1)));
+        const float duy = 0.5f * (dYi * (G(1, 1, 1) - G(1, 1, -1)));
+        const float duz = 0.5f * (J1 * dXi * (G(1, 0, 1) - G(1, 0, -1)) + J2 * dYi * (G(1, 1, 1) - G(1, 1, -1)) +
+                                  J3 * dZi * (G(1, 2, 1) - G(1, 2, -1)));
+        const float dvx = 0.5f * (dXi * (G(2, 0, 1) - G(2, 0, -1)));
+        const float dvy = 0.5f * (dYi * (G(2, 1, 1) - G(2, 1, -1)));
+        const float dvz = 0.5f * (J1 * dXi * (G(2, 0, 1) - G(2, 0, -1)) + J2 * dYi * (G(2, 1, 1) - G(2, 1, -1)) +
+                                  J3 * dZi * (G(2, 2, 1) - G(2, 2, -1)));
+        const float dwx = 0.5f * (dXi * (G(3, 0, 1) - G(3, 0, -1)));
+        const float dwy = 0.5f * (dYi * (G(3, 1, 1) - G(3, 1, -1)));
+        const float dwz = 0.5f * (J1 * dXi * (G(3, 0, 1) - G(3, 0, -1)) + J2 * dYi * (G(3, 1, 1) - G(3, 1, -1)) +
+                                  J3 * dZi * (G(3, 2, 1) - G(3, 2, -1)));
+        const float shear = (-TT(0, c) * dux) + (-TT(1, c) * duy) + (-TT(2, c) * duz) + (-TT(1, c) * dvx) +
+                            (-TT(4, c) * dvy) + (-TT(3, c) * dvz) + (-TT(2, c) * dwx) + (-TT(3, c) * dwy) +
+                            (-TT(5, c) * dwz);
+        Fe = Fe + shear;
+        const float* Gq = Q.tkeQ;
+        const long long im = c - si, jm = c - sj, km = c - 1;
+        const float tx_ = -(dXi * (Gq[ip] - Gq[im]));
+        const float ty_ = -(dYi * (Gq[n + jp] - Gq[n + jm]));
+        const float tz_ = -(J1 * dXi * (Gq[2 * n + ip] - Gq[2 * n + im]) + J2 * dYi * (Gq[2 * n + jp] - Gq[2 * n + jm]) +
+                            J3 * dZi * (Gq[2 * n + kp] - Gq[2 * n + km]));
+        Fe = Fe + (-(tx_ + ty_ + tz_));
+        F[SL_E] = Fe;
+      }
+#undef TT
+    }
+
+    // saturation adjustment (cuda_moistureDevice.cu:80-247)
+    if (mpStep && active) {
+      const float ri = rinv(r0);
+      const float mth = w[4][0];
+      const float thd = mth * ri;
+      const float prd = P.condBasePres == 1 ? powf(Q.thBS[c] * P.c1, P.cp_cv) : powf(mth * P.c1, P.cp_cv);
+      const float Td = thd * powf(prd / P.p0, P.R_cp);
+      float pvs;
+      const float Tc = fmaxf(-80.0f, (Td - 273.16f));
+      if (Td >= 273.15f) {
+        pvs = (6.11239921f + Tc * (0.443987641f + Tc * (0.142986287e-1f + Tc * (0.264847430e-3f + Tc * (0.302950461e-5f +
+              Tc * (0.206739458e-7f + Tc * (0.640689451e-10f + Tc * (-0.952447341e-13f + -0.976195544e-15f * Tc)))))))) * 100.0f;
+      } else {
+        pvs = (6.11147274f + Tc * (0.503160820f + Tc * (0.188439774e-1f + Tc * (0.420895665e-3f + Tc * (0.615021634e-5f +
+              Tc * (0.602588177e-7f + Tc * (0.385852041e-9f + Tc * (0.146898966e-11f + 0.252751365e-14f * Tc)))))))) * 100.0f;
+      }
+      pvs = fminf((0.99f * prd), pvs);
+      float ffor = 0.0f;
+      const float flim = w[SL_QL][0] * 1e-3f;
+      if (P.moistCond == 1) {
+        ffor = w[SL_QV][0] * 1e-3f - (pvs / (P.R_vapor * Td));
+      } else if (P.moistCond == 2) {
+        const float rv = w[SL_QV][0] * 1e-3f, rvs = pvs / (P.R_vapor * Td);
+        ffor = (rv - rvs) / (1.0f + (powf(P.L_v, 2.0f) * rvs * ri / (P.cp_gas * P.R_vapor * powf(Td, 2.0f))));
+      } else {
+        const float rv = w[SL_QV][0] * 1e-3f;
+        float rvs = pvs / (prd - pvs) / P.Rv_Rg;
+        rvs = rvs / ri;
+        ffor = (rv - rvs) / (1.0f + (powf(P.L_v, 2.0f) * rvs * ri / (P.cp_gas * P.R_vapor * powf(Td, 2.0f))));
+      }
+      float fc = fmaxf(ffor, 0.0f) - fmaxf(fminf(flim, -ffor), 0.0f);
+      fc = fc / P.condTscale;
+      F[SL_QV] = F[SL_QV] - fc * 1e3f;
+      F[SL_QL] = F[SL_QL] + fc * 1e3f;
+      const float prd2 = powf(mth * P.c1, P.cp_cv);
+      const float Td2 = thd * powf(prd2 / P.p0, P.R_cp);
+      F[4] = F[4] + ((thd * P.L_v) / (Td2 * P.cp_gas)) * fc;
+    }
+
+    if (active) {
+      if (MODE == MODE_FRHS) {
+        frhs[c] = F[0];
+        frhs[n + c] = F[1];
+        frhs[2 * n + c] = F[2];
+        frhs[3 * n + c] = F[3];
+        frhs[4 * n + c] = F[4];
+        if (P.ntke) frhs[5 * n + c] = F[SL_E];
+        if (P.nmoist > 0) frhs[(5 + P.ntke) * n + c] = F[SL_QV];
+        if (P.nmoist > 1) frhs[(6 + P.ntke) * n + c] = F[SL_QL];
+      } else {
+        // WS2002 RK3 commit (cuda_RKschemes.cu:113-157), rounding as in the cell kernel
+        auto rk = [&](float phi0, float Fv) -> float {
+          if (STAGE == 0) return (float)fma((1.0 / 3.0) * (double)P.dt, (double)Fv, (double)phi0);
+          if (STAGE == 1) return (float)fma(0.5 * (double)P.dt, (double)Fv, (double)phi0);
+          return __fmaf_rn(P.dt, Fv, phi0);
+        };
+        const bool same = (base == cur);
+        auto b0 = [&](int s, long long off) -> float { return same ? w[s][0] : base[off + c]; };
+        const float n0 = rk(b0(0, 0), F[0]);
+        const float n1 = rk(b0(1, n), F[1]);
+        const float n2 = rk(b0(2, 2 * n), F[2]);
+        const float n3 = rk(b0(3, 3 * n), F[3]);
+        const float n4 = rk(b0(4, 4 * n), F[4]);
+        const bool atBot = (k == P.kMin), atTop = (k == P.kMax - 1);
+        store_images(P, nxt, i, j, k, n0, 0, false);
+        store_images(P, nxt + n, i, j, k, n1, atBot ? 3 : 0, false);
+        store_images(P, nxt + 2 * n, i, j, k, n2, atBot ? 3 : 0, false);
+        store_images(P, nxt + 3 * n, i, j, k, n3, atBot ? 3 : 0, false);
+        store_images(P, nxt + 4 * n, i, j, k, n4, 0, false);
+        float nq0 = 0.0f;
+        if (P.ntke) {
+          const float ne = fmaxf(rk(b0(SL_E, 5 * n), F[SL_E]), 1e-10f);
+          store_images(P, nxt + 5 * n, i, j, k, ne, atBot ? 3 : 0, false);
+        }
+        if (P.nmoist > 0) {
+          const long long o = (5 + P.ntke) * n;
+          nq0 = fmaxf(rk(b0(SL_QV, o), F[SL_QV]), 0.0f);
+          store_images(P, nxt + o, i, j, k, nq0, atBot ? 3 : 0, atTop);
+          if (P.nmoist > 1) {
+            const float nq1 = fmaxf(rk(b0(SL_QL, o + n), F[SL_QL]), 0.0f);
+            store_images(P, nxt + o + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
+          }
+        }
+        float pn;
+        {
+          float rtm = n4;
+          if (P.nmoist > 0) rtm = (float)((double)n4 * (1.0 + (double)(P.Rv_Rg * nq0 / n0) * 1e-3));
+          pn = powf(rtm * P.c1, P.cp_cv) - Q.pBS[c];
+        }
+        store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
+      }
+    }
+
+    // plane i+1 into the other buffer: own values, contravariant velocities, ring tasks
+    float cyN = 0.0f, czN = 0.0f;
+    if (more) {
+#pragma unroll
+      for (int s = 0; s < 8; s++)
+        if (slot_on(P, s)) ns[s * PLANE + own] = w[s][1];
+      if (P.pgf) ns[SL_P * PLANE + own] = pc1;
+      const float dr = Dn / w[0][1];
+      cyN = dr * (w[2][1] + w[3][1] * J2n);
+      czN = dr * (w[3][1] * J3n);
+      float* v = ns + MSLOTS * PLANE;
+      v[(ty + 1) * MK + tx] = cyN;
+      v[T::CYN + ty * T::CZK + tx + 1] = czN;
+      if (rtKind) v[rtS] = rtKind == 1 ? contra(rD, rR, rM, rW, rJ) : (rD / rR) * (rW * rJ);
+    }
+    // shift the x window and the carried values
+#pragma unroll
+    for (int s = 0; s < 8; s++) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) w[s][d] = w[s][d + 1];
+      w[s][3] = nx[s];
+    }
+    pc1 = pnx;
+    cx0 = cxp1; upPrev = up;
+    Dc = Dn; Dn = Dnn; J1c = J1n; J1n = J1nn; J2c = J2n; J3c = J3n;
+    cyOwn = cyN; czOwn = czN;
+    float* const t = ps;
+    ps = cs; cs = ns; ns = t;
+    cp_async_wait_all();
+    __syncthreads();
+  }
+}
+
+}  // namespace fe

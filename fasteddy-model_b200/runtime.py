@@ -16,6 +16,11 @@ from . import build as _build
 
 _LIBS: dict[str, ctypes.CDLL] = {}
 
+SGS_NIN = 11      # FE_SGS_NIN
+SGS_NOUT = 9      # FE_SGS_NOUT
+KERNEL_CELL = 0   # FE_KERNEL_CELL
+KERNEL_MARCH = 1  # FE_KERNEL_MARCH
+
 c_float_p = ctypes.POINTER(ctypes.c_float)
 c_double_p = ctypes.POINTER(ctypes.c_double)
 
@@ -132,6 +137,8 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_count_nonfinite", ip, [vp, ctypes.POINTER(ctypes.c_longlong)]),
         ("fe_domain_means", ip, [vp, c_double_p]),
         ("fe_set_tiling", ip, [vp, ip, ip, ip]),
+        ("fe_set_stage_kernel", ip, [vp, ip, ip, ip]),
+        ("fe_get_stage_kernel", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_autotune", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_launch_count", ctypes.c_longlong, [vp]),
         ("fe_time_stage_kernel", ip, [vp, ip, fp]),
@@ -144,6 +151,22 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_ensemble_destroy", ip, [vp]),
         ("fe_last_error", ctypes.c_char_p, []),
         ("fe_noalloc_max_cells", ctypes.c_longlong, []),
+        ("fe_mlp_param_count", ctypes.c_longlong, []),
+        ("fe_mlp_create", ip, [ip, ctypes.c_ulonglong, ctypes.POINTER(vp)]),
+        ("fe_mlp_destroy", ip, [vp]),
+        ("fe_mlp_set_params", ip, [vp, fp]),
+        ("fe_mlp_get_params", ip, [vp, fp]),
+        ("fe_mlp_set_norm", ip, [vp, fp, fp, fp, fp]),
+        ("fe_mlp_get_norm", ip, [vp, fp, fp, fp, fp]),
+        ("fe_mlp_set_data", ip, [vp, fp, fp, ctypes.c_longlong, ctypes.c_ulonglong, ip]),
+        ("fe_mlp_gradient", ip, [vp, ctypes.c_longlong, ctypes.c_longlong, fp, c_double_p]),
+        ("fe_mlp_train", ip, [vp, ip, ctypes.c_longlong, ctypes.c_float, c_double_p]),
+        ("fe_mlp_predict", ip, [vp, fp, ctypes.c_longlong, fp]),
+        ("fe_mlp_time", ip, [vp, ip, ctypes.c_longlong, ip, fp]),
+        ("fe_mlp_check", ip, [vp]),
+        ("fe_set_sgs_mlp", ip, [vp, vp]),
+        ("fe_sgs_sample", ip, [vp, fp, fp, fp]),
+        ("fe_coarsen", ip, [vp, vp, fp]),
         ("fe_frhs_noalloc", ip, [ctypes.POINTER(FeConfig), ip, ctypes.c_float, ip, ctypes.POINTER(FeNoallocArgs), vp]),
         ("fe_noalloc_last_error", ctypes.c_char_p, []),
     ]:
@@ -375,10 +398,43 @@ class Domain:
     def set_tiling(self, tk: int, tj: int, ti: int) -> None:
         _check(self.e.fe_set_tiling(self.h, tk, tj, ti), "fe_set_tiling")
 
-    def autotune(self) -> tuple[int, int, int]:
+    def set_sgs_mlp(self, mlp: Optional["Mlp"]) -> None:
+        """Learned SGS stresses from `mlp` (None: the TKE closure)."""
+        _check(self.e.fe_set_sgs_mlp(self.h, mlp.h if mlp is not None else None), "fe_set_sgs_mlp")
+        self._mlp = mlp  # keep the network alive while the domain uses it
+
+    def sgs_sample(self) -> dict[str, np.ndarray]:
+        """Closure inputs X (cells x 11), stresses tau (cells x 9) and rho of the interior cells."""
+        cells = self.cfg.Nx * self.cfg.Ny * self.cfg.Nz
+        X = np.empty((cells, SGS_NIN), np.float32)
+        tau = np.empty((cells, SGS_NOUT), np.float32)
+        rho = np.empty(cells, np.float32)
+        _check(self.e.fe_sgs_sample(self.h, _fptr(X), _fptr(tau), _fptr(rho)), "fe_sgs_sample")
+        return {"X": X, "tau": tau, "rho": rho}
+
+    def coarsen_into(self, coarse: "Domain") -> np.ndarray:
+        """2x2x2 box filter of this (fine) state into `coarse`; returns the subfilter targets tau/rho."""
+        cells = coarse.cfg.Nx * coarse.cfg.Ny * coarse.cfg.Nz
+        tgt = np.empty((cells, SGS_NOUT), np.float32)
+        _check(self.e.fe_coarsen(self.h, coarse.h, _fptr(tgt)), "fe_coarsen")
+        return tgt
+
+    def set_stage_kernel(self, kind: str, tj: int = 0, ni: int = 0) -> None:
+        """kind 'march' (tiles of 32 levels x tj rows marching ni planes) or 'cell'."""
+        code = {"cell": KERNEL_CELL, "march": KERNEL_MARCH}[kind]
+        _check(self.e.fe_set_stage_kernel(self.h, code, tj, ni), "fe_set_stage_kernel")
+
+    def stage_kernel(self) -> tuple[str, int, int]:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(self.e.fe_get_stage_kernel(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "fe_get_stage_kernel")
+        return ("march" if a.value == KERNEL_MARCH else "cell"), b.value, c.value
+
+    def autotune(self) -> tuple[str, int, int]:
+        """Time the candidate stage-kernel forms/shapes, keep the fastest, return (kind, tj, ni|ti)."""
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(self.e.fe_autotune(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "fe_autotune")
-        return a.value, b.value, c.value
+        return self.stage_kernel()
 
     def time_stage_kernel(self, reps: int = 10) -> float:
         """Mean ms per launch of the fused dynamics stage kernel (CUDA events)."""
@@ -417,3 +473,75 @@ class Ensemble:
         if self.h:
             self.e.fe_ensemble_destroy(self.h)
             self.h = ctypes.c_void_p()
+
+
+class Mlp:
+    """The learned SGS closure (fe_mlp handle): parameters, training set, Adam, prediction."""
+
+    def __init__(self, device: int = 0, seed: int = 1) -> None:
+        self.libs = load()
+        self.e = self.libs["engine"]
+        h = ctypes.c_void_p()
+        _check(self.e.fe_mlp_create(device, seed, ctypes.byref(h)), "fe_mlp_create")
+        self.h = h
+        self.nparams = int(self.e.fe_mlp_param_count())
+
+    def close(self) -> None:
+        if self.h:
+            self.e.fe_mlp_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.nparams, np.float32)
+        _check(self.e.fe_mlp_get_params(self.h, _fptr(p)), "fe_mlp_get_params")
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparams
+        _check(self.e.fe_mlp_set_params(self.h, _fptr(p)), "fe_mlp_set_params")
+
+    def norm(self) -> dict[str, np.ndarray]:
+        a = [np.empty(SGS_NIN, np.float32), np.empty(SGS_NIN, np.float32), np.empty(SGS_NOUT, np.float32),
+             np.empty(SGS_NOUT, np.float32)]
+        _check(self.e.fe_mlp_get_norm(self.h, *(_fptr(x) for x in a)), "fe_mlp_get_norm")
+        return dict(zip(("in_mu", "in_sig", "out_mu", "out_sig"), a))
+
+    def set_norm(self, in_mu, in_sig, out_mu, out_sig) -> None:
+        a = [np.ascontiguousarray(x, np.float32) for x in (in_mu, in_sig, out_mu, out_sig)]
+        _check(self.e.fe_mlp_set_norm(self.h, *(_fptr(x) for x in a)), "fe_mlp_set_norm")
+
+    def set_data(self, X: np.ndarray, T: np.ndarray, seed: int = 7, fit_norm: bool = True) -> None:
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        assert X.shape[1] == SGS_NIN and T.shape == (X.shape[0], SGS_NOUT)
+        _check(self.e.fe_mlp_set_data(self.h, _fptr(X), _fptr(T), X.shape[0], seed, 1 if fit_norm else 0),
+               "fe_mlp_set_data")
+
+    def gradient(self, first: int, count: int) -> tuple[np.ndarray, float]:
+        g = np.empty(self.nparams, np.float32)
+        loss = ctypes.c_double()
+        _check(self.e.fe_mlp_gradient(self.h, first, count, _fptr(g), ctypes.byref(loss)), "fe_mlp_gradient")
+        return g, float(loss.value)
+
+    def train(self, steps: int, batch: int, lr: float) -> np.ndarray:
+        hist = np.zeros(steps, np.float64)
+        _check(self.e.fe_mlp_train(self.h, steps, batch, lr, hist.ctypes.data_as(c_double_p)), "fe_mlp_train")
+        return hist
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.empty((X.shape[0], SGS_NOUT), np.float32)
+        _check(self.e.fe_mlp_predict(self.h, _fptr(X), X.shape[0], _fptr(Y)), "fe_mlp_predict")
+        return Y
+
+    def time(self, train: bool, batch: int, reps: int = 10) -> float:
+        ms = ctypes.c_float()
+        _check(self.e.fe_mlp_time(self.h, 1 if train else 0, batch, reps, ctypes.byref(ms)), "fe_mlp_time")
+        return float(ms.value)

@@ -172,7 +172,16 @@ int fe_domain_means(fe_domain *d, double *means);
 /* Launch-shape control: threads per block along k and j of the stencil kernels and
  * the number of i-planes each thread block marches (0 = engine default). */
 int fe_set_tiling(fe_domain *d, int tk, int tj, int ti);
-/* Pick the tiling by timing the candidates (the autotuner); writes the choice. */
+/* Form of the fused stage kernel. FE_KERNEL_MARCH (the default): thread blocks of 32 levels
+ * by tj rows (4 or 8) march ni planes along i with the x stencil in registers and the y/z
+ * stencils in shared memory. FE_KERNEL_CELL: one thread per cell, tiled by fe_set_tiling.
+ * tj/ni <= 0 select the defaults (8, 64). */
+#define FE_KERNEL_CELL 0
+#define FE_KERNEL_MARCH 1
+int fe_set_stage_kernel(fe_domain *d, int kind, int tj, int ni);
+int fe_get_stage_kernel(const fe_domain *d, int *kind, int *tj, int *ni);
+/* Pick the stage-kernel form and launch shape by timing the candidates (the autotuner);
+ * tk/tj/ti receive the cell-kernel tiling, fe_get_stage_kernel the chosen form. */
 int fe_autotune(fe_domain *d, int *tk, int *tj, int *ti);
 /* Page-lock an existing host buffer for faster copies (cudaHostRegister) and undo it. */
 int fe_host_register(void *ptr, size_t bytes);
@@ -191,6 +200,58 @@ int fe_ensemble_advance(fe_ensemble *e, int nsteps);
 int fe_ensemble_sync(fe_ensemble *e);
 void *fe_ensemble_stream(fe_ensemble *e);
 int fe_ensemble_destroy(fe_ensemble *e);
+
+/* ======================================================= C. learned SGS closure */
+/* No counterpart in the reference: a small network that replaces the 9 stresses and heat
+ * fluxes of the TKE closure (cudaDevice_hydroCoreCalcTaus_PrognosticTKE_DeviatoricTerm,
+ * SRC/HYDRO_CORE/CUDA/cuda_sgsTurbDevice.cu:308-367) where the SGS divergence consumes them
+ * (cuda_hydroCoreDevice.cu:759-768); the TKE closure stays the fallback (no network set).
+ *
+ * Inputs per stress point (FE_SGS_NIN): the 9 velocity-gradient halves of the closure's
+ * staggered strain rates g11 g12 g13 g21 g22 g23 g31 g32 g33, the buoyancy frequency N^2 and
+ * the grid scale (dx dy dz D)^(1/3). Outputs (FE_SGS_NOUT): tau/rho in the closure's field
+ * order tau11 tau21 tau31 tau32 tau22 tau33 tauTH1 tauTH2 tauTH3. Network 11 -> 64 -> 64 ->
+ * 64 -> 9 with tanh, BF16 weights/activations on the tensor cores, FP32 accumulation;
+ * inputs standardised with (in_mu, in_sig), outputs tau/rho = out_mu + out_sig * y.
+ * Parameters (fe_mlp_param_count() FP32 values): W1[64][16] (columns 11..15 unused), b1[64],
+ * W2[64][64], b2[64], W3[64][64], b3[64], W4[16][64] (rows 9..15 unused), b4[16]. */
+#define FE_SGS_NIN 11
+#define FE_SGS_NOUT 9
+typedef struct fe_mlp fe_mlp;
+long long fe_mlp_param_count(void);
+int fe_mlp_create(int device, unsigned long long seed, fe_mlp **out); /* Glorot-uniform weights */
+int fe_mlp_destroy(fe_mlp *m);
+int fe_mlp_set_params(fe_mlp *m, const float *params); /* also resets the optimiser */
+int fe_mlp_get_params(fe_mlp *m, float *params);
+int fe_mlp_set_norm(fe_mlp *m, const float *in_mu, const float *in_sig, const float *out_mu, const float *out_sig);
+int fe_mlp_get_norm(fe_mlp *m, float *in_mu, float *in_sig, float *out_mu, float *out_sig);
+/* Training set: host arrays X[n][11] (inputs), T[n][9] (targets tau/rho); shuffled once with
+ * `seed`; fit_norm != 0 sets the standardisation to the set's means and deviations. */
+int fe_mlp_set_data(fe_mlp *m, const float *X, const float *T, long long n, unsigned long long seed, int fit_norm);
+/* Loss (mean over samples and outputs of the squared standardised error) and its gradient
+ * (fe_mlp_param_count() values) over samples [first, first+count) of the set, in set order. */
+int fe_mlp_gradient(fe_mlp *m, long long first, long long count, float *grad, double *loss);
+/* `steps` Adam steps (beta 0.9/0.999) on consecutive shuffled batches; loss_hist (may be NULL)
+ * receives the loss of every step. */
+int fe_mlp_train(fe_mlp *m, int steps, long long batch, float lr, double *loss_hist);
+/* Network outputs tau/rho for host inputs X[n][11] into Y[n][9]. */
+int fe_mlp_predict(fe_mlp *m, const float *X, long long n, float *Y);
+/* Mean device time (CUDA events) of a gradient evaluation (train != 0) or an inference over
+ * the first `batch` samples of the set. */
+int fe_mlp_time(fe_mlp *m, int train, long long batch, int reps, float *ms);
+/* Report (and clear) an expired tensor-core wait of the network's kernels. */
+int fe_mlp_check(fe_mlp *m);
+/* Use the network for the domain's SGS stresses (NULL: the TKE closure). */
+int fe_set_sgs_mlp(fe_domain *d, fe_mlp *m);
+/* Evaluate the domain's closure on its current state and sample every interior cell (row-
+ * major i, j, k): inputs X[cells][11], stresses tau[cells][9], density rho[cells] (any NULL
+ * is skipped). */
+int fe_sgs_sample(fe_domain *d, float *X, float *tau, float *rho);
+/* Coarse-grain the state of `fine` (2Nx x 2Ny x 2Nz over the same physical domain) by a
+ * 2x2x2 box filter into the state of `coarse`, and write the subfilter stresses and heat
+ * fluxes of every coarse interior cell divided by the filtered density (plus the fine
+ * model's own closure stresses) to tau_target[cells][9] (may be NULL). */
+int fe_coarsen(fe_domain *fine, fe_domain *coarse, float *tau_target);
 
 /* ---------------------------------------------- allocation-free tendency evaluation */
 /* No counterpart in the reference. For callers that cannot allocate device memory (pool

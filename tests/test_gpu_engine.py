@@ -32,9 +32,9 @@ CASES = {
 STATE_TOL = [1e-6, 1e-5, 2e-3, 2e-3, 1e-6]
 
 
-def _setup(fe, name):
+def _setup(fe, name, nx=None, ny=None, nz=None):
     c = CASES[name]
-    host = fe.cases.setup_host(c["case"], c["nx"], c["ny"], c["nz"], **c["kw"])
+    host = fe.cases.setup_host(c["case"], nx or c["nx"], ny or c["ny"], nz or c["nz"], **c["kw"])
     return host, host.inputs(), host.config()
 
 
@@ -115,20 +115,72 @@ def test_graph_replay_equals_step_by_step(fe):
 
 
 def test_tiling_and_autotune_do_not_change_results(fe):
+    """March shapes give identical bits; the cell kernel agrees to rounding."""
     host, inp, cfg = _setup(fe, "cbl_dry")
     a = fe.Domain(cfg)
     a.set_inputs(inp)
+    assert a.stage_kernel() == ("march", 8, 64)
     a.advance(3)
     b = fe.Domain(cfg)
     b.set_inputs(inp)
-    tk, tj, ti = b.autotune()
-    assert tk % 32 == 0 and tk * tj * ti <= 256
+    kind, tj, ni = b.autotune()
+    assert kind in ("march", "cell")
     b.set_inputs(inp)
-    b.set_tiling(32, 8, 1)
+    b.set_stage_kernel("march", 4, 5)
     b.advance(3)
     np.testing.assert_array_equal(interior(a.get_state()["hydroFlds"]), interior(b.get_state()["hydroFlds"]))
-    a.close()
-    b.close()
+    c = fe.Domain(cfg)
+    c.set_inputs(inp)
+    c.set_stage_kernel("cell")
+    c.set_tiling(32, 8, 1)
+    c.advance(3)
+    sa, sc = a.get_state(), c.get_state()
+    for f in range(5):
+        assert rel_l2(interior(sc["hydroFlds"][f]), interior(sa["hydroFlds"][f])) < 1e-6
+    for d in (a, b, c):
+        d.close()
+    host.cleanup()
+
+
+@pytest.mark.parametrize("case", ["cbl_dry", "moist_hill", "hill_dry"])
+def test_march_matches_cell_kernel_on_ragged_tiles(fe, case):
+    """Domain extents that are not multiples of the tile (k: 32, j: 8 or 4, i: ni) -- the
+    ring, halo and partial-tile paths of the march kernel -- against the cell kernel."""
+    host, inp, cfg = _setup(fe, case, nx=37, ny=13, nz=45)
+    ref = fe.Domain(cfg)
+    ref.set_inputs(inp)
+    ref.set_stage_kernel("cell")
+    for tj, ni in ((8, 16), (4, 7)):
+        d = fe.Domain(cfg)
+        d.set_inputs(inp)
+        d.set_stage_kernel("march", tj, ni)
+        for stage in (0, 2):
+            fr, fd = ref.build_frhs(stage), d.build_frhs(stage)
+            for key in ("hydroFrhs", "sgstkeFrhs", "moistFrhs"):
+                if fr.get(key) is None:
+                    continue
+                for f in range(fr[key].shape[0]):
+                    a_, b_ = interior(fd[key][f]), interior(fr[key][f])
+                    scale = max(np.abs(b_).max(), 1e-30)
+                    assert np.abs(a_ - b_).max() <= 2e-5 * scale, (key, f, stage, tj, ni)
+        d.advance(4)
+        ref2 = fe.Domain(cfg)
+        ref2.set_inputs(inp)
+        ref2.set_stage_kernel("cell")
+        ref2.advance(4)
+        s1, s2 = d.get_state(), ref2.get_state()
+        for key in ("hydroFlds", "sgstke", "moist"):
+            if s1.get(key) is None:
+                continue
+            for f in range(s1[key].shape[0]):
+                assert rel_l2(interior(s1[key][f]), interior(s2[key][f])) < 1e-6, (key, f, tj, ni)
+            # halo images and boundary copies too: the whole halo-inclusive arrays
+            np.testing.assert_allclose(s1[key], s2[key], rtol=1e-5, atol=1e-6 * float(np.abs(s2[key]).max()))
+        # p' = (c rho theta)^(cp/cv) - p_BS: a few ulps of rho theta move it by ~0.01 Pa
+        np.testing.assert_allclose(s1["pres"], s2["pres"], rtol=0, atol=0.1)
+        d.close()
+        ref2.close()
+    ref.close()
     host.cleanup()
 
 

@@ -1,0 +1,210 @@
+"""The learned SGS closure: the CPU oracle pinned against finite differences and torch's BF16
+rounding, the tensor-core forward/backward kernels against the oracle, training, the time-step
+hook, and what the trained network gains over the TKE closure on coarse-grained data.
+
+Tolerances. The oracle (bf16 mode) rounds to BF16 where the kernels do, so the remaining
+differences are FP32 accumulation order and tanhf against numpy's tanh, which can move a BF16
+activation by one unit (2^-8 relative) here and there: predictions are checked at relative
+L2 1e-2, gradients per parameter block at 2e-2 and the loss at 1e-3.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+
+
+def _norm(X, T):
+    return {"in_mu": X.mean(0).astype(np.float32), "in_sig": X.std(0).astype(np.float32),
+            "out_mu": T.mean(0).astype(np.float32), "out_sig": T.std(0).astype(np.float32)}
+
+
+def _synthetic(n, seed):
+    """Inputs shaped like the closure's (gradients ~1e-2 1/s, N^2 ~1e-4, Delta ~20 m) and a smooth
+    nonlinear target of them."""
+    rng = np.random.default_rng(seed)
+    X = np.empty((n, 11), np.float32)
+    X[:, :9] = rng.normal(0.0, 2e-2, (n, 9))
+    X[:, 9] = rng.normal(1e-4, 2e-4, n)
+    X[:, 10] = rng.uniform(15.0, 25.0, n)
+    g = X[:, :9].astype(np.float64)
+    S = np.sqrt((g ** 2).sum(1))
+    T = np.empty((n, 9), np.float32)
+    for q in range(9):
+        T[:, q] = -(0.17 * X[:, 10]) ** 2 * S * (g[:, q] + 0.3 * g[:, (q + 1) % 9]) * np.tanh(1.0 + 1e3 * X[:, 9])
+    return X, T
+
+
+# ---------------------------------------------------------------- CPU: the oracle itself
+def test_bf16_rounding_matches_torch():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.normal(0, 1, 20000), rng.normal(0, 1e-3, 2000), rng.normal(0, 1e4, 2000)]).astype(np.float32)
+    # exact ties: values half-way between two bf16 numbers
+    base = rng.normal(0, 1, 1000).astype(np.float32).view(np.uint32) & np.uint32(0xFFFF0000)
+    ties = (base | np.uint32(0x8000)).view(np.float32)
+    x = np.concatenate([x, ties])
+    ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy().astype(np.float64)
+    np.testing.assert_array_equal(mo.bf16(x), ref)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    X, T = _synthetic(96, 1)
+    nm = _norm(X, T)
+    p = mo.glorot(3)
+    p[mo.B1:mo.W2] = 0.05
+    p[mo.B4:mo.B4 + 9] = 0.1
+    _, g = mo.loss_and_grad(p, X, T, nm, exact=True)
+    rng = np.random.default_rng(5)
+    live = [i for i in range(mo.NPARAM) if not (
+        (i < mo.B1 and i % 16 >= 11) or (mo.W4 <= i < mo.B4 and (i - mo.W4) // 64 >= 9) or i >= mo.B4 + 9)]
+    idx = rng.choice(live, 60, replace=False)
+    h = 1e-6
+    for i in idx:
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (mo.loss_and_grad(pp, X, T, nm, exact=True)[0] - mo.loss_and_grad(pm, X, T, nm, exact=True)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])) + 1e-7 * np.abs(g).max(), (i, fd, g[i])
+
+
+def test_oracle_bf16_mode_tracks_exact_mode():
+    X, T = _synthetic(512, 2)
+    nm = _norm(X, T)
+    p = mo.glorot(4)
+    ye, yb = mo.predict(p, X, nm, exact=True), mo.predict(p, X, nm, exact=False)
+    assert np.linalg.norm(yb - ye) / np.linalg.norm(ye - nm["out_mu"]) < 3e-2
+    _, ge = mo.loss_and_grad(p, X, T, nm, exact=True)
+    _, gb = mo.loss_and_grad(p, X, T, nm, exact=False)
+    assert np.linalg.norm(gb - ge) / np.linalg.norm(ge) < 5e-2
+
+
+# ---------------------------------------------------------------- GPU: kernels vs the oracle
+def _blocks():
+    return {"W1": (mo.W1, mo.B1), "b1": (mo.B1, mo.W2), "W2": (mo.W2, mo.B2), "b2": (mo.B2, mo.W3),
+            "W3": (mo.W3, mo.B3), "b3": (mo.B3, mo.W4), "W4": (mo.W4, mo.B4), "b4": (mo.B4, mo.NPARAM)}
+
+
+@pytest.mark.gpu
+def test_tensor_core_forward_matches_oracle(fe):
+    X, T = _synthetic(3000, 11)
+    m = fe.Mlp(seed=21)
+    m.set_data(X, T)
+    nm = m.norm()
+    p = m.params().astype(np.float64)
+    # give the biases some weight too
+    rng = np.random.default_rng(2)
+    p[mo.B1:mo.W2] = rng.normal(0, 0.1, 64)
+    p[mo.B2:mo.W3] = rng.normal(0, 0.1, 64)
+    p[mo.B4:mo.B4 + 9] = rng.normal(0, 0.1, 9)
+    m.set_params(p.astype(np.float32))
+    y = m.predict(X)
+    ref = mo.predict(p.astype(np.float32).astype(np.float64), X, nm, exact=False)
+    scale = np.linalg.norm(ref - nm["out_mu"])
+    assert np.linalg.norm(y - ref) / scale < 1e-2
+    m.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("count", [1000, 128 * 148 * 2 + 77])
+def test_tensor_core_gradient_matches_oracle(fe, count):
+    """Gradients of all 8 parameter blocks, including tiles accumulated in tensor memory
+    across a CTA's tiles (the second size gives every CTA several tiles plus a ragged one)."""
+    X, T = _synthetic(count, 12)
+    m = fe.Mlp(seed=22)
+    m.set_data(X, T)
+    nm = m.norm()
+    p = m.params().astype(np.float64)
+    g, loss = m.gradient(0, count)
+    lref, gref = mo.loss_and_grad(p, X, T, nm, exact=False)
+    assert abs(loss - lref) <= 1e-3 * lref
+    for name, (a, b) in _blocks().items():
+        ref = gref[a:b]
+        assert np.linalg.norm(g[a:b] - ref) <= 2e-2 * np.linalg.norm(ref) + 1e-12, name
+    m.close()
+
+
+@pytest.mark.gpu
+def test_training_reduces_the_loss(fe):
+    X, T = _synthetic(40000, 13)
+    m = fe.Mlp(seed=23)
+    m.set_data(X, T)
+    _, l0 = m.gradient(0, 40000)
+    hist = m.train(300, 4096, 3e-3)
+    _, l1 = m.gradient(0, 40000)
+    assert np.all(np.isfinite(hist))
+    assert l1 < 0.1 * l0, (l0, l1)
+    m.close()
+
+
+# ---------------------------------------------------------------- GPU: in the model
+@pytest.mark.gpu
+def test_learned_stresses_feed_the_time_step(fe):
+    host = fe.cases.setup_host("cbl_dry", 24, 20, 16)
+    inp, cfg = host.inputs(), host.config()
+    d = fe.Domain(cfg)
+    d.set_inputs(inp)
+    d.advance(4)
+    samp = d.sgs_sample()
+    m = fe.Mlp(seed=24)
+    m.set_data(samp["X"], samp["tau"] / samp["rho"][:, None])
+    m.train(200, 4096, 3e-3)
+    d.set_sgs_mlp(m)
+    got = d.sgs_sample()
+    pred = m.predict(got["X"]) * got["rho"][:, None]
+    # the surface layer keeps tau31, tau32, tauTH3 at the first level
+    first = (np.arange(pred.shape[0]) % cfg.Nz) == 0
+    for q in range(9):
+        sel = ~first if q in (2, 3, 8) else slice(None)
+        np.testing.assert_allclose(got["tau"][sel, q], pred[sel, q], rtol=1e-5, atol=1e-6 * np.abs(pred[:, q]).max())
+    np.testing.assert_array_equal(got["tau"][first][:, [2, 3, 8]], samp["tau"][first][:, [2, 3, 8]])
+    d.advance(16)
+    assert d.nonfinite() == 0
+    d.close()
+    m.close()
+    host.cleanup()
+
+
+def _pair(fe, nxc, nyc, nzc):
+    """Host inputs of a coarse LES grid and of the 2x finer grid over the same domain."""
+    hf = fe.cases.setup_host("cbl_dry", 2 * nxc, 2 * nyc, 2 * nzc, dx=10.0, dz=5.0, dt=0.0125, seed=99)
+    fin, fcfg = hf.inputs(), hf.config()
+    hf.cleanup()
+    hc = fe.cases.setup_host("cbl_dry", nxc, nyc, nzc, dx=20.0, dz=10.0, dt=0.025, seed=99)
+    cin, ccfg = hc.inputs(), hc.config()
+    hc.cleanup()
+    return fin, fcfg, cin, ccfg
+
+
+@pytest.mark.gpu
+def test_trained_network_beats_the_tke_closure_a_priori(fe):
+    """Train on coarse-grained snapshots of a 2x finer run; on a later, held-out snapshot the
+    network's stresses and heat fluxes are closer to the true subfilter fluxes than the TKE
+    closure's evaluated on the same coarse fields."""
+    fin, fcfg, cin, ccfg = _pair(fe, 24, 24, 16)
+    fine = fe.Domain(fcfg)
+    fine.set_inputs(fin)
+    coarse = fe.Domain(ccfg)
+    coarse.set_inputs(cin)
+    Xs, Ts = [], []
+    for _ in range(3):
+        fine.advance(400)
+        tgt = fine.coarsen_into(coarse)
+        s = coarse.sgs_sample()
+        Xs.append(s["X"])
+        Ts.append(tgt)
+    fine.advance(200)
+    tgt = fine.coarsen_into(coarse)
+    s = coarse.sgs_sample()
+    m = fe.Mlp(seed=25)
+    m.set_data(np.concatenate(Xs), np.concatenate(Ts))
+    m.train(600, 4096, 2e-3)
+    pred = m.predict(s["X"])
+    tke = s["tau"] / s["rho"][:, None]
+    err_mlp = np.linalg.norm(pred - tgt) / np.linalg.norm(tgt)
+    err_tke = np.linalg.norm(tke - tgt) / np.linalg.norm(tgt)
+    print(f"a-priori relative L2 error: network {err_mlp:.3f}, TKE closure {err_tke:.3f}")
+    assert err_mlp < 0.8 * err_tke
+    for x in (fine, coarse, m):
+        x.close()

@@ -47,6 +47,22 @@ CASES = {
                       "dry CBL over a Gaussian hill, 1024x1024x256, dx=dy=20 m, dz=10 m"),
 }
 DEFAULT_CASE = "moist_hill_512"
+ENSEMBLE_CASE = "ensemble64"
+
+
+def ensemble_specs(n: int = 64, seed: int = 2024) -> list[tuple[int, int, int, float, float]]:
+    """Seeded member draws of the batched neutral-ABL ensemble: Nx, Ny in 64..192, Nz in 64..96,
+    U_g uniform in 5..15 m/s, z0 log-uniform in 0.01..0.5 m."""
+    import random
+
+    rng = random.Random(seed)
+    out = []
+    for _ in range(n):
+        nx, ny, nz = rng.randint(64, 192), rng.randint(64, 192), rng.randint(64, 96)
+        ug = rng.uniform(5.0, 15.0)
+        z0 = math.exp(rng.uniform(math.log(0.01), math.log(0.5)))
+        out.append((nx, ny, nz, round(ug, 3), round(z0, 4)))
+    return out
 
 
 def bytes_per_cell_stage(nprog: int, terrain: bool) -> int:
@@ -150,9 +166,66 @@ def measured_peak_gbs() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+def measured_peak_tflops() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+# tensor-core FLOPs the network kernels execute (tiles of 128 cells, padded widths 16/64/16)
+MLP_FWD_FLOP = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64 * 16)              # per cell
+MLP_TRAIN_FLOP = MLP_FWD_FLOP + 2 * (16 * 64 + 64 * 64 + 64 * 64) + 2 * 128 * (16 + 64 + 64 + 64)  # per sample
+
+
+def measure_learned(fe, dom, args, cells: int, stream, local: int) -> dict:
+    """The learned-SGS form of the same workload: the network (trained briefly on a strided
+    sample of this run's own closure stresses, so its outputs have the right size; the cost
+    does not depend on the weights) replaces the closure's stresses at every physics stage."""
+    import torch
+
+    m = fe.Mlp(device=local, seed=7)
+    every = max(1, cells // 524288)
+    s = dom.sgs_sample(every)
+    m.set_data(s["X"], s["tau"] / s["rho"][:, None])
+    nsamp = int(s["X"].shape[0])
+    del s
+    m.train(100, 4096, 2e-3)
+    dom.set_sgs_mlp(m)
+    dom.advance(args.warmup)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    dom.advance(args.steps, sync=False)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    nonfinite = dom.nonfinite()
+    dom.set_sgs_mlp(None)
+    peak, src = measured_peak_tflops()
+    inf_ms = m.time(False, nsamp, reps=10)
+    trn_ms = m.time(True, nsamp, reps=5)
+    m.close()
+    inf_tf = MLP_FWD_FLOP * nsamp / (inf_ms * 1e-3) / 1e12
+    trn_tf = MLP_TRAIN_FLOP * nsamp / (trn_ms * 1e-3) / 1e12
+    return {
+        "value": cells * args.steps / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / args.steps,
+        "nonfinite_cells": nonfinite,
+        "closure": "BF16 MLP 11-64-64-64-9 (tcgen05) replacing the TKE closure's 9 stresses at each physics stage",
+        "mlp_inference": {"cells_per_s": nsamp / (inf_ms * 1e-3), "tflops": inf_tf, "peak_tflops": peak,
+                          "frac": inf_tf / peak, "peak_source": src, "flop_per_cell": MLP_FWD_FLOP,
+                          "sample": f"{nsamp} cells, inputs/outputs FP32 in HBM"},
+        "mlp_training": {"samples_per_s": nsamp / (trn_ms * 1e-3), "tflops": trn_tf, "frac": trn_tf / peak,
+                         "flop_per_sample": MLP_TRAIN_FLOP},
+    }
+
+
 def profiled_traffic(case: str) -> float | None:
     """DRAM bytes per launch of the stage kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"k_stage_{case}.txt")
+    p = os.path.join(ROOT, "profiles", f"k_march_{case}.txt")
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -166,12 +239,15 @@ def profiled_traffic(case: str) -> float | None:
 def cpu_baseline(fe, case_key: str, seconds_target: float = 8.0) -> dict:
     """The FP64 C restatement of the path (oracle), single thread, on a sample of the
     workload: the same case on a horizontal subdomain with the full column."""
+    c = CASES[case_key]
+    return cpu_baseline_case(fe, c[0], c[3], seconds_target)
+
+
+def cpu_baseline_case(fe, case: str, nz: int, seconds_target: float = 8.0) -> dict:
     from oracle.pyoracle import Oracle
 
-    c = CASES[case_key]
-    nz = c[3]
     n = 32
-    host = fe.cases.setup_host(c[0], n, n, nz)
+    host = fe.cases.setup_host(case, n, n, nz)
     o = Oracle(host.config())
     o.set_inputs(host.inputs())
     t0 = time.perf_counter()
@@ -231,6 +307,7 @@ def run_ours(args, rank: int, world: int, local: int) -> dict | None:
     peak, peak_src = measured_peak_gbs()
     traffic = profiled_traffic(args.case)
     nonfinite = dom.nonfinite()
+    learned = measure_learned(fe, dom, args, cells, stream, local) if (cfg.turbulenceSelector and not args.no_learned) else None
     dom.close()
     # end to end through the drop-in C ABI with host buffers
     libs = fe.load()
@@ -271,14 +348,112 @@ def run_ours(args, rank: int, world: int, local: int) -> dict | None:
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "path": "cuda_timeIntCommence (drop-in C ABI), host buffers, one batch of K steps"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_stage (fused tendency + RK3 commit)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "k_march (fused tendency + RK3 commit, stage 2 of 3)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src, "bytes_per_cell_stage": bpc, "stage_kernel_ms": stage_ms},
         "clocks": clocks,
         "nonfinite_cells": nonfinite,
     }
+    if learned is not None:
+        line["learned_sgs"] = learned
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(fe, args.case)
+    return line
+
+
+# ---------------------------------------------------------------- batched ensemble
+def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
+    """64 uneven neutral-ABL members advanced together: every step of every member is one node
+    of one captured CUDA graph (members on parallel branches), launched once per 8 steps."""
+    import numpy as np
+    import torch
+
+    fe = importlib.import_module("fasteddy-model_b200")
+    device = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    specs = ensemble_specs()
+    doms, inputs, shapes = [], [], []
+    t_tune = time.perf_counter()
+    for i, (nx, ny, nz, ug, z0) in enumerate(specs):
+        host = fe.cases.setup_host("abl_neutral", nx, ny, nz, seed=1000 + i + 97 * rank, ug=ug, z0=z0)
+        inp, cfg = host.inputs(), host.config()
+        host.cleanup()
+        d = fe.Domain(cfg, device=local)
+        d.set_inputs(inp)
+        d.autotune()
+        doms.append(d)
+        inputs.append(inp)
+        shapes.append(d.stage_kernel())
+    t_tune = time.perf_counter() - t_tune
+    cells = sum(nx * ny * nz for nx, ny, nz, _, _ in specs)
+    ens = fe.Ensemble(doms)
+    ens.advance(8 * max(1, math.ceil(args.warmup / 8)))
+    stream = torch.cuda.ExternalStream(ens.stream(), device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = 8 * max(1, math.ceil(args.steps / 8))
+    launches0 = sum(d.launch_count() for d in doms)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        ens.advance(steps, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = sum(d.launch_count() for d in doms) - launches0
+    max_ms = max_over_ranks(ms, device)
+    value = whole_job_rate(cells, steps, max_ms / 1e3, world)
+    # stage kernels of every member, timed alone: algorithmic bytes over summed launch times
+    bpc = bytes_per_cell_stage(6, False)
+    stage_ms = sum(d.time_stage_kernel(reps=5) for d in doms)
+    achieved = bpc * cells / (stage_ms * 1e-3) / 1e9
+    peak, peak_src = measured_peak_gbs()
+    nonfinite = sum(d.nonfinite() for d in doms)
+    # end to end through the public API: upload every member's host state, K steps, download
+    barrier()
+    t0 = time.perf_counter()
+    for d, inp in zip(doms, inputs):
+        d.set_state(inp["hydroFlds"], inp.get("sgstke"), inp.get("moist"))
+    ens.advance(steps, sync=False)
+    outs = [d.get_state() for d in doms]
+    t1 = time.perf_counter()
+    barrier()
+    e2e_s = max_over_ranks(t1 - t0, device)
+    h2d = sum(inp["hydroFlds"].nbytes + (inp["sgstke"].nbytes if inp.get("sgstke") is not None else 0) for inp in inputs)
+    d2h = sum(sum(v.nbytes for v in o.values() if v is not None) for o in outs)
+    ens.close()
+    for d in doms:
+        d.close()
+    if rank != 0:
+        return None
+    kinds = {}
+    for k, tj, ni in shapes:
+        key = f"{k}:{tj}x{ni}"
+        kinds[key] = kinds.get(key, 0) + 1
+    line = {
+        "metric": "RK3 cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": steps,
+        "warmup": 8 * max(1, math.ceil(args.warmup / 8)), "ms_per_step": max_ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched ensemble of 64 neutral ABL members, Nx,Ny in 64..192, Nz in 64..96, "
+                               "U_g 5..15 m/s, z0 0.01..0.5 m (seeded), dx=dy=20 m, dz=10 m",
+                   "members": len(specs), "cells": cells, "parallelism": f"replicas{world}",
+                   "l2": f"state of all members {4 * 6 * cells / 1e9:.1f} GB >> 126 MB L2, no flush needed",
+                   "autotuned_shapes": kinds, "autotune_s": round(t_tune, 1)},
+        "e2e": {"value": whole_job_rate(cells, steps, e2e_s, world), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+                "path": "engine API: fe_set_state of every member, one ensemble advance, fe_get_state"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_march (all members, summed)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "bytes_per_cell_stage": bpc, "stage_kernel_ms_sum": stage_ms},
+        "clocks": clk.summary(),
+        "nonfinite_cells": nonfinite,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_case(fe, "abl_neutral", 80)
     return line
 
 
@@ -326,9 +501,10 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--case", choices=sorted(CASES), default=DEFAULT_CASE)
+    ap.add_argument("--case", choices=sorted(CASES) + [ENSEMBLE_CASE], default=DEFAULT_CASE)
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-SGS form")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
     if world > 1:
@@ -343,7 +519,12 @@ def main(argv=None) -> int:
             torch.cuda.set_device(local)
         dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
     try:
-        line = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world, local)
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        elif args.case == ENSEMBLE_CASE:
+            line = run_ensemble(args, rank, world, local)
+        else:
+            line = run_ours(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -57,6 +57,7 @@ struct Ptrs {
   float *ls;                   // SGS length scale
   float *mtau;                 // 3 per moisture species
   float *cd, *ch, *cq, *fricVel, *htFlux, *tskin, *invOblen, *z0m, *z0t, *qFlux, *qskin;
+  const float* delta;          // grid scale (dx dy dz D)^(1/3) per cell, or nullptr (evaluated inline)
   int *clockIt;                // simTime_it of the step being computed
   float *clockTime;            // simTime of the step being computed
 };
@@ -65,6 +66,13 @@ __device__ __forceinline__ float sgnf(float x) { return copysignf(1.0f, x); }
 
 // 1/rho with the reference's floor (rhoInv in cuda_hydroCoreDevice.cu:952-957)
 __device__ __forceinline__ float rinv(float r) { return 1.0f / fmaxf(r, 1e-6f); }
+
+// SGS grid scale (dx dy dz D)^(1/3) of cell c (cuda_sgstkeDevice.cu:96-151); constant in time, so
+// the engine evaluates it once per grid, with this same expression, into Q.delta.
+__device__ __forceinline__ float grid_scale_of(const Phys& P, float D) { return powf(P.dX * P.dY * P.dZ * D, (float)(1.0 / 3.0)); }
+__device__ __forceinline__ float grid_scale(const Phys& P, const Ptrs& Q, long long c) {
+  return Q.delta ? Q.delta[c] : grid_scale_of(P, Q.D[c]);
+}
 
 // ---------------------------------------------------------------- boundary values
 // Value of field `f` in the vertical halo cell (column source cell `src` = interior
@@ -98,37 +106,62 @@ __device__ __forceinline__ float pert_pressure(const Phys& P, const float* __res
   return powf(rtm * P.c1, P.cp_cv) - pBS[t];
 }
 
+// Perturbation pressure of the bottom halo level (k = 0) of a column after a commit: rho and
+// rho theta there are the base state, q_v the bottom copy of the first level (the reference
+// recomputes this level every stage, cuda_pressureDevice.cu:53-113; no stencil reads it).
+__device__ __forceinline__ float level0_pressure(const Phys& P, const Ptrs& Q, long long c0, int nmoist, float qv) {
+  float rt = Q.thBS[c0];
+  if (nmoist > 0) rt = (float)((double)rt * (1.0 + (double)(P.Rv_Rg * qv / Q.rhoBS[c0]) * 1e-3));
+  return powf(rt * P.c1, P.cp_cv) - Q.pBS[c0];
+}
+
 // ---------------------------------------------------------------- advection
+// The flux and velocity helpers spell out every rounding (__fmaf_rn/__fmul_rn/__fadd_rn):
+// the same face is evaluated by more than one inlined copy (a marching thread block's first
+// plane and its loop), and explicit roundings make every copy produce the same bits, so
+// results do not depend on the launch shape.
+//
 // 5th/6th-order hybrid flux across the face between cells s0 (lower) and s1 (upper):
 // arguments are the stencil m2,m1,z0,p1,p2,p3 relative to the lower cell
-// (cuda_advectionDevice.cu:365-376).
+// (cuda_advectionDevice.cu:365-376): (37(p1+z0) - 8(p2+m1) + (p3+m2)
+//  - bfac sgn(vel) ((p3-m2) - 5(p2-m1) + 10(p1-z0))) / 60.
 __device__ __forceinline__ float hyb56_flux(float m2, float m1, float z0, float p1, float p2, float p3, float vel,
                                             float bfac) {
   const float sixtieth = 1.0f / 60.0f;
-  return sixtieth * (37.0f * (p1 + z0) - 8.0f * (p2 + m1) + (p3 + m2) -
-                     bfac * sgnf(vel) * ((p3 - m2) - 5.0f * (p2 - m1) + 10.0f * (p1 - z0)));
+  const float a = __fadd_rn(p1, z0), b = __fadd_rn(p2, m1), c = __fadd_rn(p3, m2);
+  const float d = __fsub_rn(p3, m2), e = __fsub_rn(p2, m1), f = __fsub_rn(p1, z0);
+  const float cen = __fadd_rn(__fmaf_rn(37.0f, a, __fmul_rn(-8.0f, b)), c);
+  const float upw = __fmaf_rn(10.0f, f, __fmaf_rn(-5.0f, e, d));
+  const float sb = __fmul_rn(bfac, sgnf(vel));
+  return __fmul_rn(sixtieth, __fmaf_rn(-sb, upw, cen));
 }
 
 // WENO5 face value from the upwind side, stencil a..e (cuda_advectionDevice.cu:626-926).
 // The squares of the smoothness indicators are products (the reference spells them
-// powf(x, 2.0)); the three normalised weights share one reciprocal of their sum.
+// powf(x, 2.0)). The normalised weights w_k = (g_k/q_k^2) / sum_j (g_j/q_j^2), q = tol + beta,
+// are formed with one division: multiplying through by (q1 q2 q3)^2 gives w_k ~ g_k (q_i q_j)^2
+// (i, j != k). With q >= tol = 1e-6 the products stay normal, and they stay finite while the
+// smoothness indicators are below 1e9 (jumps of the advected field below ~3e4 across a cell).
 __device__ __forceinline__ float weno5_face(float a, float b, float c, float d, float e) {
   const float g1 = 1.0f / 10.0f, g2 = 3.0f / 5.0f, g3 = 3.0f / 10.0f, tol = 1e-6f;
-  const float f1 = (1.0f / 3.0f) * a - (7.0f / 6.0f) * b + (11.0f / 6.0f) * c;
-  const float f2 = -(1.0f / 6.0f) * b + (5.0f / 6.0f) * c + (1.0f / 3.0f) * d;
-  const float f3 = (1.0f / 3.0f) * c + (5.0f / 6.0f) * d - (1.0f / 6.0f) * e;
-  const float s1 = a - 2.0f * b + c, t1 = a - 4.0f * b + 3.0f * c;
-  const float s2 = b - 2.0f * c + d, t2 = b - d;
-  const float s3 = c - 2.0f * d + e, t3 = 3.0f * c - 4.0f * d + e;
-  const float b1 = (13.0f / 12.0f) * (s1 * s1) + (1.0f / 4.0f) * (t1 * t1);
-  const float b2 = (13.0f / 12.0f) * (s2 * s2) + (1.0f / 4.0f) * (t2 * t2);
-  const float b3 = (13.0f / 12.0f) * (s3 * s3) + (1.0f / 4.0f) * (t3 * t3);
-  const float q1 = tol + b1, q2 = tol + b2, q3 = tol + b3;
-  const float w1 = g1 / (q1 * q1);
-  const float w2 = g2 / (q2 * q2);
-  const float w3 = g3 / (q3 * q3);
-  const float inv = 1.0f / (w1 + w2 + w3);
-  return (w1 * inv) * f1 + (w2 * inv) * f2 + (w3 * inv) * f3;
+  const float k13 = 1.0f / 3.0f, k76 = 7.0f / 6.0f, k116 = 11.0f / 6.0f, k16 = 1.0f / 6.0f, k56 = 5.0f / 6.0f;
+  const float f1 = __fmaf_rn(k116, c, __fmaf_rn(-k76, b, __fmul_rn(k13, a)));
+  const float f2 = __fmaf_rn(k13, d, __fmaf_rn(k56, c, __fmul_rn(-k16, b)));
+  const float f3 = __fmaf_rn(-k16, e, __fmaf_rn(k56, d, __fmul_rn(k13, c)));
+  const float s1 = __fadd_rn(__fmaf_rn(-2.0f, b, a), c), t1 = __fmaf_rn(3.0f, c, __fmaf_rn(-4.0f, b, a));
+  const float s2 = __fadd_rn(__fmaf_rn(-2.0f, c, b), d), t2 = __fsub_rn(b, d);
+  const float s3 = __fadd_rn(__fmaf_rn(-2.0f, d, c), e), t3 = __fadd_rn(__fmaf_rn(-4.0f, d, __fmul_rn(3.0f, c)), e);
+  const float k1312 = 13.0f / 12.0f, k14 = 1.0f / 4.0f;
+  const float b1 = __fmaf_rn(k14, __fmul_rn(t1, t1), __fmul_rn(k1312, __fmul_rn(s1, s1)));
+  const float b2 = __fmaf_rn(k14, __fmul_rn(t2, t2), __fmul_rn(k1312, __fmul_rn(s2, s2)));
+  const float b3 = __fmaf_rn(k14, __fmul_rn(t3, t3), __fmul_rn(k1312, __fmul_rn(s3, s3)));
+  const float q1 = __fadd_rn(tol, b1), q2 = __fadd_rn(tol, b2), q3 = __fadd_rn(tol, b3);
+  const float a1 = __fmul_rn(q2, q3), a2 = __fmul_rn(q1, q3), a3 = __fmul_rn(q1, q2);
+  const float u1 = __fmul_rn(g1, __fmul_rn(a1, a1));
+  const float u2 = __fmul_rn(g2, __fmul_rn(a2, a2));
+  const float u3 = __fmul_rn(g3, __fmul_rn(a3, a3));
+  const float num = __fmaf_rn(u3, f3, __fmaf_rn(u2, f2, __fmul_rn(u1, f1)));
+  return __fdiv_rn(num, __fadd_rn(__fadd_rn(u1, u2), u3));
 }
 
 // The reference blends both one-sided values with weights 0.5(1 +- sign(u)), which are
@@ -143,6 +176,15 @@ struct FaceVel {
 };
 
 // Contravariant momentum term (D/rho)*(m + w*J) of one cell, as in the reference sum.
-__device__ __forceinline__ float contra(float D, float r, float m, float w, float J) { return (D / r) * (m + w * J); }
+__device__ __forceinline__ float contra(float D, float r, float m, float w, float J) {
+  return __fmul_rn(__fdiv_rn(D, r), __fmaf_rn(w, J, m));
+}
+// The same with D/rho already formed (one division shared by the three directions).
+__device__ __forceinline__ float contra_dr(float dr, float m, float w, float J) { return __fmul_rn(dr, __fmaf_rn(w, J, m)); }
+__device__ __forceinline__ float contra_z_dr(float dr, float w, float J) { return __fmul_rn(dr, __fmul_rn(w, J)); }
+// Its vertical form (D/rho)*(w*J33).
+__device__ __forceinline__ float contra_z(float D, float r, float w, float J) {
+  return __fmul_rn(__fdiv_rn(D, r), __fmul_rn(w, J));
+}
 
 }  // namespace fe

@@ -285,7 +285,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
     if (rc == FE_OK) rc = dev_alloc(d, &d->pr[b], n);
   }
   const size_t nscr = (size_t)(9 + 3 + 1 + 3 * std::max(P.nmoist, 1));
-  if (rc == FE_OK) rc = dev_alloc(d, &d->grid, n * 6);
+  if (rc == FE_OK) rc = dev_alloc(d, &d->grid, n * 7);
   if (rc == FE_OK) rc = dev_alloc(d, &d->base, n * 3);
   if (rc == FE_OK) rc = dev_alloc(d, &d->scratch, n * nscr);
   if (rc == FE_OK) rc = dev_alloc(d, &d->surf, n2 * 11);
@@ -306,6 +306,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   Q.J33 = d->grid + 3 * n;
   Q.D = d->grid + 4 * n;
   Q.invD = d->grid + 5 * n;
+  Q.delta = d->grid + 6 * n;
   Q.rhoBS = d->base;
   Q.thBS = d->base + n;
   Q.pBS = d->base + 2 * n;
@@ -378,6 +379,9 @@ extern "C" int fe_set_grid(fe_domain* d, const float* zPos, const float* J31, co
   if (!rc) rc = h2d(d, d->grid + 4 * n, D_Jac, n);
   if (!rc) rc = h2d(d, d->grid + 5 * n, invD_Jac, n);
   if (rc) return rc;
+  fe::k_delta<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->P, (long long)n, d->grid + 4 * n, d->grid + 6 * n);
+  d->launches++;
+  CU(cudaGetLastError());
   CU(cudaStreamSynchronize(d->stream));
   d->haveGrid = true;
   return FE_OK;
@@ -414,6 +418,69 @@ extern "C" int fe_set_surface(fe_domain* d, const float* z0m, const float* z0t, 
   if (rc) return rc;
   CU(cudaStreamSynchronize(d->stream));
   return FE_OK;
+}
+
+static int finish_state(fe_domain* d);
+
+// ------------------------------------------------------------------ checkpoint / resume
+// A checkpoint holds everything a step reads that a step also changes: the prognostic state A,
+// the 11 surface planes (the surface layer starts from the previous drag, friction velocity,
+// Obukhov length, fluxes and skin values) and the clock. Scratch, the intermediate stage
+// states and the perturbation pressure are rebuilt from these on load, so a resumed run repeats
+// the continuous one bit for bit.
+namespace {
+struct CkptHeader {
+  char magic[8];
+  int version, Nx, Ny, Nz, nf, simIt;
+  float simTime;
+  int pad[8];
+};
+const char kCkptMagic[8] = {'F', 'E', 'B', '2', '0', '0', 'C', 'K'};
+}  // namespace
+
+extern "C" size_t fe_checkpoint_bytes(const fe_domain* d) {
+  if (!d) return 0;
+  return sizeof(CkptHeader) + sizeof(float) * ((size_t)d->P.nf * (size_t)d->P.n + 11 * (size_t)d->P.n2);
+}
+
+extern "C" int fe_checkpoint_save(fe_domain* d, void* buf, size_t bytes) {
+  if (!d || !buf) return set_err(FE_ERR_ARG, "NULL argument");
+  if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
+  if (bytes < fe_checkpoint_bytes(d)) return set_err(FE_ERR_ARG, "checkpoint buffer too small");
+  CU(cudaSetDevice(d->device));
+  CU(cudaStreamSynchronize(d->stream));
+  CkptHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, kCkptMagic, 8);
+  h.version = 1; h.Nx = d->P.Nx; h.Ny = d->P.Ny; h.Nz = d->P.Nz; h.nf = d->P.nf;
+  h.simIt = d->simIt; h.simTime = d->simTime;
+  std::memcpy(buf, &h, sizeof(h));
+  float* f = reinterpret_cast<float*>(static_cast<char*>(buf) + sizeof(h));
+  const size_t ns = (size_t)d->P.nf * (size_t)d->P.n, n2 = 11 * (size_t)d->P.n2;
+  CU(cudaMemcpyAsync(f, d->st[0], ns * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+  CU(cudaMemcpyAsync(f + ns, d->surf, n2 * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_checkpoint_load(fe_domain* d, const void* buf, size_t bytes) {
+  if (!d || !buf) return set_err(FE_ERR_ARG, "NULL argument");
+  if (!d->haveGrid || !d->haveBase) return set_err(FE_ERR_STATE, "set the grid and base state before loading");
+  if (bytes < sizeof(CkptHeader)) return set_err(FE_ERR_ARG, "checkpoint too short");
+  CkptHeader h;
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1) return set_err(FE_ERR_ARG, "not a checkpoint of this engine");
+  if (h.Nx != d->P.Nx || h.Ny != d->P.Ny || h.Nz != d->P.Nz || h.nf != d->P.nf)
+    return set_err(FE_ERR_ARG, "checkpoint of a different domain shape or field set");
+  if (bytes < fe_checkpoint_bytes(d)) return set_err(FE_ERR_ARG, "checkpoint too short");
+  CU(cudaSetDevice(d->device));
+  const float* f = reinterpret_cast<const float*>(static_cast<const char*>(buf) + sizeof(h));
+  const size_t ns = (size_t)d->P.nf * (size_t)d->P.n, n2 = 11 * (size_t)d->P.n2;
+  CU(cudaMemcpyAsync(d->st[0], f, ns * sizeof(float), cudaMemcpyHostToDevice, d->stream));
+  CU(cudaMemcpyAsync(d->surf, f + ns, n2 * sizeof(float), cudaMemcpyHostToDevice, d->stream));
+  int rc = finish_state(d);
+  if (rc) return rc;
+  return fe_set_clock(d, h.simTime, h.simIt);
 }
 
 extern "C" int fe_set_clock(fe_domain* d, float simTime, int simTime_it) {
@@ -480,9 +547,11 @@ static dim3 stage_grid(const fe_domain* d) {
   const Phys& P = d->P;
   return dim3((P.Nz + d->tk - 1) / d->tk, (P.Ny + d->tj - 1) / d->tj, (P.Nx + d->ti - 1) / d->ti);
 }
-static dim3 turb_grid(const fe_domain* d) {
+// Last-stage SGS physics on the +1 ring (k_turb_ov: warps of 31 output levels plus the one below).
+static void launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
   const Phys& P = d->P;
-  return dim3((P.Nz + 2 + d->tk - 1) / d->tk, (P.Ny + 2 + d->tj - 1) / d->tj, (P.Nx + 2 + d->ti - 1) / d->ti);
+  const dim3 g((P.Nz + 2 + 30) / 31, (P.Ny + 2 + 3) / 4, (P.Nx + 2 + 1) / 2);
+  fe::k_turb_ov<<<g, dim3(32, 4, 2), 0, s>>>(P, d->Q, st, stage);
 }
 
 static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }
@@ -491,11 +560,14 @@ static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK
 // default at 8 rows); set on the current device before any launch or capture.
 template <int STAGE, int MODE>
 static cudaError_t march_attrs_one() {
-  cudaError_t e = cudaFuncSetAttribute(fe::k_march<STAGE, MODE, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       fe::MarchTile<8>::SMEM_BYTES);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fe::k_march<STAGE, MODE, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             fe::MarchTile<4>::SMEM_BYTES);
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f, int bytes) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  };
+  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_ANY>, fe::MarchTile<8>::SMEM_BYTES);
+  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_DRY>, fe::MarchTile<8>::SMEM_BYTES);
+  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST>, fe::MarchTile<8>::SMEM_BYTES);
+  set((const void*)fe::k_march<STAGE, MODE, 4, fe::FL_ANY>, fe::MarchTile<4>::SMEM_BYTES);
   return e;
 }
 static int march_attrs() {
@@ -509,21 +581,39 @@ static int march_attrs() {
   return FE_OK;
 }
 
+// Flavour of the march kernel that matches the configuration (fe_march.cuh).
+static int march_flavor(const Phys& P) {
+  if (P.pgf && P.tke && P.ntke == 1 && P.advSel == 3 && P.tkeAdvSel == 3) {
+    if (P.nmoist == 0) return fe::FL_DRY;
+    if (P.nmoist == 2 && P.qvAdvSel == 3) return fe::FL_MOIST;
+  }
+  return fe::FL_ANY;
+}
+
+template <int STAGE, int MODE, int TJ, int FL>
+static void launch_march(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
+                         const float* pcur, float* pnxt, float* frhs) {
+  const Phys& P = d->P;
+  const int ni = d->mni;
+  dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + TJ - 1) / TJ, (P.Nx + ni - 1) / ni);
+  fe::k_march<STAGE, MODE, TJ, FL><<<g, dim3(fe::MK, TJ), fe::MarchTile<TJ>::SMEM_BYTES, s>>>(P, d->Q, cur, base, nxt,
+                                                                                              pcur, pnxt, frhs, ni);
+}
+
 // Launch the fused stage kernel of stage STAGE in the domain's chosen form.
 template <int STAGE, int MODE>
 static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
                          const float* pcur, float* pnxt, float* frhs) {
   const Phys& P = d->P;
   if (d->kind == FE_KERNEL_MARCH) {
-    const int ni = d->mni;
     if (d->mtj == 4) {
-      dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + 3) / 4, (P.Nx + ni - 1) / ni);
-      fe::k_march<STAGE, MODE, 4><<<g, dim3(fe::MK, 4), fe::MarchTile<4>::SMEM_BYTES, s>>>(P, d->Q, cur, base, nxt, pcur,
-                                                                                        pnxt, frhs, ni);
+      launch_march<STAGE, MODE, 4, fe::FL_ANY>(d, s, cur, base, nxt, pcur, pnxt, frhs);
     } else {
-      dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + 7) / 8, (P.Nx + ni - 1) / ni);
-      fe::k_march<STAGE, MODE, 8><<<g, dim3(fe::MK, 8), fe::MarchTile<8>::SMEM_BYTES, s>>>(P, d->Q, cur, base, nxt, pcur,
-                                                                                        pnxt, frhs, ni);
+      switch (march_flavor(P)) {
+        case fe::FL_DRY: launch_march<STAGE, MODE, 8, fe::FL_DRY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
+        case fe::FL_MOIST: launch_march<STAGE, MODE, 8, fe::FL_MOIST>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
+        default: launch_march<STAGE, MODE, 8, fe::FL_ANY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
+      }
     }
   } else {
     fe::k_stage<STAGE, MODE><<<stage_grid(d), dim3(d->tk, d->tj, d->ti), 0, s>>>(P, d->Q, cur, base, nxt, pcur, pnxt, frhs);
@@ -534,24 +624,23 @@ static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, c
 static void enqueue_step(fe_domain* d, cudaStream_t s) {
   const Phys& P = d->P;
   const Ptrs& Q = d->Q;
-  dim3 blk(d->tk, d->tj, d->ti), gt = turb_grid(d);
   float *A = d->st[0], *B = d->st[1], *C = d->st[2];
   const bool physPrep = (P.turb || P.surf > 0);
   const bool learned = d->mlp && P.turb;
   if (physPrep && stage_has_physics(d, 0)) {
-    fe::k_turb<<<gt, blk, 0, s>>>(P, Q, A, 0);
+    launch_turb(d, s, A, 0);
     d->launches++;
     if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, A, s); d->launches++; }
   }
   launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
   if (physPrep && stage_has_physics(d, 1)) {
-    fe::k_turb<<<gt, blk, 0, s>>>(P, Q, B, 1);
+    launch_turb(d, s, B, 1);
     d->launches++;
     if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, B, s); d->launches++; }
   }
   launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
   if (physPrep && stage_has_physics(d, 2)) {
-    fe::k_turb<<<gt, blk, 0, s>>>(P, Q, C, 2);
+    launch_turb(d, s, C, 2);
     d->launches++;
     if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, C, s); d->launches++; }
   }
@@ -669,10 +758,9 @@ extern "C" int fe_build_frhs(fe_domain* d, int stage) {
     int rc = dev_alloc(d, &d->frhs, (size_t)P.n * P.nf);
     if (rc) return rc;
   }
-  dim3 blk(d->tk, d->tj, d->ti);
   float* A = d->st[0];
   if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
-    fe::k_turb<<<turb_grid(d), blk, 0, d->stream>>>(P, d->Q, A, stage);
+    launch_turb(d, d->stream, A, stage);
     d->launches++;
     if (d->mlp && P.turb) {
       CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
@@ -845,21 +933,22 @@ extern "C" int fe_host_unregister(void* ptr) {
 
 // ------------------------------------------------------------------ learned SGS closure: data
 namespace fe {
-// inputs, closure stresses and density of every interior cell (row-major i, j, k)
-__global__ void k_sgs_sample(Phys P, Ptrs Q, const float* __restrict__ st, float* __restrict__ X, float* __restrict__ tau,
-                             float* __restrict__ rho) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// inputs, closure stresses and density of every `every`-th interior cell (row-major i, j, k)
+__global__ void k_sgs_sample(Phys P, Ptrs Q, const float* __restrict__ st, long long every, float* __restrict__ X,
+                             float* __restrict__ tau, float* __restrict__ rho) {
+  const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long cells = (long long)P.Nx * P.Ny * P.Nz;
+  const long long t = s * every;
   if (t >= cells) return;
   const int k = (int)(t % P.Nz), j = (int)((t / P.Nz) % P.Ny), i = (int)(t / ((long long)P.Nz * P.Ny));
   const long long c = (long long)(i + P.iMin) * P.si + (long long)(j + P.jMin) * P.sj + (k + P.kMin);
   float x[SGS_NIN];
   sgs_inputs(P, Q, st, c, x);
   if (X)
-    for (int q = 0; q < SGS_NIN; q++) X[t * SGS_NIN + q] = x[q];
+    for (int q = 0; q < SGS_NIN; q++) X[s * SGS_NIN + q] = x[q];
   if (tau)
-    for (int q = 0; q < SGS_NOUT; q++) tau[t * SGS_NOUT + q] = Q.tau[q * P.n + c];
-  if (rho) rho[t] = st[c];
+    for (int q = 0; q < SGS_NOUT; q++) tau[s * SGS_NOUT + q] = Q.tau[q * P.n + c];
+  if (rho) rho[s] = st[c];
 }
 
 // 2x2x2 box filter (flux form, Favre averages) of a fine state onto a coarse interior, and the
@@ -921,17 +1010,17 @@ extern "C" int fe_set_sgs_mlp(fe_domain* d, fe_mlp* m) {
   return FE_OK;
 }
 
-// Evaluate the closure (TKE, or the network when set) on the current state and sample the
-// interior cells: inputs X (cells x 11), stresses tau (cells x 9), density rho (cells).
-extern "C" int fe_sgs_sample(fe_domain* d, float* X, float* tau, float* rho) {
-  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+// Evaluate the closure (TKE, or the network when set) on the current state and sample every
+// `every`-th interior cell: inputs X (samples x 11), stresses tau (samples x 9), density rho.
+extern "C" int fe_sgs_sample(fe_domain* d, long long every, float* X, float* tau, float* rho) {
+  if (!d || every < 1) return set_err(FE_ERR_ARG, "bad argument");
   if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
   if (!d->P.turb) return set_err(FE_ERR_CONFIG, "no SGS closure configured");
   CU(cudaSetDevice(d->device));
   const Phys& P = d->P;
-  const long long cells = (long long)P.Nx * P.Ny * P.Nz;
+  const long long cells = ((long long)P.Nx * P.Ny * P.Nz + every - 1) / every;
   float* A = d->st[0];
-  fe::k_turb<<<turb_grid(d), dim3(d->tk, d->tj, d->ti), 0, d->stream>>>(P, d->Q, A, 2);
+  launch_turb(d, d->stream, A, 2);
   d->launches++;
   if (d->mlp) {
     CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
@@ -942,7 +1031,7 @@ extern "C" int fe_sgs_sample(fe_domain* d, float* X, float* tau, float* rho) {
   if (e == cudaSuccess) e = cudaMalloc(&dT, sizeof(float) * cells * fe::SGS_NOUT);
   if (e == cudaSuccess) e = cudaMalloc(&dR, sizeof(float) * cells);
   if (e == cudaSuccess) {
-    fe::k_sgs_sample<<<blocks1d(cells, 256), 256, 0, d->stream>>>(P, d->Q, A, dX, dT, dR);
+    fe::k_sgs_sample<<<blocks1d(cells, 256), 256, 0, d->stream>>>(P, d->Q, A, every, dX, dT, dR);
     d->launches++;
     e = cudaGetLastError();
   }
@@ -971,7 +1060,7 @@ extern "C" int fe_coarsen(fe_domain* fine, fe_domain* coarse, float* tau_target)
   if (!Pf.turb) return set_err(FE_ERR_CONFIG, "the fine domain needs an SGS closure");
   CU(cudaSetDevice(fine->device));
   // the fine model's own subgrid stresses of its current state
-  fe::k_turb<<<turb_grid(fine), dim3(fine->tk, fine->tj, fine->ti), 0, fine->stream>>>(Pf, fine->Q, fine->st[0], 2);
+  launch_turb(fine, fine->stream, fine->st[0], 2);
   fine->launches++;
   const long long cells = (long long)Pc.Nx * Pc.Ny * Pc.Nz;
   float* dT = nullptr;

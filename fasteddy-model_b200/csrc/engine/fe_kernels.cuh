@@ -24,6 +24,11 @@ __global__ void k_consts(float R_gas, float p0, float R_cp, float presGrnd, floa
   out[1] = powf((p0 / presGrnd), R_cp);
 }
 
+__global__ void k_delta(Phys P, long long n, const float* __restrict__ D, float* __restrict__ delta) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) delta[t] = grid_scale_of(P, D[t]);
+}
+
 __global__ void k_pbs(long long n, const float* __restrict__ thBS, float c1, float cp_cv, float* __restrict__ pBS) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) pBS[t] = powf(thBS[t] * c1, cp_cv);
@@ -86,7 +91,7 @@ __device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, cons
                                              (Q.J33[c] * P.dZi * (THr(c + 1) - THr(c - 1)))));
   const float N2 = (P.g / THr(c)) * dthdz;
 #undef THr
-  const float len2 = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
+  const float len2 = grid_scale(P, Q, c);
   if (N2 > 0.0f) {
     const float tb = powf(N2, -0.5f);
     const float ec = e[c] * rinv(rho[c]);
@@ -238,11 +243,10 @@ __device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __rest
 // ------------------------------------------------------------------ last-stage SGS physics
 // One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
 // (the reference's ring minus the i=iMax+1/j=jMax+1 cells, which nothing reads).
-__global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
-  const int k = P.kMin - 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = P.jMin - 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = P.iMin - 1 + blockIdx.z * blockDim.z + threadIdx.z;
-  if (k > P.kMax || j > P.jMax || i > P.iMax) return;
+// SGS physics of ring cell (i,j,k), given the length scale of the cell (lsc) and of the level
+// below (lsm) and sqrt(e/rho) of the level below (sem), all 0 without prognostic TKE.
+__device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int k,
+                                          float lsc, float lsm, float sem, int stage) {
   const long long n = P.n;
   const int si = P.si, sj = P.sj;
   const long long c = (long long)i * si + (long long)j * sj + k;
@@ -250,9 +254,8 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
   const float* e = P.ntke ? st + 5 * n : nullptr;
   if (P.turb) {
     float* T = Q.tau;
-    float Km = 0.0f, lsc = 0.0f;
-    const float delta = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
-    if (P.tke) lsc = length_scale(P, Q, rho, mth, e, c);
+    float Km = 0.0f;
+    const float delta = grid_scale(P, Q, c);
     if (k >= P.kMin) {
       const long long a = c - si, b = c - sj, d = c - 1, ab = a - sj, ad = a - 1, bd = b - 1, abd = ab - 1;
       const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
@@ -285,9 +288,8 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
 #undef TH_
       const float r = rho[c];
       if (P.tke) {
-        const float lsm = length_scale(P, Q, rho, mth, e, d);
-        const float e0 = e[c] * rinv(r), e1 = e[d] * rinv(rho[d]);
-        Km = (float)((double)P.c_k * 0.5 * (double)(lsc * powf(e0, 0.5f) + lsm * powf(e1, 0.5f)));
+        const float e0 = e[c] * rinv(r);
+        Km = (float)((double)P.c_k * 0.5 * (double)(lsc * powf(e0, 0.5f) + lsm * sem));
         const float invPr = 1.0f + 2.0f * lsc / delta;
         const float dev = (float)((2.0 / 3.0) * (double)r *
                                   (double)(Km * (dXi * (mu[c] / r - mu[a] / rho[a]) + dYi * (mv[c] / r - mv[b] / rho[b]) +
@@ -355,6 +357,48 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
     }
   }
   if (P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin) surface_column(P, Q, st, i, j, stage);
+}
+
+// One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
+// (the reference's ring minus the i=iMax+1/j=jMax+1 cells, which nothing reads). The length
+// scale of the level below is recomputed by the same thread (no race on it).
+__global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+  const int k = P.kMin - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = P.jMin - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = P.iMin - 1 + blockIdx.z * blockDim.z + threadIdx.z;
+  if (k > P.kMax || j > P.jMax || i > P.iMax) return;
+  float lsc = 0.0f, lsm = 0.0f, sem = 0.0f;
+  if (P.turb && P.tke) {
+    const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+    const float *rho = st, *mth = st + 4 * P.n, *e = st + 5 * P.n;
+    lsc = length_scale(P, Q, rho, mth, e, c);
+    if (k >= P.kMin) {
+      lsm = length_scale(P, Q, rho, mth, e, c - 1);
+      sem = powf(e[c - 1] * rinv(rho[c - 1]), 0.5f);
+    }
+  }
+  turb_cell(P, Q, st, i, j, k, lsc, lsm, sem, stage);
+}
+
+// The same ring with each warp along k covering 31 output levels plus the level below them
+// (lane 0): every thread evaluates the length scale and sqrt(e/rho) of its own level once and
+// the level below arrives by a shuffle. Block (32, 4, 2); grid ((Nz+2+30)/31, (Ny+5)/4, (Nx+3)/2).
+__global__ void __launch_bounds__(256) k_turb_ov(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+  const int lane = threadIdx.x;
+  const int k = P.kMin - 2 + blockIdx.x * 31 + lane;
+  const int j = P.jMin - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = P.iMin - 1 + blockIdx.z * blockDim.z + threadIdx.z;
+  const bool col = j <= P.jMax && i <= P.iMax;
+  float lsc = 0.0f, se = 0.0f;
+  if (P.turb && P.tke && col && k >= 1 && k <= P.kMax + 1) {
+    const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+    const float *rho = st, *mth = st + 4 * P.n, *e = st + 5 * P.n;
+    lsc = length_scale(P, Q, rho, mth, e, c);
+    se = powf(e[c] * rinv(rho[c]), 0.5f);
+  }
+  const float lsm = __shfl_up_sync(0xffffffffu, lsc, 1), sem = __shfl_up_sync(0xffffffffu, se, 1);
+  if (lane == 0 || !col || k > P.kMax) return;
+  turb_cell(P, Q, st, i, j, k, lsc, k >= P.kMin ? lsm : 0.0f, k >= P.kMin ? sem : 0.0f, stage);
 }
 
 // Write value v of one field at interior cell (i,j,k) and at its periodic images; `nbot`
@@ -444,9 +488,9 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
     const float cyp = contra(D[jp], rho[jp], mv[jp], mw[jp], Q.J32[jp]);
     fv.vm = (0.5f * dYi) * (cyc + cym);
     fv.vp = (0.5f * dYi) * (cyp + cyc);
-    const float czc = (D[c] / rho[c]) * (mw[c] * J3);
-    const float czm = (D[km] / rho[km]) * (mw[km] * Q.J33[km]);
-    const float czp = (D[kp] / rho[kp]) * (mw[kp] * Q.J33[kp]);
+    const float czc = contra_z(D[c], rho[c], mw[c], J3);
+    const float czm = contra_z(D[km], rho[km], mw[km], Q.J33[km]);
+    const float czp = contra_z(D[kp], rho[kp], mw[kp], Q.J33[kp]);
     fv.wm = (k == P.kMin) ? 0.0f : (0.5f * dZi) * (czc + czm);
     fv.wp = (k + 1 >= P.kMax) ? 0.0f : (0.5f * dZi) * (czp + czc);
   }
@@ -575,7 +619,7 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
     // SGS TKE budget (cuda_sgstkeDevice.cu:155-397)
     if (P.tke) {
       const float ri = rinv(rho[c]);
-      const float delta = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
+      const float delta = grid_scale(P, Q, c);
       const float lsc = Q.ls[c];
       Fe = Fe + P.g / (mth[c] * ri) * TT(8, c);
       const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
@@ -702,6 +746,7 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
     pn = powf(rtm * P.c1, P.cp_cv) - Q.pBS[c];
   }
   store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
+  if (atBot) store_images(P, pnxt, i, j, 0, level0_pressure(P, Q, c - k, P.nmoist, nq0), 0, false);
 }
 
 __global__ void k_clock(Ptrs Q, float dt) {

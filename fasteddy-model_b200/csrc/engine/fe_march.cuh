@@ -96,10 +96,43 @@ __device__ __forceinline__ float slot_b(const Phys& P, int s) {
   return 0.0f;
 }
 
-template <int STAGE, int MODE, int TJ>
+// Compile-time configurations ("flavours") of the march kernel. FL_ANY reads every selector at
+// run time; the others fix the field set and the advection schemes of the common cases (PGF on,
+// prognostic TKE, HYB56 for the hydro fields, TKE and q_v, WENO5 for q_l), so the field loop has
+// no run-time branches. The host picks the flavour that matches the configuration.
+constexpr int FL_ANY = 0;
+constexpr int FL_DRY = 1;    // rho, rho u, rho v, rho w, rho theta, rho e
+constexpr int FL_MOIST = 2;  // ... plus rho q_v and rho q_l
+
+template <int FL>
+__device__ __forceinline__ bool f_on(const Phys& P, int s) {
+  if constexpr (FL == FL_DRY) return s <= SL_E || s == SL_P;
+  else if constexpr (FL == FL_MOIST) return true;
+  else return slot_on(P, s);
+}
+template <int FL>
+__device__ __forceinline__ int f_sel(const Phys& P, int s) {
+  if constexpr (FL != FL_ANY) return s == SL_QL ? 5 : 3;
+  else return slot_sel(P, s);
+}
+template <int FL>
+__device__ __forceinline__ const float* f_src(const Phys& P, const float* cur, const float* pcur, int s) {
+  if constexpr (FL != FL_ANY) {
+    if (s == SL_P) return pcur;
+    return cur + (long long)s * P.n;  // slots 0..7 are fields 0..7 when TKE is prognostic
+  } else {
+    return slot_src(P, cur, pcur, s);
+  }
+}
+
+template <int STAGE, int MODE, int TJ, int FL>
 __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     k_march(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base, float* __restrict__ nxt,
             const float* __restrict__ pcur, float* __restrict__ pnxt, float* __restrict__ frhs, int ni) {
+  const int ntke = FL == FL_ANY ? P.ntke : 1;
+  const int nmoist = FL == FL_ANY ? P.nmoist : (FL == FL_MOIST ? 2 : 0);
+  const bool pgf = FL == FL_ANY ? (P.pgf != 0) : true;
+  const bool tke = FL == FL_ANY ? (P.tke != 0) : true;
   using T = MarchTile<TJ>;
   constexpr int PK = T::PK, PLANE = T::PLANE;
   extern __shared__ __align__(16) float sm[];
@@ -158,8 +191,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     const long long pl = (long long)ip * si + tile0;
 #pragma unroll
     for (int s = 0; s < MSLOTS; s++) {
-      if (!slot_on(P, s)) continue;
-      const float* src = slot_src(P, cur, pcur, s) + pl;
+      if (!f_on<FL>(P, s)) continue;
+      const float* src = f_src<FL>(P, cur, pcur, s) + pl;
 #pragma unroll
       for (int q = 0; q < T::RPT; q++)
         if (rV[q] && (s != SL_P || rN[q])) cp_async4(buf + s * PLANE + rS[q], src + rG[q]);
@@ -188,12 +221,12 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     Dm1 = Q.D[cA - si]; Dc = Q.D[cA]; Dn = Q.D[cA + si];
     J1m1 = Q.J31[cA - si]; J1c = Q.J31[cA]; J1n = Q.J31[cA + si];
     J2c = Q.J32[cA]; J3c = Q.J33[cA];
-    if (P.pgf) { pm1 = pcur[cA - si]; p0v = pcur[cA]; pc1 = pcur[cA + si]; }
+    if (pgf) { pm1 = pcur[cA - si]; p0v = pcur[cA]; pc1 = pcur[cA + si]; }
   }
 #pragma unroll
   for (int s = 0; s < 8; s++) {
-    if (!slot_on(P, s)) continue;
-    const float* src = slot_src(P, cur, pcur, s);
+    if (!f_on<FL>(P, s)) continue;
+    const float* src = f_src<FL>(P, cur, pcur, s);
     float sm2 = 0.0f, sm1 = 0.0f;
     if (inArr) {
       sm2 = src[cA - 2 * (long long)si]; sm1 = src[cA - si];
@@ -207,7 +240,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     if (s == 1) um1 = sm1;
     if (s == 3) wm1 = sm1;
   }
-  if (P.pgf) { B0[SL_P * PLANE + own] = p0v; B2[SL_P * PLANE + own] = pm1; }
+  if (pgf) { B0[SL_P * PLANE + own] = p0v; B2[SL_P * PLANE + own] = pm1; }
   float cx0 = contra(Dc, w[0][0], w[1][0], w[3][0], J1c);
   float upPrev;
   {
@@ -215,35 +248,34 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     upPrev = (0.5f * dXi) * (cx0 + cxm);  // velocity of the face i0-1/2
 #pragma unroll
     for (int s = 0; s < 8; s++) {
-      if (!slot_on(P, s)) continue;
-      const float* src = slot_src(P, cur, pcur, s);
+      if (!f_on<FL>(P, s)) continue;
+      const float* src = f_src<FL>(P, cur, pcur, s);
       const float m3 = inArr ? src[cA - 3 * (long long)si] : 0.0f;
       const float m2 = B1[s * PLANE + own], m1 = B2[s * PLANE + own];
-      const float f = slot_sel(P, s) == 3
+      const float f = f_sel<FL>(P, s) == 3
                           ? hyb56_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev, 1.0f - slot_b(P, s))
                           : weno5_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev);
-      xc[s] = upPrev * f;
+      xc[s] = __fmul_rn(upPrev, f);
     }
   }
   float cyOwn, czOwn;
   {
     issue_ring(i0, B0);
-    const float dr = Dc / w[0][0];
-    cyOwn = dr * (w[2][0] + w[3][0] * J2c);
-    czOwn = dr * (w[3][0] * J3c);
+    cyOwn = contra(Dc, w[0][0], w[2][0], w[3][0], J2c);
+    czOwn = contra_z(Dc, w[0][0], w[3][0], J3c);
     float* v = B0 + MSLOTS * PLANE;
     v[(ty + 1) * MK + tx] = cyOwn;
     v[T::CYN + ty * T::CZK + tx + 1] = czOwn;
     if (rtKind) {
       const long long c = (long long)i0 * si + rtOff;
       const float D = Q.D[c], r = cur[c];
-      v[rtS] = rtKind == 1 ? contra(D, r, cur[2 * n + c], cur[3 * n + c], Q.J32[c]) : (D / r) * (cur[3 * n + c] * Q.J33[c]);
+      v[rtS] = rtKind == 1 ? contra(D, r, cur[2 * n + c], cur[3 * n + c], Q.J32[c]) : contra_z(D, r, cur[3 * n + c], Q.J33[c]);
     }
     cp_async_wait_all();
     __syncthreads();
   }
 
-  const bool mpStep = phys && P.nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
+  const bool mpStep = phys && nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
 
   // ---------------------------------------------------------------- march
   float *cs = B0, *ns = B1, *ps = B2;  // planes i, i+1 (own cell: s(i-2) until refilled), i-1
@@ -257,8 +289,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const bool has4 = (i + 4) < P.nxh;
 #pragma unroll
       for (int s = 0; s < 8; s++)
-        if (slot_on(P, s) && has4) nx[s] = slot_src(P, cur, pcur, s)[c + 4 * (long long)si];
-      if (P.pgf) pnx = pcur[c + 2 * (long long)si];
+        if (f_on<FL>(P, s) && has4) nx[s] = f_src<FL>(P, cur, pcur, s)[c + 4 * (long long)si];
+      if (pgf) pnx = pcur[c + 2 * (long long)si];
       Dnn = Q.D[c + 2 * (long long)si];
       J1nn = Q.J31[c + 2 * (long long)si];
       J2n = Q.J32[c + si];
@@ -274,7 +306,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     }
 
     // face velocities of this cell (cuda_advectionDevice.cu:89-106)
-    const float cxp1 = contra(Dn, w[0][1], w[1][1], w[3][1], J1n);
+    const float dr1 = __fdiv_rn(Dn, w[0][1]);  // D/rho of plane i+1, shared by its three velocities
+    const float cxp1 = contra_dr(dr1, w[1][1], w[3][1], J1n);
     const float up = (0.5f * dXi) * (cxp1 + cx0);
     const float* cyP = cs + MSLOTS * PLANE;
     const float* czP = cyP + T::CYN;
@@ -291,15 +324,15 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     for (int s = 0; s < 8; s++) F[s] = 0.0f;
 
     // pressure-gradient force (cuda_pressureDevice.cu:118-194)
-    if (P.pgf) {
+    if (pgf) {
       const float* pp = cs + SL_P * PLANE + own;
       const float dpx = pc1 - ps[SL_P * PLANE + own];
       const float dpy = pp[PK] - pp[-PK];
       const float dpz = pp[1] - pp[-1];
-      if (P.nmoist > 0) {
+      if (nmoist > 0) {
         float rmd = 1.0f;
         rmd = (float)((double)rmd + (double)(w[SL_QV][0] / r0) * 1e-3);
-        if (P.nmoist > 1) rmd = (float)((double)rmd + (double)(w[SL_QL][0] / r0) * 1e-3);
+        if (nmoist > 1) rmd = (float)((double)rmd + (double)(w[SL_QL][0] / r0) * 1e-3);
         const float rdm = 1.0f / rmd;
         F[1] = (float)((double)F[1] - (double)rdm * 0.5 * (double)dXi * (double)dpx);
         F[2] = (float)((double)F[2] - (double)rdm * 0.5 * (double)dYi * (double)dpy);
@@ -314,15 +347,15 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     // advection of every field (cuda_hydroCoreDevice.cu:631-672; WENO5 as x, y, z updates)
 #pragma unroll
     for (int s = 0; s < 8; s++) {
-      if (!slot_on(P, s)) continue;
+      if (!f_on<FL>(P, s)) continue;
       const float* pl = cs + s * PLANE + own;
       const float z0 = w[s][0];
       const float xm2 = ns[s * PLANE + own], xm1 = ps[s * PLANE + own];
-      if (slot_sel(P, s) == 3) {
+      if (f_sel<FL>(P, s) == 3) {
         const float bf = 1.0f - slot_b(P, s);
         const float fxp = hyb56_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
-        const float pxp = up * fxp;
-        const float Dx = pxp - xc[s];
+        const float pxp = __fmul_rn(up, fxp);
+        const float Dx = __fsub_rn(pxp, xc[s]);
         xc[s] = pxp;
         float Dy, Dz;
         {
@@ -336,8 +369,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         F[s] = F[s] - invD * (Dx + Dy + Dz);
       } else {
         const float fxp = weno5_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up);
-        const float pxp = up * fxp;
-        F[s] = F[s] - invD * (pxp - xc[s]);
+        const float pxp = __fmul_rn(up, fxp);
+        F[s] = F[s] - invD * __fsub_rn(pxp, xc[s]);
         xc[s] = pxp;
         {
           const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
@@ -367,9 +400,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         }
         if (P.buoy) {
           const float rbs = inArr ? Q.rhoBS[c] : 0.0f;
-          if (P.nmoist > 0) {
+          if (nmoist > 0) {
             double rm = (double)r0 + (double)w[SL_QV][0] * 1e-3;
-            if (P.nmoist == 2) rm += (double)w[SL_QL][0] * 1e-3;
+            if (nmoist == 2) rm += (double)w[SL_QL][0] * 1e-3;
             const float ratio = r0 / (float)rm;
             F[3] = (float)((double)F[3] - (double)(ratio * P.g) * (rm - (double)rbs));
           } else {
@@ -401,12 +434,12 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
                      J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c)));
       F[4] = F[4] - (dXi * (TT(6, ip) - TT(6, c)) + dYi * (TT(7, jp) - TT(7, c)) + J1 * dXi * (TT(8, ip) - TT(8, c)) +
                      J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c)));
-      if (P.nmoist > 0 && P.moistSGS > 0) {
+      if (nmoist > 0 && P.moistSGS > 0) {
         const float* M = Q.mtau;
         F[SL_QV] = F[SL_QV] - (dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) +
                                J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) + J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) +
                                J3 * dZi * (M[2 * n + kp] - M[2 * n + c]));
-        if (P.nmoist > 1) {
+        if (nmoist > 1) {
           const float* M1 = M + 3 * n;
           F[SL_QL] = F[SL_QL] - (dXi * (M1[ip] - M1[c]) + dYi * (M1[n + jp] - M1[n + c]) +
                                  J1 * dXi * (M1[2 * n + ip] - M1[2 * n + c]) + J2 * dYi * (M1[2 * n + jp] - M1[2 * n + c]) +
@@ -414,9 +447,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         }
       }
       // SGS TKE budget (cuda_sgstkeDevice.cu:155-397)
-      if (P.tke) {
+      if (tke) {
         const float ri = rinv(r0);
-        const float delta = powf(P.dX * P.dY * P.dZ * Dc, (float)(1.0 / 3.0));
+        const float delta = grid_scale(P, Q, c);
         const float lsc = Q.ls[c];
         const float mec = w[SL_E][0];
         float Fe = F[SL_E];
@@ -505,9 +538,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         frhs[2 * n + c] = F[2];
         frhs[3 * n + c] = F[3];
         frhs[4 * n + c] = F[4];
-        if (P.ntke) frhs[5 * n + c] = F[SL_E];
-        if (P.nmoist > 0) frhs[(5 + P.ntke) * n + c] = F[SL_QV];
-        if (P.nmoist > 1) frhs[(6 + P.ntke) * n + c] = F[SL_QL];
+        if (ntke) frhs[5 * n + c] = F[SL_E];
+        if (nmoist > 0) frhs[(5 + ntke) * n + c] = F[SL_QV];
+        if (nmoist > 1) frhs[(6 + ntke) * n + c] = F[SL_QL];
       } else {
         // WS2002 RK3 commit (cuda_RKschemes.cu:113-157), rounding as in the cell kernel
         auto rk = [&](float phi0, float Fv) -> float {
@@ -529,15 +562,15 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         store_images(P, nxt + 3 * n, i, j, k, n3, atBot ? 3 : 0, false);
         store_images(P, nxt + 4 * n, i, j, k, n4, 0, false);
         float nq0 = 0.0f;
-        if (P.ntke) {
+        if (ntke) {
           const float ne = fmaxf(rk(b0(SL_E, 5 * n), F[SL_E]), 1e-10f);
           store_images(P, nxt + 5 * n, i, j, k, ne, atBot ? 3 : 0, false);
         }
-        if (P.nmoist > 0) {
-          const long long o = (5 + P.ntke) * n;
+        if (nmoist > 0) {
+          const long long o = (5 + ntke) * n;
           nq0 = fmaxf(rk(b0(SL_QV, o), F[SL_QV]), 0.0f);
           store_images(P, nxt + o, i, j, k, nq0, atBot ? 3 : 0, atTop);
-          if (P.nmoist > 1) {
+          if (nmoist > 1) {
             const float nq1 = fmaxf(rk(b0(SL_QL, o + n), F[SL_QL]), 0.0f);
             store_images(P, nxt + o + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
           }
@@ -545,10 +578,11 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         float pn;
         {
           float rtm = n4;
-          if (P.nmoist > 0) rtm = (float)((double)n4 * (1.0 + (double)(P.Rv_Rg * nq0 / n0) * 1e-3));
+          if (nmoist > 0) rtm = (float)((double)n4 * (1.0 + (double)(P.Rv_Rg * nq0 / n0) * 1e-3));
           pn = powf(rtm * P.c1, P.cp_cv) - Q.pBS[c];
         }
         store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
+        if (atBot) store_images(P, pnxt, i, j, 0, level0_pressure(P, Q, c - k, nmoist, nq0), 0, false);
       }
     }
 
@@ -557,15 +591,14 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     if (more) {
 #pragma unroll
       for (int s = 0; s < 8; s++)
-        if (slot_on(P, s)) ns[s * PLANE + own] = w[s][1];
-      if (P.pgf) ns[SL_P * PLANE + own] = pc1;
-      const float dr = Dn / w[0][1];
-      cyN = dr * (w[2][1] + w[3][1] * J2n);
-      czN = dr * (w[3][1] * J3n);
+        if (f_on<FL>(P, s)) ns[s * PLANE + own] = w[s][1];
+      if (pgf) ns[SL_P * PLANE + own] = pc1;
+      cyN = contra_dr(dr1, w[2][1], w[3][1], J2n);
+      czN = contra_z_dr(dr1, w[3][1], J3n);
       float* v = ns + MSLOTS * PLANE;
       v[(ty + 1) * MK + tx] = cyN;
       v[T::CYN + ty * T::CZK + tx + 1] = czN;
-      if (rtKind) v[rtS] = rtKind == 1 ? contra(rD, rR, rM, rW, rJ) : (rD / rR) * (rW * rJ);
+      if (rtKind) v[rtS] = rtKind == 1 ? contra(rD, rR, rM, rW, rJ) : contra_z(rD, rR, rW, rJ);
     }
     // shift the x window and the carried values
 #pragma unroll

@@ -49,7 +49,7 @@ __device__ __forceinline__ void sgs_inputs(const Phys& P, const Ptrs& Q, const f
                                              (J3 * dZi * (THr(c + 1) - THr(c - 1)))));
   x[9] = (P.g / THr(c)) * dthdz;
 #undef THr
-  x[10] = powf(P.dX * P.dY * P.dZ * Q.D[c], (float)(1.0 / 3.0));
+  x[10] = grid_scale(P, Q, c);
 }
 
 }  // namespace fe

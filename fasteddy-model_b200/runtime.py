@@ -151,6 +151,9 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_ensemble_destroy", ip, [vp]),
         ("fe_last_error", ctypes.c_char_p, []),
         ("fe_noalloc_max_cells", ctypes.c_longlong, []),
+        ("fe_checkpoint_bytes", ctypes.c_size_t, [vp]),
+        ("fe_checkpoint_save", ip, [vp, vp, ctypes.c_size_t]),
+        ("fe_checkpoint_load", ip, [vp, vp, ctypes.c_size_t]),
         ("fe_mlp_param_count", ctypes.c_longlong, []),
         ("fe_mlp_create", ip, [ip, ctypes.c_ulonglong, ctypes.POINTER(vp)]),
         ("fe_mlp_destroy", ip, [vp]),
@@ -165,7 +168,7 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_mlp_time", ip, [vp, ip, ctypes.c_longlong, ip, fp]),
         ("fe_mlp_check", ip, [vp]),
         ("fe_set_sgs_mlp", ip, [vp, vp]),
-        ("fe_sgs_sample", ip, [vp, fp, fp, fp]),
+        ("fe_sgs_sample", ip, [vp, ctypes.c_longlong, fp, fp, fp]),
         ("fe_coarsen", ip, [vp, vp, fp]),
         ("fe_frhs_noalloc", ip, [ctypes.POINTER(FeConfig), ip, ctypes.c_float, ip, ctypes.POINTER(FeNoallocArgs), vp]),
         ("fe_noalloc_last_error", ctypes.c_char_p, []),
@@ -398,18 +401,35 @@ class Domain:
     def set_tiling(self, tk: int, tj: int, ti: int) -> None:
         _check(self.e.fe_set_tiling(self.h, tk, tj, ti), "fe_set_tiling")
 
+    def clock(self) -> tuple[float, int]:
+        t, it = ctypes.c_float(), ctypes.c_int()
+        _check(self.e.fe_get_clock(self.h, ctypes.byref(t), ctypes.byref(it)), "fe_get_clock")
+        return float(t.value), int(it.value)
+
+    def checkpoint(self) -> bytes:
+        """State, surface planes and clock as one byte string (fe_checkpoint_save)."""
+        n = int(self.e.fe_checkpoint_bytes(self.h))
+        buf = ctypes.create_string_buffer(n)
+        _check(self.e.fe_checkpoint_save(self.h, buf, n), "fe_checkpoint_save")
+        return buf.raw
+
+    def restore(self, blob: bytes) -> None:
+        """Resume from a checkpoint (the grid and base state must already be set)."""
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        _check(self.e.fe_checkpoint_load(self.h, buf, len(blob)), "fe_checkpoint_load")
+
     def set_sgs_mlp(self, mlp: Optional["Mlp"]) -> None:
         """Learned SGS stresses from `mlp` (None: the TKE closure)."""
         _check(self.e.fe_set_sgs_mlp(self.h, mlp.h if mlp is not None else None), "fe_set_sgs_mlp")
         self._mlp = mlp  # keep the network alive while the domain uses it
 
-    def sgs_sample(self) -> dict[str, np.ndarray]:
-        """Closure inputs X (cells x 11), stresses tau (cells x 9) and rho of the interior cells."""
-        cells = self.cfg.Nx * self.cfg.Ny * self.cfg.Nz
+    def sgs_sample(self, every: int = 1) -> dict[str, np.ndarray]:
+        """Closure inputs X (n x 11), stresses tau (n x 9) and rho of every `every`-th interior cell."""
+        cells = (self.cfg.Nx * self.cfg.Ny * self.cfg.Nz + every - 1) // every
         X = np.empty((cells, SGS_NIN), np.float32)
         tau = np.empty((cells, SGS_NOUT), np.float32)
         rho = np.empty(cells, np.float32)
-        _check(self.e.fe_sgs_sample(self.h, _fptr(X), _fptr(tau), _fptr(rho)), "fe_sgs_sample")
+        _check(self.e.fe_sgs_sample(self.h, every, _fptr(X), _fptr(tau), _fptr(rho)), "fe_sgs_sample")
         return {"X": X, "tau": tau, "rho": rho}
 
     def coarsen_into(self, coarse: "Domain") -> np.ndarray:

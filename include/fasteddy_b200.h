@@ -201,6 +201,14 @@ int fe_ensemble_sync(fe_ensemble *e);
 void *fe_ensemble_stream(fe_ensemble *e);
 int fe_ensemble_destroy(fe_ensemble *e);
 
+/* Checkpoint / resume: the prognostic state, the 11 surface planes and the clock in one host
+ * buffer of fe_checkpoint_bytes() bytes (a header checks the domain shape on load). Loading
+ * into a domain with the same grid and base state and advancing repeats the run that wrote it
+ * bit for bit (the reference restarts through its netCDF inFile, io_netcdf.c:106-300). */
+size_t fe_checkpoint_bytes(const fe_domain *d);
+int fe_checkpoint_save(fe_domain *d, void *buf, size_t bytes);
+int fe_checkpoint_load(fe_domain *d, const void *buf, size_t bytes);
+
 /* ======================================================= C. learned SGS closure */
 /* No counterpart in the reference: a small network that replaces the 9 stresses and heat
  * fluxes of the TKE closure (cudaDevice_hydroCoreCalcTaus_PrognosticTKE_DeviatoricTerm,
@@ -243,10 +251,10 @@ int fe_mlp_time(fe_mlp *m, int train, long long batch, int reps, float *ms);
 int fe_mlp_check(fe_mlp *m);
 /* Use the network for the domain's SGS stresses (NULL: the TKE closure). */
 int fe_set_sgs_mlp(fe_domain *d, fe_mlp *m);
-/* Evaluate the domain's closure on its current state and sample every interior cell (row-
- * major i, j, k): inputs X[cells][11], stresses tau[cells][9], density rho[cells] (any NULL
- * is skipped). */
-int fe_sgs_sample(fe_domain *d, float *X, float *tau, float *rho);
+/* Evaluate the domain's closure on its current state and sample every `every`-th interior cell
+ * (row-major i, j, k; every >= 1): inputs X[n][11], stresses tau[n][9], density rho[n] with
+ * n = ceil(cells/every) (any NULL is skipped). */
+int fe_sgs_sample(fe_domain *d, long long every, float *X, float *tau, float *rho);
 /* Coarse-grain the state of `fine` (2Nx x 2Ny x 2Nz over the same physical domain) by a
  * 2x2x2 box filter into the state of `coarse`, and write the subfilter stresses and heat
  * fluxes of every coarse interior cell divided by the filtered density (plus the fine

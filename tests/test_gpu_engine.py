@@ -97,6 +97,46 @@ def test_state_matches_oracle_after_1_and_10_steps(fe, name):
     host.cleanup()
 
 
+def test_error_table_against_the_fp64_oracle(fe):
+    """Error of the FP32 device path against the FP64 oracle after 1, 10 and 100 steps on the
+    moist hill case: relative L2 of every prognostic field and of the perturbations the
+    solution is about (theta' = rho theta / rho - theta_BS and p'). Prints the table (pytest -s);
+    the bounds are the ones the design states for FP32 storage with the stage sums rounded
+    once from double (stages 1-2) or fused (stage 3)."""
+    host, inp, cfg = _setup(fe, "moist_hill")
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    base = inp["baseState"].astype(np.float64)
+    th_bs = interior(base[1] / base[0])
+    names = ["rho", "rho u", "rho v", "rho w", "rho theta", "rho e", "rho qv", "rho ql"]
+    rows, done = [], 0
+    for n in (1, 10, 100):
+        dom.advance(n - done)
+        o.step(n - done)
+        done = n
+        g, r = dom.get_state(), o.get_state()
+        gf = np.concatenate([g["hydroFlds"], g["sgstke"], g["moist"]])
+        rf = np.concatenate([r["hydroFlds"], r["sgstke"], r["moist"]])
+        errs = [rel_l2(interior(gf[f]), interior(rf[f])) for f in range(gf.shape[0])]
+        thp_g = interior(gf[4].astype(np.float64) / gf[0]) - th_bs
+        thp_r = interior(rf[4].astype(np.float64) / rf[0]) - th_bs
+        errs.append(rel_l2(thp_g, thp_r))
+        errs.append(rel_l2(interior(g["pres"]), interior(r["pres"])))
+        rows.append((n, errs))
+    print("\nsteps  " + "  ".join(f"{h:>9s}" for h in names + ["theta'", "p'"]))
+    for n, e in rows:
+        print(f"{n:5d}  " + "  ".join(f"{v:9.2e}" for v in e))
+    e1, e10, e100 = (r[1] for r in rows)
+    assert e100[0] < 1e-5 and e100[4] < 1e-5        # rho, rho theta
+    assert e100[8] < 2e-2                           # theta' (perturbation of ~0.25 K)
+    assert e10[9] < 2e-2 and e100[9] < 5e-2          # p'
+    dom.close()
+    o.close()
+    host.cleanup()
+
+
 def test_graph_replay_equals_step_by_step(fe):
     host, inp, cfg = _setup(fe, "moist_hill")
     a = fe.Domain(cfg)
@@ -115,7 +155,8 @@ def test_graph_replay_equals_step_by_step(fe):
 
 
 def test_tiling_and_autotune_do_not_change_results(fe):
-    """March shapes give identical bits; the cell kernel agrees to rounding."""
+    """March shapes give identical bits (every inlined copy of the flux arithmetic rounds
+    explicitly); the cell kernel agrees to FP32 rounding (per-field state tolerances)."""
     host, inp, cfg = _setup(fe, "cbl_dry")
     a = fe.Domain(cfg)
     a.set_inputs(inp)
@@ -136,7 +177,7 @@ def test_tiling_and_autotune_do_not_change_results(fe):
     c.advance(3)
     sa, sc = a.get_state(), c.get_state()
     for f in range(5):
-        assert rel_l2(interior(sc["hydroFlds"][f]), interior(sa["hydroFlds"][f])) < 1e-6
+        assert rel_l2(interior(sc["hydroFlds"][f]), interior(sa["hydroFlds"][f])) < STATE_TOL[f]
     for d in (a, b, c):
         d.close()
     host.cleanup()
@@ -145,11 +186,21 @@ def test_tiling_and_autotune_do_not_change_results(fe):
 @pytest.mark.parametrize("case", ["cbl_dry", "moist_hill", "hill_dry"])
 def test_march_matches_cell_kernel_on_ragged_tiles(fe, case):
     """Domain extents that are not multiples of the tile (k: 32, j: 8 or 4, i: ni) -- the
-    ring, halo and partial-tile paths of the march kernel -- against the cell kernel."""
+    ring, halo and partial-tile paths of the march kernel -- against the cell kernel.
+
+    The two kernels sum the same flux differences in different orders, so they agree to FP32
+    rounding of the fluxes, not of the (often much smaller) tendency: each tendency field is
+    checked to 1e-4 of its own maximum plus 1e-6 of the largest tendency of its block; states
+    and halos after 4 steps to the per-field tolerances used against the FP64 oracle."""
     host, inp, cfg = _setup(fe, case, nx=37, ny=13, nz=45)
     ref = fe.Domain(cfg)
     ref.set_inputs(inp)
     ref.set_stage_kernel("cell")
+    ref2 = fe.Domain(cfg)
+    ref2.set_inputs(inp)
+    ref2.set_stage_kernel("cell")
+    ref2.advance(4)
+    s2 = ref2.get_state()
     for tj, ni in ((8, 16), (4, 7)):
         d = fe.Domain(cfg)
         d.set_inputs(inp)
@@ -159,28 +210,57 @@ def test_march_matches_cell_kernel_on_ragged_tiles(fe, case):
             for key in ("hydroFrhs", "sgstkeFrhs", "moistFrhs"):
                 if fr.get(key) is None:
                     continue
+                big = max(float(np.abs(interior(fr[key][f])).max()) for f in range(fr[key].shape[0]))
                 for f in range(fr[key].shape[0]):
                     a_, b_ = interior(fd[key][f]), interior(fr[key][f])
-                    scale = max(np.abs(b_).max(), 1e-30)
-                    assert np.abs(a_ - b_).max() <= 2e-5 * scale, (key, f, stage, tj, ni)
+                    tol = 1e-4 * float(np.abs(b_).max()) + 1e-6 * big
+                    assert np.abs(a_ - b_).max() <= tol, (key, f, stage, tj, ni)
         d.advance(4)
-        ref2 = fe.Domain(cfg)
-        ref2.set_inputs(inp)
-        ref2.set_stage_kernel("cell")
-        ref2.advance(4)
-        s1, s2 = d.get_state(), ref2.get_state()
-        for key in ("hydroFlds", "sgstke", "moist"):
-            if s1.get(key) is None:
-                continue
-            for f in range(s1[key].shape[0]):
-                assert rel_l2(interior(s1[key][f]), interior(s2[key][f])) < 1e-6, (key, f, tj, ni)
-            # halo images and boundary copies too: the whole halo-inclusive arrays
-            np.testing.assert_allclose(s1[key], s2[key], rtol=1e-5, atol=1e-6 * float(np.abs(s2[key]).max()))
+        s1 = d.get_state()
+        for f in range(5):
+            assert rel_l2(s1["hydroFlds"][f], s2["hydroFlds"][f]) < STATE_TOL[f], ("hydro", f, tj, ni)
+        for key in ("sgstke", "moist"):
+            if s1.get(key) is not None:
+                for f in range(s1[key].shape[0]):
+                    assert rel_l2(s1[key][f], s2[key][f]) < 2e-3, (key, f, tj, ni)
         # p' = (c rho theta)^(cp/cv) - p_BS: a few ulps of rho theta move it by ~0.01 Pa
         np.testing.assert_allclose(s1["pres"], s2["pres"], rtol=0, atol=0.1)
         d.close()
-        ref2.close()
     ref.close()
+    ref2.close()
+    host.cleanup()
+
+
+@pytest.mark.parametrize("name", ["moist_hill", "cbl_dry"])
+def test_checkpoint_resume_is_bit_identical(fe, name):
+    """16 steps in one go against 8 steps, checkpoint, a fresh domain, resume, 8 steps: state,
+    pressure, surface planes and clock agree bit for bit (the graph path on both sides)."""
+    host, inp, cfg = _setup(fe, name)
+    a = fe.Domain(cfg)
+    a.set_inputs(inp)
+    a.advance(16)
+    b = fe.Domain(cfg)
+    b.set_inputs(inp)
+    b.advance(8)
+    blob = b.checkpoint()
+    b.close()
+    c = fe.Domain(cfg)
+    c.set_inputs(inp)  # grid, base state (the state is replaced by the checkpoint)
+    c.restore(blob)
+    c.advance(8)
+    sa, sc = a.get_state(), c.get_state()
+    for k in ("hydroFlds", "sgstke", "moist", "pres"):
+        if sa[k] is not None:
+            np.testing.assert_array_equal(sa[k], sc[k])
+    for k, v in a.get_surface().items():
+        np.testing.assert_array_equal(v, c.get_surface()[k])
+    assert a.clock() == c.clock()
+    bad = bytearray(blob)
+    bad[0:8] = b"XXXXXXXX"
+    with pytest.raises(fe.FeError):
+        c.restore(bytes(bad))
+    a.close()
+    c.close()
     host.cleanup()
 
 

@@ -1,10 +1,10 @@
 """The allocation-free tendency entry point (fe_frhs_noalloc) against the engine's own
 tendency evaluation (fe_build_frhs), through the C ABI.
 
-fe_frhs_noalloc exists for callers that cannot allocate device memory -- code inside a
-CUDA graph that someone else is capturing, allocators that own all device memory, or
-embedders whose footprint is fixed after start-up. It keeps its scratch in one static
-device array instead of calling cudaMalloc. This file is collected last so that a run
+fe_frhs_noalloc exists for callers that cannot allocate device memory -- allocators that own
+all device memory, or embedders whose footprint is fixed after start-up. It keeps its scratch
+in one static device array instead of calling cudaMalloc. It is a variant of the engine's
+per-cell stage kernel, so it is compared against that kernel (FE_KERNEL_CELL). This file is collected last so that a run
 stopping at the first failure has already run every other test; it also passes alone.
 """
 from __future__ import annotations
@@ -31,6 +31,7 @@ def test_noalloc_tendency_matches_engine_on_two_calls(fe):
     inp, cfg = host.inputs(), host.config()
     dom = fe.Domain(cfg)
     dom.set_inputs(inp)
+    dom.set_stage_kernel("cell")
     st = dom.get_state()  # halo cells filled by the engine
     state = np.concatenate([st["hydroFlds"], st["sgstke"], st["moist"]])
     zero2 = np.zeros_like(inp["z0m"])

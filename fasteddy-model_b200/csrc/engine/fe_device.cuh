@@ -165,9 +165,11 @@ __device__ __forceinline__ float weno5_face(float a, float b, float c, float d, 
 }
 
 // The reference blends both one-sided values with weights 0.5(1 +- sign(u)), which are
-// exactly 1 and 0; only the upwind value is evaluated here (same result).
+// exactly 1 and 0; only the upwind value is evaluated here (same result). The upwind stencil
+// is selected value by value, so lanes of one warp with opposite velocities do not diverge.
 __device__ __forceinline__ float weno5_flux(float m2, float m1, float z0, float p1, float p2, float p3, float vel) {
-  return sgnf(vel) > 0.0f ? weno5_face(m2, m1, z0, p1, p2) : weno5_face(p3, p2, p1, z0, m1);
+  const bool up = sgnf(vel) > 0.0f;
+  return weno5_face(up ? m2 : p3, up ? m1 : p2, up ? z0 : p1, up ? p1 : z0, up ? p2 : m1);
 }
 
 // Face velocities of a cell: lower/upper faces in x, y, z (cuda_advectionDevice.cu:54-121).

@@ -291,12 +291,14 @@ __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const fl
         const float e0 = e[c] * rinv(r);
         Km = (float)((double)P.c_k * 0.5 * (double)(lsc * powf(e0, 0.5f) + lsm * sem));
         const float invPr = 1.0f + 2.0f * lsc / delta;
+        // the velocities as the strain rates form them (phi * rhoInv), so no further divisions
+        const float ic = rinv(r), ia = rinv(rho[a]), ib = rinv(rho[b]), id = rinv(rho[d]);
         const float dev = (float)((2.0 / 3.0) * (double)r *
-                                  (double)(Km * (dXi * (mu[c] / r - mu[a] / rho[a]) + dYi * (mv[c] / r - mv[b] / rho[b]) +
-                                                 J1 * dXi * (mw[c] / r - mw[a] / rho[a]) +
-                                                 J2 * dYi * (mw[c] / r - mw[b] / rho[b]) +
-                                                 J3 * dZi * (mw[c] / r - mw[d] / rho[d])) +
-                                           e[c] / r));
+                                  (double)(Km * (dXi * (mu[c] * ic - mu[a] * ia) + dYi * (mv[c] * ic - mv[b] * ib) +
+                                                 J1 * dXi * (mw[c] * ic - mw[a] * ia) +
+                                                 J2 * dYi * (mw[c] * ic - mw[b] * ib) +
+                                                 J3 * dZi * (mw[c] * ic - mw[d] * id)) +
+                                           e[c] * ic));
         T[c] = -2.0f * r * Km * S11 + dev;
         T[n + c] = -2.0f * r * Km * S21;
         T[2 * n + c] = -2.0f * r * Km * S31;

@@ -14,6 +14,10 @@
 //   face velocities  the contravariant velocities (D/rho)(m + w J) of plane i+1 are produced
 //                 one plane ahead into the same buffers (own cell plus a one-cell ring), so a
 //                 y or z face velocity costs one shared load.
+//   own-column inputs  s(i+4) of every field, p'(i+2), the metrics of plane i+2 and 1/D of
+//                 plane i+1 are copied by cp.async into a per-thread table one plane ahead, and
+//                 the carried x fluxes live in shared memory too: the registers hold only the
+//                 x window, so the 8-field flavour stays within 128 registers per thread.
 //
 // Everything else -- PGF, Rayleigh damping, buoyancy, Coriolis, SGS divergence and TKE budget,
 // saturation adjustment, the WS2002 commit with its halo images and the perturbation pressure
@@ -41,7 +45,12 @@ struct MarchTile {
   static constexpr int RPT = (RING + NT - 1) / NT;  // ring cells per thread
   static constexpr int CYT = 2 * MK, CZT = 2 * TJ;   // ring tasks of the velocity planes
   static constexpr int NBUF = 3;
-  static constexpr int SMEM_BYTES = NBUF * BUF * 4;
+  // per-thread tables: the inputs of the next plane (cp.async, double-buffered) and the
+  // carried x-face flux times velocity of every field
+  static constexpr int NAUX = 14;
+  static constexpr int AUX = 2 * NAUX * NT;
+  static constexpr int XC = 8 * NT;
+  static constexpr int SMEM_BYTES = (NBUF * BUF + AUX + XC) * 4;
 };
 
 // Ring cell r of a staged plane: the 3 rows above and below the tile (full width), then the
@@ -203,25 +212,51 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   // ---------------------------------------------------------------- prologue (plane i0)
   // buffers: plane i0 -> 0, plane i0+1 -> 1 (holds s(i0-2) at the own cell until it is
   // refilled), plane i0-1 -> 2
-  float w[8][4], nx[8], xc[8];
-  float pc1 = 0.0f, pnx = 0.0f;   // p'(i+1), p'(i+2)
+  float w[8][4];
+  float pc1 = 0.0f;   // p'(i+1)
   float Dc = 0.0f, Dn = 0.0f, J1c = 0.0f, J1n = 0.0f, J2c = 0.0f, J3c = 0.0f;
   const long long cA = (long long)i0 * si + col;
 #pragma unroll
   for (int s = 0; s < 8; s++) {
 #pragma unroll
     for (int d = 0; d < 4; d++) w[s][d] = 0.0f;
-    nx[s] = 0.0f; xc[s] = 0.0f;
   }
   float* const B0 = sm;
   float* const B1 = sm + T::BUF;
   float* const B2 = sm + 2 * T::BUF;
+  float* const aux = sm + T::NBUF * T::BUF;   // [2][NAUX][NT]
+  float* const xcs = aux + T::AUX;            // [8][NT]
+  // the inputs of step ib+1 (loaded during step ib): slots 0..7 s(ib+4), 8 p'(ib+2), 9 D(ib+2),
+  // 10 J31(ib+2), 11 J32(ib+2), 12 J33(ib+2), 13 invD(ib+1)
+  auto issue_aux = [&](int ib, float* tbl) {
+    float* const buf = tbl + tid;  // this thread's entry of each slot
+    const long long c = (long long)ib * si + col;
+    if (inArr) {
+      if (ib + 4 < P.nxh) {
+#pragma unroll
+        for (int s = 0; s < 8; s++)
+          if (f_on<FL>(P, s)) cp_async4(buf + s * T::NT, f_src<FL>(P, cur, pcur, s) + c + 4 * (long long)si);
+      }
+      if (pgf) cp_async4(buf + 8 * T::NT, pcur + c + 2 * (long long)si);
+      cp_async4(buf + 9 * T::NT, Q.D + c + 2 * (long long)si);
+      cp_async4(buf + 10 * T::NT, Q.J31 + c + 2 * (long long)si);
+      cp_async4(buf + 11 * T::NT, Q.J32 + c + 2 * (long long)si);
+      cp_async4(buf + 12 * T::NT, Q.J33 + c + 2 * (long long)si);
+      cp_async4(buf + 13 * T::NT, Q.invD + c + si);
+    }
+    cp_async_commit();
+  };
+  if (!inArr) {
+    for (int q = 0; q < 2 * T::NAUX; q++) aux[q * T::NT + tid] = 0.0f;
+    for (int q = 0; q < 8; q++) xcs[q * T::NT + tid] = 0.0f;
+  }
+  issue_aux(i0 - 1, aux + T::NAUX * T::NT);  // read by step i0 (buffer 1)
   float Dm1 = 0.0f, J1m1 = 0.0f, rm1 = 0.0f, um1 = 0.0f, wm1 = 0.0f, p0v = 0.0f, pm1 = 0.0f;
   if (inArr) {
-    Dm1 = Q.D[cA - si]; Dc = Q.D[cA]; Dn = Q.D[cA + si];
-    J1m1 = Q.J31[cA - si]; J1c = Q.J31[cA]; J1n = Q.J31[cA + si];
+    Dm1 = Q.D[cA - si]; Dc = Q.D[cA];
+    J1m1 = Q.J31[cA - si]; J1c = Q.J31[cA];
     J2c = Q.J32[cA]; J3c = Q.J33[cA];
-    if (pgf) { pm1 = pcur[cA - si]; p0v = pcur[cA]; pc1 = pcur[cA + si]; }
+    if (pgf) { pm1 = pcur[cA - si]; p0v = pcur[cA]; }
   }
 #pragma unroll
   for (int s = 0; s < 8; s++) {
@@ -231,7 +266,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     if (inArr) {
       sm2 = src[cA - 2 * (long long)si]; sm1 = src[cA - si];
 #pragma unroll
-      for (int d = 0; d < 4; d++) w[s][d] = src[cA + d * (long long)si];
+      for (int d = 0; d < 3; d++) w[s][d] = src[cA + d * (long long)si];
     }
     B1[s * PLANE + own] = sm2;
     B2[s * PLANE + own] = sm1;
@@ -255,7 +290,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float f = f_sel<FL>(P, s) == 3
                           ? hyb56_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev, 1.0f - slot_b(P, s))
                           : weno5_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev);
-      xc[s] = __fmul_rn(upPrev, f);
+      xcs[s * T::NT + tid] = __fmul_rn(upPrev, f);
     }
   }
   float cyOwn, czOwn;
@@ -283,19 +318,16 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     const bool more = (i + 1 < i1);
     const long long c = (long long)i * si + col;
 
-    // prefetch: plane i+4 of the x window, p'(i+2), D and J31 at i+2, J32 and J33 at i+1
-    float Dnn = 0.0f, J1nn = 0.0f, J2n = 0.0f, J3n = 0.0f;
-    if (inArr) {
-      const bool has4 = (i + 4) < P.nxh;
+    // this plane's table (loaded during the previous step): the new end of the x window and the
+    // metrics of plane i+1; then start the next one
+    const float* ax = aux + ((i - i0 + 1) & 1) * T::NAUX * T::NT + tid;
 #pragma unroll
-      for (int s = 0; s < 8; s++)
-        if (f_on<FL>(P, s) && has4) nx[s] = f_src<FL>(P, cur, pcur, s)[c + 4 * (long long)si];
-      if (pgf) pnx = pcur[c + 2 * (long long)si];
-      Dnn = Q.D[c + 2 * (long long)si];
-      J1nn = Q.J31[c + 2 * (long long)si];
-      J2n = Q.J32[c + si];
-      J3n = Q.J33[c + si];
-    }
+    for (int s = 0; s < 8; s++)
+      if (f_on<FL>(P, s)) w[s][3] = ax[s * T::NT];
+    if (pgf) pc1 = ax[8 * T::NT];
+    Dn = ax[9 * T::NT];
+    J1n = ax[10 * T::NT];
+    if (more) issue_aux(i, aux + ((i - i0) & 1) * T::NAUX * T::NT);
     if (more) issue_ring(i + 1, ns);
     float rD = 0.0f, rR = 1.0f, rM = 0.0f, rW = 0.0f, rJ = 0.0f;
     if (more && rtKind) {
@@ -317,7 +349,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     const float wp = (k + 1 >= P.kMax) ? 0.0f : (0.5f * dZi) * (czP[ty * T::CZK + tx + 2] + czOwn);
 
     const float J1 = J1c, J2 = J2c, J3 = J3c;
-    const float invD = inArr ? Q.invD[c] : 0.0f;
+    const float invD = ax[13 * T::NT];
     const float r0 = w[0][0];
     float F[8];
 #pragma unroll
@@ -355,8 +387,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         const float bf = 1.0f - slot_b(P, s);
         const float fxp = hyb56_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
         const float pxp = __fmul_rn(up, fxp);
-        const float Dx = __fsub_rn(pxp, xc[s]);
-        xc[s] = pxp;
+        const float Dx = __fsub_rn(pxp, xcs[s * T::NT + tid]);
+        xcs[s * T::NT + tid] = pxp;
         float Dy, Dz;
         {
           const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
@@ -370,8 +402,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       } else {
         const float fxp = weno5_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up);
         const float pxp = __fmul_rn(up, fxp);
-        F[s] = F[s] - invD * __fsub_rn(pxp, xc[s]);
-        xc[s] = pxp;
+        F[s] = F[s] - invD * __fsub_rn(pxp, xcs[s * T::NT + tid]);
+        xcs[s * T::NT + tid] = pxp;
         {
           const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
           const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, vp);
@@ -593,8 +625,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       for (int s = 0; s < 8; s++)
         if (f_on<FL>(P, s)) ns[s * PLANE + own] = w[s][1];
       if (pgf) ns[SL_P * PLANE + own] = pc1;
-      cyN = contra_dr(dr1, w[2][1], w[3][1], J2n);
-      czN = contra_z_dr(dr1, w[3][1], J3n);
+      cyN = contra_dr(dr1, w[2][1], w[3][1], ax[11 * T::NT]);
+      czN = contra_z_dr(dr1, w[3][1], ax[12 * T::NT]);
       float* v = ns + MSLOTS * PLANE;
       v[(ty + 1) * MK + tx] = cyN;
       v[T::CYN + ty * T::CZK + tx + 1] = czN;
@@ -605,11 +637,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     for (int s = 0; s < 8; s++) {
 #pragma unroll
       for (int d = 0; d < 3; d++) w[s][d] = w[s][d + 1];
-      w[s][3] = nx[s];
     }
-    pc1 = pnx;
     cx0 = cxp1; upPrev = up;
-    Dc = Dn; Dn = Dnn; J1c = J1n; J1n = J1nn; J2c = J2n; J3c = J3n;
+    Dc = Dn; J1c = J1n; J2c = ax[11 * T::NT]; J3c = ax[12 * T::NT];
     cyOwn = cyN; czOwn = czN;
     float* const t = ps;
     ps = cs; cs = ns; ns = t;

@@ -1,6 +1,7 @@
 // fe_mlp.cuh -- the learned SGS closure on the 5th-generation tensor cores (sm_100a).
 //
-// Network: 11 -> 64 -> 64 -> 64 -> 9, tanh on the hidden layers; inputs standardised,
+// Network: 11 -> 64 -> 64 -> 64 -> 9, tanh on the hidden layers (hardware tanh.approx, see
+// tanh_hw); inputs standardised,
 // outputs tau/rho = out_mu + out_sig * y. Every layer is one 128-row tile of tcgen05.mma
 // (kind::f16, BF16 A and B operands from shared memory, FP32 accumulators in tensor memory),
 // issued by one thread; the epilogue (tcgen05.ld, bias, tanh, BF16 pack) runs on all 128
@@ -185,6 +186,15 @@ __device__ __forceinline__ void put_inputs(char* x0, int r, const float* x, cons
   st_chunk(x0, r, 1, 16, v + 8);
 }
 
+// tanh of the hidden layers: the hardware approximation (tanh.approx.f32, relative error
+// about 2^-11), below the resolution of the BF16 activations it feeds (2^-9), at one
+// instruction instead of a library tanh
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // hidden-layer epilogue: accumulator row + bias -> tanh -> BF16 tile row
 __device__ __forceinline__ void epi_tanh(uint32_t tacc, const float* bias, char* out, int r) {
 #pragma unroll
@@ -193,7 +203,7 @@ __device__ __forceinline__ void epi_tanh(uint32_t tacc, const float* bias, char*
     tmem_ld16(tacc + g * 16, v);
     tmem_wait_ld();
 #pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = tanhf(v[q] + bias[g * 16 + q]);
+    for (int q = 0; q < 16; q++) v[q] = tanh_hw(v[q] + bias[g * 16 + q]);
     st_chunk(out, r, 2 * g, 64, v);
     st_chunk(out, r, 2 * g + 1, 64, v + 8);
   }

@@ -547,11 +547,11 @@ static dim3 stage_grid(const fe_domain* d) {
   const Phys& P = d->P;
   return dim3((P.Nz + d->tk - 1) / d->tk, (P.Ny + d->tj - 1) / d->tj, (P.Nx + d->ti - 1) / d->ti);
 }
-// Last-stage SGS physics on the +1 ring (k_turb_ov: warps of 31 output levels plus the one below).
+// Last-stage SGS physics on the +1 ring (k_turb_t: shared-memory tiles of primitives).
 static void launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
   const Phys& P = d->P;
-  const dim3 g((P.Nz + 2 + 30) / 31, (P.Ny + 2 + 3) / 4, (P.Nx + 2 + 1) / 2);
-  fe::k_turb_ov<<<g, dim3(32, 4, 2), 0, s>>>(P, d->Q, st, stage);
+  const dim3 g((P.Nz + 2 + fe::TT_K - 1) / fe::TT_K, (P.Ny + 2 + fe::TT_J - 1) / fe::TT_J, (P.Nx + 2 + fe::TT_I - 1) / fe::TT_I);
+  fe::k_turb_t<<<g, dim3(fe::TT_K, fe::TT_J, fe::TT_I), 0, s>>>(P, d->Q, st, stage);
 }
 
 static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }

@@ -81,24 +81,46 @@ __global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, float* 
   pres[t] = pert_pressure(P, st, Q.pBS, src);
 }
 
-// SGS length scale at cell c (cuda_sgstkeDevice.cu:96-151).
-__device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, const float* __restrict__ rho,
-                                              const float* __restrict__ th, const float* __restrict__ e, long long c) {
-  const int si = P.si, sj = P.sj;
-#define THr(x) (th[x] * rinv(rho[x]))
-  const float dthdz = (float)(0.5 * (double)((Q.J31[c] * P.dXi * (THr(c + si) - THr(c - si))) +
-                                             (Q.J32[c] * P.dYi * (THr(c + sj) - THr(c - sj))) +
-                                             (Q.J33[c] * P.dZi * (THr(c + 1) - THr(c - 1)))));
-  const float N2 = (P.g / THr(c)) * dthdz;
-#undef THr
+// Primitive variables (phi/rho, formed as phi * rinv(rho)) of a cell and its neighbours, read
+// straight from the flux-form state. Offsets (di, dj, dk) are relative to cell c.
+struct GlobalPrims {
+  const float *rho, *mu, *mv, *mw, *mth, *e, *q;
+  long long n, c;
+  int si, sj;
+  __device__ __forceinline__ long long at(int di, int dj, int dk) const { return c + di * (long long)si + dj * (long long)sj + dk; }
+  __device__ __forceinline__ float r(int di, int dj, int dk) const { return rho[at(di, dj, dk)]; }
+  __device__ __forceinline__ float u(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mu[x] * rinv(rho[x]); }
+  __device__ __forceinline__ float v(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mv[x] * rinv(rho[x]); }
+  __device__ __forceinline__ float w(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mw[x] * rinv(rho[x]); }
+  __device__ __forceinline__ float th(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mth[x] * rinv(rho[x]); }
+  __device__ __forceinline__ float ev(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return e[x] * rinv(rho[x]); }
+  __device__ __forceinline__ float qm(int m, int di, int dj, int dk) const {
+    const long long x = at(di, dj, dk);
+    return q[m * n + x] * rinv(rho[x]);
+  }
+};
+
+// SGS length scale at cell c + dk (cuda_sgstkeDevice.cu:96-151), from primitives.
+template <class A>
+__device__ __forceinline__ float length_scale_a(const Phys& P, const Ptrs& Q, const A& pr, long long c, int dk) {
+  const float dthdz = (float)(0.5 * (double)((Q.J31[c] * P.dXi * (pr.th(1, 0, dk) - pr.th(-1, 0, dk))) +
+                                             (Q.J32[c] * P.dYi * (pr.th(0, 1, dk) - pr.th(0, -1, dk))) +
+                                             (Q.J33[c] * P.dZi * (pr.th(0, 0, dk + 1) - pr.th(0, 0, dk - 1)))));
+  const float N2 = (P.g / pr.th(0, 0, dk)) * dthdz;
   const float len2 = grid_scale(P, Q, c);
   if (N2 > 0.0f) {
     const float tb = powf(N2, -0.5f);
-    const float ec = e[c] * rinv(rho[c]);
+    const float ec = pr.ev(0, 0, dk);
     const float len1 = (float)(0.76 * (double)powf(ec, 0.5f) * (double)tb);
     return fmaxf(fminf(len1, len2), 1e-2f);
   }
   return len2;
+}
+
+__device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, const float* __restrict__ rho,
+                                              const float* __restrict__ th, const float* __restrict__ e, long long c) {
+  GlobalPrims pr{rho, nullptr, nullptr, nullptr, th, e, nullptr, P.n, c, P.si, P.sj};
+  return length_scale_a(P, Q, pr, c, 0);
 }
 
 // ------------------------------------------------------------------ surface layer
@@ -241,64 +263,51 @@ __device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __rest
 }
 
 // ------------------------------------------------------------------ last-stage SGS physics
-// One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
-// (the reference's ring minus the i=iMax+1/j=jMax+1 cells, which nothing reads).
 // SGS physics of ring cell (i,j,k), given the length scale of the cell (lsc) and of the level
-// below (lsm) and sqrt(e/rho) of the level below (sem), all 0 without prognostic TKE.
-__device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int k,
-                                          float lsc, float lsm, float sem, int stage) {
+// below (lsm) and sqrt(e/rho) of the level below (sem), all 0 without prognostic TKE; the
+// neighbours' primitive variables come from accessor `pr` (state or shared-memory tile).
+template <class A>
+__device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const A& pr, const float* __restrict__ st, int i,
+                                            int j, int k, float lsc, float lsm, float sem, int stage) {
   const long long n = P.n;
-  const int si = P.si, sj = P.sj;
-  const long long c = (long long)i * si + (long long)j * sj + k;
-  const float *rho = st, *mu = st + n, *mv = st + 2 * n, *mw = st + 3 * n, *mth = st + 4 * n;
-  const float* e = P.ntke ? st + 5 * n : nullptr;
+  const long long c = (long long)i * P.si + (long long)j * P.sj + k;
   if (P.turb) {
     float* T = Q.tau;
     float Km = 0.0f;
     const float delta = grid_scale(P, Q, c);
     if (k >= P.kMin) {
-      const long long a = c - si, b = c - sj, d = c - 1, ab = a - sj, ad = a - 1, bd = b - 1, abd = ab - 1;
       const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
       const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
-#define U_(x) (mu[x] * rinv(rho[x]))
-#define V_(x) (mv[x] * rinv(rho[x]))
-#define W_(x) (mw[x] * rinv(rho[x]))
-#define TH_(x) (mth[x] * rinv(rho[x]))
-      float S11 = dXi * (U_(c) - U_(a));
-      float S22 = dYi * (V_(c) - V_(b));
-      float S33 = J1 * dXi * (W_(c) - W_(a)) + J2 * dYi * (W_(c) - W_(b)) + J3 * dZi * (W_(c) - W_(d));
-      float S21 = 0.5f * (0.5f * (dXi * (V_(c) - V_(a)) + dXi * (V_(b) - V_(ab))) +
-                          0.5f * (dYi * (U_(c) - U_(b)) + dYi * (U_(a) - U_(ab))));
-      float S31 = 0.5f * (0.5f * (dXi * (W_(c) - W_(a)) + dXi * (W_(d) - W_(ad))) +
-                          0.5f * (J1 * dXi * (U_(c) - U_(a)) + J1 * dXi * (U_(d) - U_(ad))) +
-                          0.25f * (J2 * dYi * (U_(c) - U_(b)) + J2 * dYi * (U_(a) - U_(ab)) + J2 * dYi * (U_(d) - U_(bd)) +
-                                   J2 * dYi * (U_(ad) - U_(abd))) +
-                          0.5f * (J3 * dZi * (U_(c) - U_(d)) + J3 * dZi * (U_(a) - U_(ad))));
-      float S32 = 0.5f * (0.5f * (dYi * (W_(c) - W_(b)) + dYi * (W_(d) - W_(bd))) +
-                          0.25f * (J1 * dXi * (V_(c) - V_(a)) + J1 * dXi * (V_(b) - V_(ab)) + J1 * dXi * (V_(d) - V_(ad)) +
-                                   J1 * dXi * (V_(bd) - V_(abd))) +
-                          0.5f * (J2 * dYi * (V_(c) - V_(b)) + J2 * dYi * (V_(d) - V_(bd))) +
-                          0.5f * (J3 * dZi * (V_(c) - V_(d)) + J3 * dZi * (V_(b) - V_(bd))));
-      float ST1 = dXi * (TH_(c) - TH_(a));
-      float ST2 = dYi * (TH_(c) - TH_(b));
-      float ST3 = (J1 * dXi * (TH_(c) - TH_(a))) + (J2 * dYi * (TH_(c) - TH_(b))) + (J3 * dZi * (TH_(c) - TH_(d)));
-#undef U_
-#undef V_
-#undef W_
-#undef TH_
-      const float r = rho[c];
+      // c, a = i-1, b = j-1, d = k-1 and their combinations
+      const float uc = pr.u(0, 0, 0), ua = pr.u(-1, 0, 0), ub = pr.u(0, -1, 0), ud = pr.u(0, 0, -1);
+      const float uab = pr.u(-1, -1, 0), uad = pr.u(-1, 0, -1), ubd = pr.u(0, -1, -1), uabd = pr.u(-1, -1, -1);
+      const float vc = pr.v(0, 0, 0), va = pr.v(-1, 0, 0), vb = pr.v(0, -1, 0), vd = pr.v(0, 0, -1);
+      const float vab = pr.v(-1, -1, 0), vad = pr.v(-1, 0, -1), vbd = pr.v(0, -1, -1), vabd = pr.v(-1, -1, -1);
+      const float wc = pr.w(0, 0, 0), wa = pr.w(-1, 0, 0), wb = pr.w(0, -1, 0), wd = pr.w(0, 0, -1);
+      const float wad = pr.w(-1, 0, -1), wbd = pr.w(0, -1, -1);
+      const float thc = pr.th(0, 0, 0), tha = pr.th(-1, 0, 0), thb = pr.th(0, -1, 0), thd = pr.th(0, 0, -1);
+      float S11 = dXi * (uc - ua);
+      float S22 = dYi * (vc - vb);
+      float S33 = J1 * dXi * (wc - wa) + J2 * dYi * (wc - wb) + J3 * dZi * (wc - wd);
+      float S21 = 0.5f * (0.5f * (dXi * (vc - va) + dXi * (vb - vab)) + 0.5f * (dYi * (uc - ub) + dYi * (ua - uab)));
+      float S31 = 0.5f * (0.5f * (dXi * (wc - wa) + dXi * (wd - wad)) + 0.5f * (J1 * dXi * (uc - ua) + J1 * dXi * (ud - uad)) +
+                          0.25f * (J2 * dYi * (uc - ub) + J2 * dYi * (ua - uab) + J2 * dYi * (ud - ubd) + J2 * dYi * (uad - uabd)) +
+                          0.5f * (J3 * dZi * (uc - ud) + J3 * dZi * (ua - uad)));
+      float S32 = 0.5f * (0.5f * (dYi * (wc - wb) + dYi * (wd - wbd)) +
+                          0.25f * (J1 * dXi * (vc - va) + J1 * dXi * (vb - vab) + J1 * dXi * (vd - vad) + J1 * dXi * (vbd - vabd)) +
+                          0.5f * (J2 * dYi * (vc - vb) + J2 * dYi * (vd - vbd)) + 0.5f * (J3 * dZi * (vc - vd) + J3 * dZi * (vb - vbd)));
+      float ST1 = dXi * (thc - tha);
+      float ST2 = dYi * (thc - thb);
+      float ST3 = (J1 * dXi * (thc - tha)) + (J2 * dYi * (thc - thb)) + (J3 * dZi * (thc - thd));
+      const float r = pr.r(0, 0, 0);
       if (P.tke) {
-        const float e0 = e[c] * rinv(r);
+        const float e0 = pr.ev(0, 0, 0);
         Km = (float)((double)P.c_k * 0.5 * (double)(lsc * powf(e0, 0.5f) + lsm * sem));
         const float invPr = 1.0f + 2.0f * lsc / delta;
-        // the velocities as the strain rates form them (phi * rhoInv), so no further divisions
-        const float ic = rinv(r), ia = rinv(rho[a]), ib = rinv(rho[b]), id = rinv(rho[d]);
         const float dev = (float)((2.0 / 3.0) * (double)r *
-                                  (double)(Km * (dXi * (mu[c] * ic - mu[a] * ia) + dYi * (mv[c] * ic - mv[b] * ib) +
-                                                 J1 * dXi * (mw[c] * ic - mw[a] * ia) +
-                                                 J2 * dYi * (mw[c] * ic - mw[b] * ib) +
-                                                 J3 * dZi * (mw[c] * ic - mw[d] * id)) +
-                                           e[c] * ic));
+                                  (double)(Km * (dXi * (uc - ua) + dYi * (vc - vb) + J1 * dXi * (wc - wa) +
+                                                 J2 * dYi * (wc - wb) + J3 * dZi * (wc - wd)) +
+                                           e0));
         T[c] = -2.0f * r * Km * S11 + dev;
         T[n + c] = -2.0f * r * Km * S21;
         T[2 * n + c] = -2.0f * r * Km * S31;
@@ -310,7 +319,7 @@ __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const fl
         T[8 * n + c] = -r * Km * invPr * ST3;
       } else {
         const float t1 = 0.5f * (S11 * S11 + S22 * S22 + S33 * S33) + S21 * S21 + S31 * S31 + S32 * S32;
-        const float N2 = P.g / (mth[c] * rinv(r)) * ST3;
+        const float N2 = P.g / thc * ST3;
         const float t2 = N2 * 3.0f;
         Km = (P.c_s * delta) * (P.c_s * delta) * sqrtf(fmaxf(0.0f, t1 - fmaxf(0.0f, t2)));
         const float invPr = 1.0f + 2.0f * delta / delta;
@@ -328,29 +337,30 @@ __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const fl
     if (P.tke) {
       Q.ls[c] = lsc;
       // TKE transport fluxes (de/dx_j)*Km*rho (cuda_sgstkeDevice.cu:309-397), Km = 0 below kMin
-      const float ex = e[c + si] * rinv(rho[c + si]) - e[c - si] * rinv(rho[c - si]);
-      const float ey = e[c + sj] * rinv(rho[c + sj]) - e[c - sj] * rinv(rho[c - sj]);
-      const float ez = e[c + 1] * rinv(rho[c + 1]) - e[c - 1] * rinv(rho[c - 1]);
+      const float ex = pr.ev(1, 0, 0) - pr.ev(-1, 0, 0);
+      const float ey = pr.ev(0, 1, 0) - pr.ev(0, -1, 0);
+      const float ez = pr.ev(0, 0, 1) - pr.ev(0, 0, -1);
       const float dedx = 0.5f * (P.dXi * ex);
       const float dedy = 0.5f * (P.dYi * ey);
       const float dedz = 0.5f * (Q.J31[c] * P.dXi * ex + Q.J32[c] * P.dYi * ey + Q.J33[c] * P.dZi * ez);
-      Q.tkeQ[c] = dedx * Km * rho[c];
-      Q.tkeQ[n + c] = dedy * Km * rho[c];
-      Q.tkeQ[2 * n + c] = dedz * Km * rho[c];
+      const float rc = pr.r(0, 0, 0);
+      Q.tkeQ[c] = dedx * Km * rc;
+      Q.tkeQ[n + c] = dedy * Km * rc;
+      Q.tkeQ[2 * n + c] = dedz * Km * rc;
     }
     if (P.moist && P.moistSGS > 0) {
       const float invPr = 1.0f + 2.0f * (P.tke ? lsc : delta) / delta;
+      const float rc = pr.r(0, 0, 0);
       for (int m = 0; m < P.nmoist; m++) {
-        const float* q = st + (long long)(5 + P.ntke + m) * n;
-        const float qc = q[c] * rinv(rho[c]), qa = q[c - si] * rinv(rho[c - si]);
-        const float qb = q[c - sj] * rinv(rho[c - sj]), qd = q[c - 1] * rinv(rho[c - 1]);
+        const float qc = pr.qm(m, 0, 0, 0), qa = pr.qm(m, -1, 0, 0);
+        const float qb = pr.qm(m, 0, -1, 0), qd = pr.qm(m, 0, 0, -1);
         float g1 = P.dXi * (qc - qa);
         float g2 = P.dYi * (qc - qb);
         float g3 = Q.J31[c] * P.dXi * (qc - qa) + Q.J32[c] * P.dYi * (qc - qb) + Q.J33[c] * P.dZi * (qc - qd);
         if (k >= P.kMin) {
-          g1 = -rho[c] * Km * invPr * g1;
-          g2 = -rho[c] * Km * invPr * g2;
-          g3 = -rho[c] * Km * invPr * g3;
+          g1 = -rc * Km * invPr * g1;
+          g2 = -rc * Km * invPr * g2;
+          g3 = -rc * Km * invPr * g3;
         }
         Q.mtau[(3 * m + 0) * n + c] = g1;
         Q.mtau[(3 * m + 1) * n + c] = g2;
@@ -359,6 +369,14 @@ __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const fl
     }
   }
   if (P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin) surface_column(P, Q, st, i, j, stage);
+}
+
+__device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int k,
+                                          float lsc, float lsm, float sem, int stage) {
+  const long long n = P.n;
+  GlobalPrims pr{st, st + n, st + 2 * n, st + 3 * n, st + 4 * n, P.ntke ? st + 5 * n : nullptr,
+                 P.nmoist ? st + (5 + P.ntke) * n : nullptr, n, (long long)i * P.si + (long long)j * P.sj + k, P.si, P.sj};
+  turb_cell_a(P, Q, pr, st, i, j, k, lsc, lsm, sem, stage);
 }
 
 // One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
@@ -382,25 +400,81 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
   turb_cell(P, Q, st, i, j, k, lsc, lsm, sem, stage);
 }
 
-// The same ring with each warp along k covering 31 output levels plus the level below them
-// (lane 0): every thread evaluates the length scale and sqrt(e/rho) of its own level once and
-// the level below arrives by a shuffle. Block (32, 4, 2); grid ((Nz+2+30)/31, (Ny+5)/4, (Nx+3)/2).
-__global__ void __launch_bounds__(256) k_turb_ov(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
-  const int lane = threadIdx.x;
-  const int k = P.kMin - 2 + blockIdx.x * 31 + lane;
-  const int j = P.jMin - 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = P.iMin - 1 + blockIdx.z * blockDim.z + threadIdx.z;
-  const bool col = j <= P.jMax && i <= P.iMax;
-  float lsc = 0.0f, se = 0.0f;
-  if (P.turb && P.tke && col && k >= 1 && k <= P.kMax + 1) {
-    const long long c = (long long)i * P.si + (long long)j * P.sj + k;
-    const float *rho = st, *mth = st + 4 * P.n, *e = st + 5 * P.n;
-    lsc = length_scale(P, Q, rho, mth, e, c);
-    se = powf(e[c] * rinv(rho[c]), 0.5f);
+// The same ring in tiles of 32 levels x 4 rows x 2 planes per block of 256 threads. The block
+// first forms the primitive variables (phi * rinv(rho), the same expression the per-cell form
+// evaluates) of the tile and its stencil halo once into shared memory, then the length scale and
+// sqrt(e/rho) of every tile column including the level below the tile, then each thread runs
+// the SGS physics of its cell on the shared copies. Results equal the per-cell form's bit for bit.
+constexpr int TT_K = 32, TT_J = 4, TT_I = 2;
+constexpr int TP_K = TT_K + 3, TP_J = TT_J + 2, TP_I = TT_I + 2;  // points k0-2..k0+32, j0-1..j0+4, i0-1..i0+2
+constexpr int TP_N = TP_I * TP_J * TP_K;
+constexpr int TP_F = 8;  // rho, u, v, w, theta, e/rho, qv/rho, ql/rho
+
+struct TilePrims {
+  const float* t;
+  int o;  // own point
+  __device__ __forceinline__ float at(int f, int di, int dj, int dk) const { return t[f * TP_N + o + di * (TP_J * TP_K) + dj * TP_K + dk]; }
+  __device__ __forceinline__ float r(int di, int dj, int dk) const { return at(0, di, dj, dk); }
+  __device__ __forceinline__ float u(int di, int dj, int dk) const { return at(1, di, dj, dk); }
+  __device__ __forceinline__ float v(int di, int dj, int dk) const { return at(2, di, dj, dk); }
+  __device__ __forceinline__ float w(int di, int dj, int dk) const { return at(3, di, dj, dk); }
+  __device__ __forceinline__ float th(int di, int dj, int dk) const { return at(4, di, dj, dk); }
+  __device__ __forceinline__ float ev(int di, int dj, int dk) const { return at(5, di, dj, dk); }
+  __device__ __forceinline__ float qm(int m, int di, int dj, int dk) const { return at(6 + m, di, dj, dk); }
+};
+
+__global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+  __shared__ float tile[TP_F * TP_N];
+  __shared__ float lsT[TT_I][TT_J][TT_K + 1];  // length scale, levels k0-1..k0+31
+  __shared__ float seT[TT_I][TT_J][TT_K + 1];  // sqrt(e/rho), same levels
+  const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
+  const int tid = (tz * TT_J + ty) * TT_K + tx;
+  const int k0 = P.kMin - 1 + blockIdx.x * TT_K, j0 = P.jMin - 1 + blockIdx.y * TT_J, i0 = P.iMin - 1 + blockIdx.z * TT_I;
+  const long long n = P.n;
+  for (int p = tid; p < TP_N; p += TT_K * TT_J * TT_I) {
+    const int pk = p % TP_K, pj = (p / TP_K) % TP_J, pi = p / (TP_K * TP_J);
+    const int i = i0 - 1 + pi, j = j0 - 1 + pj, k = k0 - 2 + pk;  // >= 1, >= 1, >= 0
+    float v[TP_F] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (i < P.nxh && j < P.nyh && k < P.nzh) {
+      const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+      const float rr = st[c];
+      const float ri = rinv(rr);
+      v[0] = rr;
+      v[1] = st[n + c] * ri;
+      v[2] = st[2 * n + c] * ri;
+      v[3] = st[3 * n + c] * ri;
+      v[4] = st[4 * n + c] * ri;
+      if (P.ntke) v[5] = st[5 * n + c] * ri;
+      if (P.nmoist > 0) v[6] = st[(long long)(5 + P.ntke) * n + c] * ri;
+      if (P.nmoist > 1) v[7] = st[(long long)(6 + P.ntke) * n + c] * ri;
+    }
+#pragma unroll
+    for (int f = 0; f < TP_F; f++) tile[f * TP_N + p] = v[f];
   }
-  const float lsm = __shfl_up_sync(0xffffffffu, lsc, 1), sem = __shfl_up_sync(0xffffffffu, se, 1);
-  if (lane == 0 || !col || k > P.kMax) return;
-  turb_cell(P, Q, st, i, j, k, lsc, k >= P.kMin ? lsm : 0.0f, k >= P.kMin ? sem : 0.0f, stage);
+  __syncthreads();
+  const bool tke = P.turb && P.tke;
+  if (tke) {
+    for (int q = tid; q < TT_I * TT_J * (TT_K + 1); q += TT_K * TT_J * TT_I) {
+      const int lk = q % (TT_K + 1), lj = (q / (TT_K + 1)) % TT_J, li = q / ((TT_K + 1) * TT_J);
+      const int i = i0 + li, j = j0 + lj, k = k0 - 1 + lk;
+      float ls = 0.0f, se = 0.0f;
+      if (i <= P.iMax && j <= P.jMax && k >= 1 && k <= P.kMax) {
+        const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+        const TilePrims pr{tile, (li + 1) * (TP_J * TP_K) + (lj + 1) * TP_K + (lk + 1)};
+        ls = length_scale_a(P, Q, pr, c, 0);
+        se = powf(pr.ev(0, 0, 0), 0.5f);
+      }
+      lsT[li][lj][lk] = ls;
+      seT[li][lj][lk] = se;
+    }
+    __syncthreads();
+  }
+  const int i = i0 + tz, j = j0 + ty, k = k0 + tx;
+  if (i > P.iMax || j > P.jMax || k > P.kMax) return;
+  const TilePrims pr{tile, (tz + 1) * (TP_J * TP_K) + (ty + 1) * TP_K + (tx + 2)};
+  const bool below = tke && k >= P.kMin;
+  turb_cell_a(P, Q, pr, st, i, j, k, tke ? lsT[tz][ty][tx + 1] : 0.0f, below ? lsT[tz][ty][tx] : 0.0f,
+              below ? seT[tz][ty][tx] : 0.0f, stage);
 }
 
 // Write value v of one field at interior cell (i,j,k) and at its periodic images; `nbot`

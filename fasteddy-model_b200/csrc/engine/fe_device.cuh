@@ -58,6 +58,7 @@ struct Ptrs {
   float *mtau;                 // 3 per moisture species
   float *cd, *ch, *cq, *fricVel, *htFlux, *tskin, *invOblen, *z0m, *z0t, *qFlux, *qskin;
   const float* delta;          // grid scale (dx dy dz D)^(1/3) per cell, or nullptr (evaluated inline)
+  float* feat;                 // inputs of the learned closure per ring cell (11 fields), or nullptr
   int *clockIt;                // simTime_it of the step being computed
   float *clockTime;            // simTime of the step being computed
 };
@@ -114,6 +115,26 @@ __device__ __forceinline__ float level0_pressure(const Phys& P, const Ptrs& Q, l
   if (nmoist > 0) rt = (float)((double)rt * (1.0 + (double)(P.Rv_Rg * qv / Q.rhoBS[c0]) * 1e-3));
   return powf(rt * P.c1, P.cp_cv) - Q.pBS[c0];
 }
+
+// Primitive variables (phi/rho, formed as phi * rinv(rho)) of a cell and its neighbours, read
+// straight from the flux-form state. Offsets (di, dj, dk) are relative to cell c. The product is
+// rounded on its own (never fused into a following add), as when it is staged in a tile.
+struct GlobalPrims {
+  const float *rho, *mu, *mv, *mw, *mth, *e, *q;
+  long long n, c;
+  int si, sj;
+  __device__ __forceinline__ long long at(int di, int dj, int dk) const { return c + di * (long long)si + dj * (long long)sj + dk; }
+  __device__ __forceinline__ float r(int di, int dj, int dk) const { return rho[at(di, dj, dk)]; }
+  __device__ __forceinline__ float u(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return __fmul_rn(mu[x], rinv(rho[x])); }
+  __device__ __forceinline__ float v(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return __fmul_rn(mv[x], rinv(rho[x])); }
+  __device__ __forceinline__ float w(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return __fmul_rn(mw[x], rinv(rho[x])); }
+  __device__ __forceinline__ float th(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return __fmul_rn(mth[x], rinv(rho[x])); }
+  __device__ __forceinline__ float ev(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return __fmul_rn(e[x], rinv(rho[x])); }
+  __device__ __forceinline__ float qm(int m, int di, int dj, int dk) const {
+    const long long x = at(di, dj, dk);
+    return __fmul_rn(q[m * n + x], rinv(rho[x]));
+  }
+};
 
 // ---------------------------------------------------------------- advection
 // The flux and velocity helpers spell out every rounding (__fmaf_rn/__fmul_rn/__fadd_rn):

@@ -70,6 +70,7 @@ struct fe_domain {
   int kind = FE_KERNEL_MARCH;        // stage-kernel form
   int mtj = 8, mni = 64;             // march kernel: rows per tile, planes per thread block
   fe_mlp* mlp = nullptr;             // learned SGS closure (nullptr: TKE closure)
+  float* feat = nullptr;             // its inputs per ring cell (allocated with the first network)
   cudaGraphExec_t graph = nullptr;
   int graphSteps = 0;
   long long launches = 0;
@@ -252,6 +253,7 @@ static void free_domain(fe_domain* d) {
   cudaFree(d->scratch);
   cudaFree(d->surf);
   cudaFree(d->frhs);
+  cudaFree(d->feat);
   cudaFree(d->clock);
   cudaFree(d->counter);
   if (d->stream) cudaStreamDestroy(d->stream);
@@ -1005,6 +1007,12 @@ extern "C" int fe_set_sgs_mlp(fe_domain* d, fe_mlp* m) {
   if (!d) return set_err(FE_ERR_ARG, "NULL handle");
   if (m && fe_learn_device(m) != d->device) return set_err(FE_ERR_ARG, "network and domain must be on one device");
   if (m && !d->P.turb) return set_err(FE_ERR_CONFIG, "the learned closure needs turbulenceSelector > 0");
+  if (m && !d->feat) {
+    CU(cudaSetDevice(d->device));
+    int rc = dev_alloc(d, &d->feat, (size_t)d->P.n * fe::SGS_NIN);
+    if (rc) return rc;
+  }
+  d->Q.feat = m ? d->feat : nullptr;
   d->mlp = m;
   invalidate_graph(d);
   return FE_OK;

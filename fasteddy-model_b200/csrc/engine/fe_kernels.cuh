@@ -13,6 +13,7 @@
 //   k_nonfinite, k_means   device reductions (NaN/Inf count, FP64 domain means)
 #pragma once
 #include "fe_device.cuh"
+#include "fe_sgs.cuh"
 
 namespace fe {
 
@@ -80,25 +81,6 @@ __global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, float* 
   else if (k >= P.kMax) src = t - k + P.kMax - 1;
   pres[t] = pert_pressure(P, st, Q.pBS, src);
 }
-
-// Primitive variables (phi/rho, formed as phi * rinv(rho)) of a cell and its neighbours, read
-// straight from the flux-form state. Offsets (di, dj, dk) are relative to cell c.
-struct GlobalPrims {
-  const float *rho, *mu, *mv, *mw, *mth, *e, *q;
-  long long n, c;
-  int si, sj;
-  __device__ __forceinline__ long long at(int di, int dj, int dk) const { return c + di * (long long)si + dj * (long long)sj + dk; }
-  __device__ __forceinline__ float r(int di, int dj, int dk) const { return rho[at(di, dj, dk)]; }
-  __device__ __forceinline__ float u(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mu[x] * rinv(rho[x]); }
-  __device__ __forceinline__ float v(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mv[x] * rinv(rho[x]); }
-  __device__ __forceinline__ float w(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mw[x] * rinv(rho[x]); }
-  __device__ __forceinline__ float th(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return mth[x] * rinv(rho[x]); }
-  __device__ __forceinline__ float ev(int di, int dj, int dk) const { const long long x = at(di, dj, dk); return e[x] * rinv(rho[x]); }
-  __device__ __forceinline__ float qm(int m, int di, int dj, int dk) const {
-    const long long x = at(di, dj, dk);
-    return q[m * n + x] * rinv(rho[x]);
-  }
-};
 
 // SGS length scale at cell c + dk (cuda_sgstkeDevice.cu:96-151), from primitives.
 template <class A>
@@ -333,6 +315,13 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
         T[7 * n + c] = -r * Km * invPr * ST2;
         T[8 * n + c] = -r * Km * invPr * ST3;
       }
+    }
+    if (Q.feat && k >= P.kMin) {
+      // inputs of the learned closure at this stress point, for its time-step kernel
+      float x[SGS_NIN];
+      sgs_inputs_a(P, Q, pr, c, x);
+#pragma unroll
+      for (int q = 0; q < SGS_NIN; q++) Q.feat[q * n + c] = x[q];
     }
     if (P.tke) {
       Q.ls[c] = lsc;

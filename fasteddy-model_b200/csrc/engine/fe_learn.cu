@@ -56,6 +56,8 @@ int attrs_set(void) {
     e = cudaFuncSetAttribute(fe::k_mlp_infer<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, fe::MlpInferSmem::BYTES);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fe::k_mlp_infer<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fe::MlpInferSmem::BYTES);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fe::k_mlp_infer<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, fe::MlpInferSmem::BYTES);
   if (e != cudaSuccess) return fe_internal_error(FE_ERR_CUDA, cudaGetErrorString(e));
   return FE_OK;
 }
@@ -94,8 +96,12 @@ int fe_learn_device(const fe_mlp* m) { return m ? m->device : -1; }
 cudaError_t fe_learn_enqueue_tau(const fe_mlp* m, const fe::Phys& P, const fe::Ptrs& Q, const float* st, cudaStream_t s) {
   const long long cells = (long long)(P.Nx + 2) * (P.Ny + 2) * (P.Nz + 1);
   const long long tiles = (cells + fe::MLP_M - 1) / fe::MLP_M;
-  fe::k_mlp_infer<1><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
-                                                                                    nullptr, 0, m->err);
+  if (Q.feat)
+    fe::k_mlp_infer<2><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
+                                                                                      nullptr, 0, m->err);
+  else
+    fe::k_mlp_infer<1><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
+                                                                                      nullptr, 0, m->err);
   return cudaGetLastError();
 }
 

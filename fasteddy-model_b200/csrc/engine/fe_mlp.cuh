@@ -222,6 +222,7 @@ __device__ __forceinline__ void sync_for_mma() {
 // SRC 1: inputs from the state at the stress points of the +1 ring (levels kMin..kMax), the
 //        9 stress/flux fields tau = rho (out_mu + out_sig y) written to Q.tau; the surface
 //        layer's tau31, tau32, tauTH3 at kMin are kept.
+// SRC 2: as SRC 1 with the inputs read from Q.feat (written by the last-stage SGS kernel).
 template <int SRC>
 __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* __restrict__ st,
                                                    const float* __restrict__ params, const MlpNorm* __restrict__ nmp,
@@ -278,7 +279,12 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* 
         j = P.jMin - 1 + (int)((row / rk) % rj);
         i = P.iMin - 1 + (int)(row / ((long long)rk * rj));
         c = (long long)i * P.si + (long long)j * P.sj + k;
-        sgs_inputs(P, Q, st, c, x);
+        if (SRC == 2) {
+#pragma unroll
+          for (int q = 0; q < SGS_NIN; q++) x[q] = Q.feat[q * P.n + c];
+        } else {
+          sgs_inputs(P, Q, st, c, x);
+        }
         rho = st[c];
       }
     }

@@ -121,3 +121,57 @@ def glorot(seed: int) -> np.ndarray:
     fill(W3, 64, 64, 64, 64)
     fill(W4, 16, 64, NOUT, 64)
     return p
+
+
+def closure_inputs(hydro: np.ndarray, J31: np.ndarray, J32: np.ndarray, J33: np.ndarray, D: np.ndarray,
+                   dX: float, dY: float, dZ: float, g: float, halo: int = 3) -> np.ndarray:
+    """FP64 closure inputs of every interior cell (rows in i, j, k order, k fastest).
+
+    hydro is the flux-form state [rho, rho u, rho v, rho w, rho theta][i][j][k] with `halo` cells
+    per side; J31/J32/J33/D the grid metrics on the same points. The 9 velocity-gradient halves
+    are the staggered strain-rate terms of cuda_sgsTurbDevice.cu:60-197 at the stress point (the
+    cell's lower faces and edges); N^2 = g/theta * dtheta/dz with the centred terrain-following
+    derivative of cuda_sgstkeDevice.cu:96-151; the grid scale is (dx dy dz D)^(1/3).
+    """
+    h = hydro.astype(np.float64)
+    r = np.maximum(h[0], 1e-6)
+    u, v, w, th = h[1] / r, h[2] / r, h[3] / r, h[4] / r
+    j1, j2, j3 = (a.astype(np.float64) for a in (J31, J32, J33))
+    nx, ny, nz = h.shape[1] - 2 * halo, h.shape[2] - 2 * halo, h.shape[3] - 2 * halo
+    dxi, dyi, dzi = 1.0 / dX, 1.0 / dY, 1.0 / dZ
+
+    def at(a, di, dj, dk):
+        return a[halo + di:halo + di + nx, halo + dj:halo + dj + ny, halo + dk:halo + dk + nz]
+
+    J1, J2, J3 = at(j1, 0, 0, 0), at(j2, 0, 0, 0), at(j3, 0, 0, 0)
+
+    def dx(a, o1, o2):  # d/dx between points o1 and o2 (o1 - o2 = one cell in x)
+        return dxi * (at(a, *o1) - at(a, *o2))
+
+    def dy(a, o1, o2):
+        return dyi * (at(a, *o1) - at(a, *o2))
+
+    def dz(a, o1, o2):
+        return dzi * (at(a, *o1) - at(a, *o2))
+
+    C, Ai, Bj, Dk = (0, 0, 0), (-1, 0, 0), (0, -1, 0), (0, 0, -1)
+    AB, AD, BD, ABD = (-1, -1, 0), (-1, 0, -1), (0, -1, -1), (-1, -1, -1)
+    x = np.empty((11, nx, ny, nz))
+    x[0] = dx(u, C, Ai)
+    x[1] = 0.5 * (dy(u, C, Bj) + dy(u, Ai, AB))
+    x[2] = (0.5 * J1 * (dx(u, C, Ai) + dx(u, Dk, AD))
+            + 0.25 * J2 * (dy(u, C, Bj) + dy(u, Ai, AB) + dy(u, Dk, BD) + dy(u, AD, ABD))
+            + 0.5 * J3 * (dz(u, C, Dk) + dz(u, Ai, AD)))
+    x[3] = 0.5 * (dx(v, C, Ai) + dx(v, Bj, AB))
+    x[4] = dy(v, C, Bj)
+    x[5] = (0.25 * J1 * (dx(v, C, Ai) + dx(v, Bj, AB) + dx(v, Dk, AD) + dx(v, BD, ABD))
+            + 0.5 * J2 * (dy(v, C, Bj) + dy(v, Dk, BD))
+            + 0.5 * J3 * (dz(v, C, Dk) + dz(v, Bj, BD)))
+    x[6] = 0.5 * (dx(w, C, Ai) + dx(w, Dk, AD))
+    x[7] = 0.5 * (dy(w, C, Bj) + dy(w, Dk, BD))
+    x[8] = J1 * dx(w, C, Ai) + J2 * dy(w, C, Bj) + J3 * dz(w, C, Dk)
+    dthdz = 0.5 * (J1 * dxi * (at(th, 1, 0, 0) - at(th, -1, 0, 0)) + J2 * dyi * (at(th, 0, 1, 0) - at(th, 0, -1, 0))
+                   + J3 * dzi * (at(th, 0, 0, 1) - at(th, 0, 0, -1)))
+    x[9] = g / at(th, 0, 0, 0) * dthdz
+    x[10] = np.cbrt(float(dX) * float(dY) * float(dZ) * at(D.astype(np.float64), 0, 0, 0))
+    return x.reshape(11, -1).T

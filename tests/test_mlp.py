@@ -141,6 +141,29 @@ def test_training_reduces_the_loss(fe):
 
 # ---------------------------------------------------------------- GPU: in the model
 @pytest.mark.gpu
+def test_closure_inputs_match_the_fp64_restatement(fe):
+    """The 11 inputs sampled on the device against the oracle's FP64 restatement from the same
+    state. Tolerances are the FP32 rounding of the primitives (a few ulps of u ~ 10 m/s and of
+    theta ~ 300 K) carried through one difference: 1e-4 of a gradient column's largest value,
+    2e-3 for N^2 (differences of theta), 1e-6 relative for the grid scale."""
+    host = fe.cases.setup_host("cbl_dry", 24, 20, 16)
+    inp, cfg = host.inputs(), host.config()
+    d = fe.Domain(cfg)
+    d.set_inputs(inp)
+    d.advance(6)
+    X = d.sgs_sample()["X"].astype(np.float64)
+    st = d.get_state()
+    ref = mo.closure_inputs(st["hydroFlds"], inp["J31"], inp["J32"], inp["J33"], inp["D_Jac"],
+                            cfg.dX, cfg.dY, cfg.dZ, cfg.accel_g)
+    for q in range(9):
+        np.testing.assert_allclose(X[:, q], ref[:, q], rtol=0, atol=1e-4 * np.abs(ref[:, q]).max())
+    np.testing.assert_allclose(X[:, 9], ref[:, 9], rtol=0, atol=2e-3 * np.abs(ref[:, 9]).max())
+    np.testing.assert_allclose(X[:, 10], ref[:, 10], rtol=1e-6)
+    d.close()
+    host.cleanup()
+
+
+@pytest.mark.gpu
 def test_learned_stresses_feed_the_time_step(fe):
     host = fe.cases.setup_host("cbl_dry", 24, 20, 16)
     inp, cfg = host.inputs(), host.config()

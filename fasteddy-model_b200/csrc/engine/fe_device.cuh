@@ -110,10 +110,17 @@ __device__ __forceinline__ float pert_pressure(const Phys& P, const float* __res
 // Perturbation pressure of the bottom halo level (k = 0) of a column after a commit: rho and
 // rho theta there are the base state, q_v the bottom copy of the first level (the reference
 // recomputes this level every stage, cuda_pressureDevice.cu:53-113; no stencil reads it).
+struct Level0 {
+  float thBS, rhoBS, pBS;
+};
+__device__ __forceinline__ Level0 level0_inputs(const Ptrs& Q, long long c0) { return {Q.thBS[c0], Q.rhoBS[c0], Q.pBS[c0]}; }
+__device__ __forceinline__ float level0_pressure(const Phys& P, const Level0& b, int nmoist, float qv) {
+  float rt = b.thBS;
+  if (nmoist > 0) rt = (float)((double)rt * (1.0 + (double)(P.Rv_Rg * qv / b.rhoBS) * 1e-3));
+  return powf(rt * P.c1, P.cp_cv) - b.pBS;
+}
 __device__ __forceinline__ float level0_pressure(const Phys& P, const Ptrs& Q, long long c0, int nmoist, float qv) {
-  float rt = Q.thBS[c0];
-  if (nmoist > 0) rt = (float)((double)rt * (1.0 + (double)(P.Rv_Rg * qv / Q.rhoBS[c0]) * 1e-3));
-  return powf(rt * P.c1, P.cp_cv) - Q.pBS[c0];
+  return level0_pressure(P, level0_inputs(Q, c0), nmoist, qv);
 }
 
 // Primitive variables (phi/rho, formed as phi * rinv(rho)) of a cell and its neighbours, read

@@ -550,10 +550,15 @@ static dim3 stage_grid(const fe_domain* d) {
   return dim3((P.Nz + d->tk - 1) / d->tk, (P.Ny + d->tj - 1) / d->tj, (P.Nx + d->ti - 1) / d->ti);
 }
 // Last-stage SGS physics on the +1 ring (k_turb_t: shared-memory tiles of primitives).
-static void launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
+// The last-stage SGS physics of the +1 ring (tiled kernel) and then the surface layer of its
+// columns; returns the number of kernels launched.
+static int launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
   const Phys& P = d->P;
   const dim3 g((P.Nz + 2 + fe::TT_K - 1) / fe::TT_K, (P.Ny + 2 + fe::TT_J - 1) / fe::TT_J, (P.Nx + 2 + fe::TT_I - 1) / fe::TT_I);
   fe::k_turb_t<<<g, dim3(fe::TT_K, fe::TT_J, fe::TT_I), 0, s>>>(P, d->Q, st, stage);
+  if (P.surf <= 0) return 1;
+  fe::k_surface<<<dim3((P.Ny + 1 + 127) / 128, P.Nx + 1), 128, 0, s>>>(P, d->Q, st, stage);
+  return 2;
 }
 
 static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }
@@ -630,20 +635,17 @@ static void enqueue_step(fe_domain* d, cudaStream_t s) {
   const bool physPrep = (P.turb || P.surf > 0);
   const bool learned = d->mlp && P.turb;
   if (physPrep && stage_has_physics(d, 0)) {
-    launch_turb(d, s, A, 0);
-    d->launches++;
+    d->launches += launch_turb(d, s, A, 0);
     if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, A, s); d->launches++; }
   }
   launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
   if (physPrep && stage_has_physics(d, 1)) {
-    launch_turb(d, s, B, 1);
-    d->launches++;
+    d->launches += launch_turb(d, s, B, 1);
     if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, B, s); d->launches++; }
   }
   launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
   if (physPrep && stage_has_physics(d, 2)) {
-    launch_turb(d, s, C, 2);
-    d->launches++;
+    d->launches += launch_turb(d, s, C, 2);
     if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, C, s); d->launches++; }
   }
   launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], nullptr);
@@ -762,8 +764,7 @@ extern "C" int fe_build_frhs(fe_domain* d, int stage) {
   }
   float* A = d->st[0];
   if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
-    launch_turb(d, d->stream, A, stage);
-    d->launches++;
+    d->launches += launch_turb(d, d->stream, A, stage);
     if (d->mlp && P.turb) {
       CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
       d->launches++;
@@ -1028,8 +1029,7 @@ extern "C" int fe_sgs_sample(fe_domain* d, long long every, float* X, float* tau
   const Phys& P = d->P;
   const long long cells = ((long long)P.Nx * P.Ny * P.Nz + every - 1) / every;
   float* A = d->st[0];
-  launch_turb(d, d->stream, A, 2);
-  d->launches++;
+  d->launches += launch_turb(d, d->stream, A, 2);
   if (d->mlp) {
     CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
     d->launches++;
@@ -1068,8 +1068,7 @@ extern "C" int fe_coarsen(fe_domain* fine, fe_domain* coarse, float* tau_target)
   if (!Pf.turb) return set_err(FE_ERR_CONFIG, "the fine domain needs an SGS closure");
   CU(cudaSetDevice(fine->device));
   // the fine model's own subgrid stresses of its current state
-  launch_turb(fine, fine->stream, fine->st[0], 2);
-  fine->launches++;
+  fine->launches += launch_turb(fine, fine->stream, fine->st[0], 2);
   const long long cells = (long long)Pc.Nx * Pc.Ny * Pc.Nz;
   float* dT = nullptr;
   if (tau_target) CU(cudaMalloc(&dT, sizeof(float) * cells * 9));

@@ -248,7 +248,7 @@ __device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __rest
 // SGS physics of ring cell (i,j,k), given the length scale of the cell (lsc) and of the level
 // below (lsm) and sqrt(e/rho) of the level below (sem), all 0 without prognostic TKE; the
 // neighbours' primitive variables come from accessor `pr` (state or shared-memory tile).
-template <class A>
+template <class A, bool SURF = true>
 __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const A& pr, const float* __restrict__ st, int i,
                                             int j, int k, float lsc, float lsm, float sem, int stage) {
   const long long n = P.n;
@@ -357,7 +357,7 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
       }
     }
   }
-  if (P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin) surface_column(P, Q, st, i, j, stage);
+  if (SURF && P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin) surface_column(P, Q, st, i, j, stage);
 }
 
 __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int k,
@@ -462,8 +462,20 @@ __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __r
   if (i > P.iMax || j > P.jMax || k > P.kMax) return;
   const TilePrims pr{tile, (tz + 1) * (TP_J * TP_K) + (ty + 1) * TP_K + (tx + 2)};
   const bool below = tke && k >= P.kMin;
-  turb_cell_a(P, Q, pr, st, i, j, k, tke ? lsT[tz][ty][tx + 1] : 0.0f, below ? lsT[tz][ty][tx] : 0.0f,
+  turb_cell_a<TilePrims, false>(P, Q, pr, st, i, j, k, tke ? lsT[tz][ty][tx + 1] : 0.0f, below ? lsT[tz][ty][tx] : 0.0f,
               below ? seT[tz][ty][tx] : 0.0f, stage);
+}
+
+// The surface layer of the columns the tiled SGS kernel covers (i in [iMin, iMax], j in
+// [jMin, jMax]), one thread per column, launched right after it. In the tiled kernel the
+// Monin-Obukhov iteration would run on one lane of every warp holding the first level while the
+// other 31 lanes wait; here every lane works. It overwrites the same first-level components
+// (tau31, tau32, tauTH3, the q_v flux) the per-cell form's in-kernel call does.
+__global__ void __launch_bounds__(128) k_surface(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+  const int j = P.jMin + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = P.iMin + blockIdx.y;
+  if (j > P.jMax || i > P.iMax) return;
+  surface_column(P, Q, st, i, j, stage);
 }
 
 // Write value v of one field at interior cell (i,j,k) and at its periodic images; `nbot`

@@ -74,6 +74,9 @@ __device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+// Pull the line holding p into L2 (no register, no wait). Only ever given addresses of cells
+// that exist in the array.
+__device__ __forceinline__ void prefetch_l2(const float* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -310,6 +313,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     __syncthreads();
   }
 
+  const bool same = (base == cur);  // first stage: the commit base is the input state
   const bool mpStep = phys && nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
 
   // ---------------------------------------------------------------- march
@@ -327,6 +331,50 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     if (pgf) pc1 = ax[8 * T::NT];
     Dn = ax[9 * T::NT];
     J1n = ax[10 * T::NT];
+    // the next plane's single-cell reads (commit base, base state, SGS fields written by the
+    // physics kernel) into L2 while this plane is computed
+    if (more && active) {
+      const long long cn = c + si;
+      if (MODE != MODE_FRHS && !same) {
+#pragma unroll
+        for (int s = 0; s < 8; s++)
+          if (f_on<FL>(P, s)) prefetch_l2(f_src<FL>(P, base, pcur, s) + cn);
+      }
+      if (MODE != MODE_FRHS) prefetch_l2(Q.pBS + cn);
+      if (P.buoy || P.cor || P.damp) prefetch_l2(Q.rhoBS + cn);
+      if (P.cor || P.damp) prefetch_l2(Q.zPos + cn);
+      if (phys && P.turb) {
+#pragma unroll
+        for (int m = 0; m < 9; m++) prefetch_l2(Q.tau + m * n + cn);
+        if (nmoist > 0 && P.moistSGS > 0)
+          for (int m = 0; m < 3 * nmoist; m++) prefetch_l2(Q.mtau + m * n + cn);
+        if (tke) {
+#pragma unroll
+          for (int m = 0; m < 3; m++) prefetch_l2(Q.tkeQ + m * n + cn);
+          prefetch_l2(Q.ls + cn);
+          if (Q.delta) prefetch_l2(Q.delta + cn);
+        }
+      }
+    }
+    // inputs of this plane's commit, loaded before the advection so that their memory latency
+    // overlaps it (and before any store of the plane: the stores may alias `base`)
+    float cb[8];
+    float pbs = 0.0f;
+#pragma unroll
+    for (int s = 0; s < 8; s++) cb[s] = 0.0f;
+    if (MODE != MODE_FRHS && active) {
+#pragma unroll
+      for (int s = 0; s < 8; s++)
+        if (f_on<FL>(P, s) && !same) cb[s] = f_src<FL>(P, base, pcur, s)[c];
+      pbs = Q.pBS[c];
+    }
+    // base state of the buoyancy, Rayleigh and Coriolis terms
+    float zc = 0.0f, ztop = 0.0f, rbsc = 0.0f;
+    if (inArr) {
+      if (P.buoy || P.cor || P.damp) rbsc = Q.rhoBS[c];
+      if (P.cor || P.damp) zc = Q.zPos[c];
+      if (P.damp) ztop = Q.zPos[c - k + (P.kMax - 1)];
+    }
     if (more) issue_aux(i, aux + ((i - i0) & 1) * T::NAUX * T::NT);
     if (more) issue_ring(i + 1, ns);
     float rD = 0.0f, rR = 1.0f, rM = 0.0f, rW = 0.0f, rJ = 0.0f;
@@ -420,10 +468,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       if (s == 3) {
         // Rayleigh damping and buoyancy act on F_w right after its advection
         if (P.damp && inArr) {
-          const long long ctop = c - k + (P.kMax - 1);
-          const float z = Q.zPos[c], zt = Q.zPos[ctop];
+          const float z = zc, zt = ztop;
           if (z >= (zt - P.dampDepth)) {
-            const float rbs = Q.rhoBS[c];
+            const float rbs = rbsc;
             const float wbs = momentum_bs(P, 3, z, rbs);
             const float pio2 = 1.5707963267948966f;
             const double sn = (double)sinf((float)((double)pio2 * (1.0 - (double)((zt - z) / P.dampDepth))));
@@ -431,7 +478,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
           }
         }
         if (P.buoy) {
-          const float rbs = inArr ? Q.rhoBS[c] : 0.0f;
+          const float rbs = rbsc;
           if (nmoist > 0) {
             double rm = (double)r0 + (double)w[SL_QV][0] * 1e-3;
             if (nmoist == 2) rm += (double)w[SL_QL][0] * 1e-3;
@@ -446,7 +493,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
 
     // Coriolis (cuda_coriolisDevice.cu:50-58)
     if (P.cor && inArr) {
-      const float z = Q.zPos[c], rbs = Q.rhoBS[c];
+      const float z = zc, rbs = rbsc;
       const float ubs = momentum_bs(P, 1, z, rbs), vbs = momentum_bs(P, 2, z, rbs), wbs = momentum_bs(P, 3, z, rbs);
       F[1] = F[1] + (P.fHorz * (w[2][0] / r0 - P.fLS * vbs / rbs) - P.fVert * (w[3][0] / r0 - P.fLS * wbs / rbs));
       F[2] = F[2] - (P.fHorz * (w[1][0] / r0 - P.fLS * ubs / rbs));
@@ -580,14 +627,20 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
           if (STAGE == 1) return (float)fma(0.5 * (double)P.dt, (double)Fv, (double)phi0);
           return __fmaf_rn(P.dt, Fv, phi0);
         };
-        const bool same = (base == cur);
-        auto b0 = [&](int s, long long off) -> float { return same ? w[s][0] : base[off + c]; };
-        const float n0 = rk(b0(0, 0), F[0]);
-        const float n1 = rk(b0(1, n), F[1]);
-        const float n2 = rk(b0(2, 2 * n), F[2]);
-        const float n3 = rk(b0(3, 3 * n), F[3]);
-        const float n4 = rk(b0(4, 4 * n), F[4]);
+        auto b0 = [&](int s) -> float { return same ? w[s][0] : cb[s]; };
+        const long long oq = (5 + ntke) * n;
+        const float a0 = b0(0), a1 = b0(1), a2 = b0(2), a3 = b0(3), a4 = b0(4);
+        const float ae = ntke ? b0(SL_E) : 0.0f;
+        const float aq0 = nmoist > 0 ? b0(SL_QV) : 0.0f;
+        const float aq1 = nmoist > 1 ? b0(SL_QL) : 0.0f;
         const bool atBot = (k == P.kMin), atTop = (k == P.kMax - 1);
+        Level0 l0{};
+        if (atBot) l0 = level0_inputs(Q, c - k);
+        const float n0 = rk(a0, F[0]);
+        const float n1 = rk(a1, F[1]);
+        const float n2 = rk(a2, F[2]);
+        const float n3 = rk(a3, F[3]);
+        const float n4 = rk(a4, F[4]);
         store_images(P, nxt, i, j, k, n0, 0, false);
         store_images(P, nxt + n, i, j, k, n1, atBot ? 3 : 0, false);
         store_images(P, nxt + 2 * n, i, j, k, n2, atBot ? 3 : 0, false);
@@ -595,26 +648,25 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         store_images(P, nxt + 4 * n, i, j, k, n4, 0, false);
         float nq0 = 0.0f;
         if (ntke) {
-          const float ne = fmaxf(rk(b0(SL_E, 5 * n), F[SL_E]), 1e-10f);
+          const float ne = fmaxf(rk(ae, F[SL_E]), 1e-10f);
           store_images(P, nxt + 5 * n, i, j, k, ne, atBot ? 3 : 0, false);
         }
         if (nmoist > 0) {
-          const long long o = (5 + ntke) * n;
-          nq0 = fmaxf(rk(b0(SL_QV, o), F[SL_QV]), 0.0f);
-          store_images(P, nxt + o, i, j, k, nq0, atBot ? 3 : 0, atTop);
+          nq0 = fmaxf(rk(aq0, F[SL_QV]), 0.0f);
+          store_images(P, nxt + oq, i, j, k, nq0, atBot ? 3 : 0, atTop);
           if (nmoist > 1) {
-            const float nq1 = fmaxf(rk(b0(SL_QL, o + n), F[SL_QL]), 0.0f);
-            store_images(P, nxt + o + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
+            const float nq1 = fmaxf(rk(aq1, F[SL_QL]), 0.0f);
+            store_images(P, nxt + oq + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
           }
         }
         float pn;
         {
           float rtm = n4;
           if (nmoist > 0) rtm = (float)((double)n4 * (1.0 + (double)(P.Rv_Rg * nq0 / n0) * 1e-3));
-          pn = powf(rtm * P.c1, P.cp_cv) - Q.pBS[c];
+          pn = powf(rtm * P.c1, P.cp_cv) - pbs;
         }
         store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
-        if (atBot) store_images(P, pnxt, i, j, 0, level0_pressure(P, Q, c - k, nmoist, nq0), 0, false);
+        if (atBot) store_images(P, pnxt, i, j, 0, level0_pressure(P, l0, nmoist, nq0), 0, false);
       }
     }
 

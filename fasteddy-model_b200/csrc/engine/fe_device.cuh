@@ -59,6 +59,7 @@ struct Ptrs {
   float *cd, *ch, *cq, *fricVel, *htFlux, *tskin, *invOblen, *z0m, *z0t, *qFlux, *qskin;
   const float* delta;          // grid scale (dx dy dz D)^(1/3) per cell, or nullptr (evaluated inline)
   float* feat;                 // inputs of the learned closure per ring cell (11 fields), or nullptr
+  float* sgsF;                 // SGS tendencies for the march kernel's physics stages (7 fields), or nullptr
   int *clockIt;                // simTime_it of the step being computed
   float *clockTime;            // simTime of the step being computed
 };

@@ -286,7 +286,8 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
     rc = dev_alloc(d, &d->st[b], n * P.nf);
     if (rc == FE_OK) rc = dev_alloc(d, &d->pr[b], n);
   }
-  const size_t nscr = (size_t)(9 + 3 + 1 + 3 * std::max(P.nmoist, 1));
+  const size_t nsgs = (size_t)(9 + 3 + 1 + 3 * std::max(P.nmoist, 1));
+  const size_t nscr = nsgs + (P.turb ? 7 : 0);  // + the march kernel's SGS tendencies
   if (rc == FE_OK) rc = dev_alloc(d, &d->grid, n * 7);
   if (rc == FE_OK) rc = dev_alloc(d, &d->base, n * 3);
   if (rc == FE_OK) rc = dev_alloc(d, &d->scratch, n * nscr);
@@ -316,6 +317,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   Q.tkeQ = d->scratch + 9 * n;
   Q.ls = d->scratch + 12 * n;
   Q.mtau = d->scratch + 13 * n;
+  Q.sgsF = P.turb ? d->scratch + nsgs * n : nullptr;
   float* s = d->surf;
   Q.cd = s; Q.ch = s + n2; Q.cq = s + 2 * n2; Q.fricVel = s + 3 * n2; Q.htFlux = s + 4 * n2; Q.tskin = s + 5 * n2;
   Q.invOblen = s + 6 * n2; Q.z0m = s + 7 * n2; Q.z0t = s + 8 * n2; Q.qFlux = s + 9 * n2; Q.qskin = s + 10 * n2;
@@ -561,6 +563,23 @@ static int launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int 
   return 2;
 }
 
+// Everything a physics stage needs before its stage kernel, on state st: the SGS kernel and
+// surface layer, the learned closure's stresses (when a network is set) and, for the march
+// kernel, the SGS tendencies it reads. Returns the number of kernels launched.
+static int launch_physics(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
+  const Phys& P = d->P;
+  int l = launch_turb(d, s, st, stage);
+  if (d->mlp && P.turb) {
+    fe_learn_enqueue_tau(d->mlp, P, d->Q, st, s);
+    l++;
+  }
+  if (d->kind == FE_KERNEL_MARCH && P.turb) {
+    fe::k_sgs_tend<<<dim3((P.Nz + 31) / 32, (P.Ny + 7) / 8, P.Nx), dim3(32, 8), 0, s>>>(P, d->Q, st);
+    l++;
+  }
+  return l;
+}
+
 static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK == 0 || stage == 2; }
 
 // Dynamic shared memory limits of the march kernels (three plane buffers exceed the 48 KB
@@ -633,21 +652,11 @@ static void enqueue_step(fe_domain* d, cudaStream_t s) {
   const Ptrs& Q = d->Q;
   float *A = d->st[0], *B = d->st[1], *C = d->st[2];
   const bool physPrep = (P.turb || P.surf > 0);
-  const bool learned = d->mlp && P.turb;
-  if (physPrep && stage_has_physics(d, 0)) {
-    d->launches += launch_turb(d, s, A, 0);
-    if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, A, s); d->launches++; }
-  }
+  if (physPrep && stage_has_physics(d, 0)) d->launches += launch_physics(d, s, A, 0);
   launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
-  if (physPrep && stage_has_physics(d, 1)) {
-    d->launches += launch_turb(d, s, B, 1);
-    if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, B, s); d->launches++; }
-  }
+  if (physPrep && stage_has_physics(d, 1)) d->launches += launch_physics(d, s, B, 1);
   launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
-  if (physPrep && stage_has_physics(d, 2)) {
-    d->launches += launch_turb(d, s, C, 2);
-    if (learned) { fe_learn_enqueue_tau(d->mlp, P, Q, C, s); d->launches++; }
-  }
+  if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2);
   launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], nullptr);
   fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
   d->launches += 4;
@@ -675,8 +684,12 @@ static int build_graph(fe_domain* d) {
 }
 
 static int launches_per_step(const fe_domain* d) {
+  const Phys& P = d->P;
   int l = 4;
-  if (d->P.turb || d->P.surf > 0) l += (d->P.oneRK ? 1 : 3) * ((d->mlp && d->P.turb) ? 2 : 1);
+  if (P.turb || P.surf > 0) {
+    const int phys = 1 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) + ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
+    l += (P.oneRK ? 1 : 3) * phys;
+  }
   return l;
 }
 
@@ -764,11 +777,8 @@ extern "C" int fe_build_frhs(fe_domain* d, int stage) {
   }
   float* A = d->st[0];
   if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
-    d->launches += launch_turb(d, d->stream, A, stage);
-    if (d->mlp && P.turb) {
-      CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
-      d->launches++;
-    }
+    d->launches += launch_physics(d, d->stream, A, stage);
+    CU(cudaGetLastError());
   }
   switch (stage) {
     case 0: launch_stage<0, fe::MODE_FRHS>(d, d->stream, A, A, nullptr, d->pr[0], nullptr, d->frhs); break;

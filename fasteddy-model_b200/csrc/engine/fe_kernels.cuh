@@ -250,7 +250,7 @@ __device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __rest
 // neighbours' primitive variables come from accessor `pr` (state or shared-memory tile).
 template <class A, bool SURF = true>
 __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const A& pr, const float* __restrict__ st, int i,
-                                            int j, int k, float lsc, float lsm, float sem, int stage) {
+                                            int j, int k, float lsc, float lsm, float sem, float sec, int stage) {
   const long long n = P.n;
   const long long c = (long long)i * P.si + (long long)j * P.sj + k;
   if (P.turb) {
@@ -284,7 +284,8 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
       const float r = pr.r(0, 0, 0);
       if (P.tke) {
         const float e0 = pr.ev(0, 0, 0);
-        Km = (float)((double)P.c_k * 0.5 * (double)(lsc * powf(e0, 0.5f) + lsm * sem));
+        const float se0 = sec >= 0.0f ? sec : powf(e0, 0.5f);  // sqrt(e/rho) of this cell (given by the tiled form)
+        Km = (float)((double)P.c_k * 0.5 * (double)(lsc * se0 + lsm * sem));
         const float invPr = 1.0f + 2.0f * lsc / delta;
         const float dev = (float)((2.0 / 3.0) * (double)r *
                                   (double)(Km * (dXi * (uc - ua) + dYi * (vc - vb) + J1 * dXi * (wc - wa) +
@@ -365,7 +366,7 @@ __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const fl
   const long long n = P.n;
   GlobalPrims pr{st, st + n, st + 2 * n, st + 3 * n, st + 4 * n, P.ntke ? st + 5 * n : nullptr,
                  P.nmoist ? st + (5 + P.ntke) * n : nullptr, n, (long long)i * P.si + (long long)j * P.sj + k, P.si, P.sj};
-  turb_cell_a(P, Q, pr, st, i, j, k, lsc, lsm, sem, stage);
+  turb_cell_a(P, Q, pr, st, i, j, k, lsc, lsm, sem, -1.0f, stage);
 }
 
 // One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
@@ -463,7 +464,7 @@ __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __r
   const TilePrims pr{tile, (tz + 1) * (TP_J * TP_K) + (ty + 1) * TP_K + (tx + 2)};
   const bool below = tke && k >= P.kMin;
   turb_cell_a<TilePrims, false>(P, Q, pr, st, i, j, k, tke ? lsT[tz][ty][tx + 1] : 0.0f, below ? lsT[tz][ty][tx] : 0.0f,
-              below ? seT[tz][ty][tx] : 0.0f, stage);
+              below ? seT[tz][ty][tx] : 0.0f, tke ? seT[tz][ty][tx + 1] : -1.0f, stage);
 }
 
 // The surface layer of the columns the tiled SGS kernel covers (i in [iMin, iMax], j in

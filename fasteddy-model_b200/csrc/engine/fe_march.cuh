@@ -24,6 +24,8 @@
 // of the new state -- is the cell kernel's arithmetic (fe_kernels.cuh), term by term and in the
 // same order, evaluated on the register/shared copies.
 #pragma once
+#include <type_traits>
+
 #include "fe_kernels.cuh"
 
 namespace fe {
@@ -135,6 +137,94 @@ __device__ __forceinline__ const float* f_src(const Phys& P, const float* cur, c
   } else {
     return slot_src(P, cur, pcur, s);
   }
+}
+
+// SGS tendencies of the last-stage physics for the march kernel, one thread per interior cell
+// (levels along x of the block): with the SGS stresses and fluxes written by the SGS kernel (and
+// the learned closure, when set), seven fields of Q.sgsF at the cell's index:
+//   0..3  divergence of the stresses on rho u, rho v, rho w and of the heat flux on rho theta
+//         (cuda_sgsTurbDevice.cu:447-547), subtracted from the tendency
+//   4     the TKE budget: buoyancy, dissipation, shear production and transport
+//         (cuda_sgstkeDevice.cu:155-397), added
+//   5, 6  divergence of the q_v and q_l SGS fluxes, subtracted
+// Each expression is the per-cell stage kernel's; the TKE terms are summed here and added to the
+// tendency once. `st` is the stage's input state; the shear production's velocity gradients use
+// central differences of phi/rho at the six neighbours.
+__global__ void __launch_bounds__(256) k_sgs_tend(Phys P, Ptrs Q, const float* __restrict__ st) {
+  const int k = P.kMin + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = P.jMin + blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = P.iMin + blockIdx.z;
+  if (k >= P.kMax || j >= P.jMax) return;
+  const long long n = P.n;
+  const int si = P.si, sj = P.sj;
+  const long long c = (long long)i * si + (long long)j * sj + k;
+  const long long ip = c + si, jp = c + sj, kp = c + 1;
+  const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
+  const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
+  const float* Tt = Q.tau;
+#define TT(m, x) Tt[(m) * n + (x)]
+  // all loads before the first store: the compiler cannot tell the output from the inputs
+  const float s0 = dXi * (TT(0, ip) - TT(0, c)) + dYi * (TT(1, jp) - TT(1, c)) + J1 * dXi * (TT(2, ip) - TT(2, c)) +
+         J2 * dYi * (TT(2, jp) - TT(2, c)) + J3 * dZi * (TT(2, kp) - TT(2, c));
+  const float s1 = dXi * (TT(1, ip) - TT(1, c)) + dYi * (TT(4, jp) - TT(4, c)) + J1 * dXi * (TT(3, ip) - TT(3, c)) +
+             J2 * dYi * (TT(3, jp) - TT(3, c)) + J3 * dZi * (TT(3, kp) - TT(3, c));
+  const float s2 = dXi * (TT(2, ip) - TT(2, c)) + dYi * (TT(3, jp) - TT(3, c)) + J1 * dXi * (TT(5, ip) - TT(5, c)) +
+                 J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c));
+  const float s3 = dXi * (TT(6, ip) - TT(6, c)) + dYi * (TT(7, jp) - TT(7, c)) + J1 * dXi * (TT(8, ip) - TT(8, c)) +
+                 J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c));
+  float sq[2] = {0.0f, 0.0f};
+  const int nq = (P.nmoist > 0 && P.moistSGS > 0) ? min(P.nmoist, 2) : 0;
+  if (nq > 0) {
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      if (m >= nq) break;
+      const float* M = Q.mtau + 3 * m * n;
+      sq[m] = dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) + J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) +
+                           J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) + J3 * dZi * (M[2 * n + kp] - M[2 * n + c]);
+    }
+  }
+  float se = 0.0f;
+  if (P.tke) {
+    const float r0 = st[c];
+    const float ri = rinv(r0);
+    const float delta = grid_scale(P, Q, c);
+    const float lsc = Q.ls[c];
+    const float mec = st[5 * n + c];
+    float Se = P.g / (st[4 * n + c] * ri) * TT(8, c);
+    const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
+    const float ec = mec * ri;
+    Se = Se + (-ce * mec * powf(ec, 0.5f) / lsc);
+    // (rho phi)/rho of field f at the neighbour c + o
+    auto G = [&](int f, long long o) -> float { return st[f * n + c + o] * rinv(st[c + o]); };
+    const float ux = G(1, si) - G(1, -si), uy = G(1, sj) - G(1, -sj), uz = G(1, 1) - G(1, -1);
+    const float vx = G(2, si) - G(2, -si), vy = G(2, sj) - G(2, -sj), vz = G(2, 1) - G(2, -1);
+    const float wx = G(3, si) - G(3, -si), wy = G(3, sj) - G(3, -sj), wz = G(3, 1) - G(3, -1);
+    const float dux = 0.5f * (dXi * ux), duy = 0.5f * (dYi * uy);
+    const float duz = 0.5f * (J1 * dXi * ux + J2 * dYi * uy + J3 * dZi * uz);
+    const float dvx = 0.5f * (dXi * vx), dvy = 0.5f * (dYi * vy);
+    const float dvz = 0.5f * (J1 * dXi * vx + J2 * dYi * vy + J3 * dZi * vz);
+    const float dwx = 0.5f * (dXi * wx), dwy = 0.5f * (dYi * wy);
+    const float dwz = 0.5f * (J1 * dXi * wx + J2 * dYi * wy + J3 * dZi * wz);
+    const float shear = (-TT(0, c) * dux) + (-TT(1, c) * duy) + (-TT(2, c) * duz) + (-TT(1, c) * dvx) +
+                        (-TT(4, c) * dvy) + (-TT(3, c) * dvz) + (-TT(2, c) * dwx) + (-TT(3, c) * dwy) + (-TT(5, c) * dwz);
+    Se = Se + shear;
+    const float* Gq = Q.tkeQ;
+    const long long im = c - si, jm = c - sj, km = c - 1;
+    const float tx_ = -(dXi * (Gq[ip] - Gq[im]));
+    const float ty_ = -(dYi * (Gq[n + jp] - Gq[n + jm]));
+    const float tz_ = -(J1 * dXi * (Gq[2 * n + ip] - Gq[2 * n + im]) + J2 * dYi * (Gq[2 * n + jp] - Gq[2 * n + jm]) +
+                        J3 * dZi * (Gq[2 * n + kp] - Gq[2 * n + km]));
+    Se = Se + (-(tx_ + ty_ + tz_));
+    se = Se;
+  }
+#undef TT
+  float* S = Q.sgsF + c;
+  S[0] = s0;
+  S[n] = s1;
+  S[2 * n] = s2;
+  S[3 * n] = s3;
+  if (P.tke) S[4 * n] = se;
+  for (int m = 0; m < nq; m++) S[(5 + m) * n] = sq[m];
 }
 
 template <int STAGE, int MODE, int TJ, int FL>
@@ -345,15 +435,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       if (P.cor || P.damp) prefetch_l2(Q.zPos + cn);
       if (phys && P.turb) {
 #pragma unroll
-        for (int m = 0; m < 9; m++) prefetch_l2(Q.tau + m * n + cn);
+        for (int m = 0; m < 5; m++) prefetch_l2(Q.sgsF + m * n + cn);
         if (nmoist > 0 && P.moistSGS > 0)
-          for (int m = 0; m < 3 * nmoist; m++) prefetch_l2(Q.mtau + m * n + cn);
-        if (tke) {
-#pragma unroll
-          for (int m = 0; m < 3; m++) prefetch_l2(Q.tkeQ + m * n + cn);
-          prefetch_l2(Q.ls + cn);
-          if (Q.delta) prefetch_l2(Q.delta + cn);
-        }
+          for (int m = 0; m < nmoist; m++) prefetch_l2(Q.sgsF + (5 + m) * n + cn);
       }
     }
     // inputs of this plane's commit, loaded before the advection so that their memory latency
@@ -367,6 +451,20 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       for (int s = 0; s < 8; s++)
         if (f_on<FL>(P, s) && !same) cb[s] = f_src<FL>(P, base, pcur, s)[c];
       pbs = Q.pBS[c];
+    }
+    // SGS tendencies of this cell (k_sgs_tend): stress divergence on rho u, rho v, rho w, heat
+    // flux divergence, the TKE budget, moisture flux divergences
+    float sg[7];
+#pragma unroll
+    for (int m = 0; m < 7; m++) sg[m] = 0.0f;
+    if (phys && P.turb && active) {
+#pragma unroll
+      for (int m = 0; m < 4; m++) sg[m] = Q.sgsF[m * n + c];
+      if (tke) sg[4] = Q.sgsF[4 * n + c];
+      if (nmoist > 0 && P.moistSGS > 0) {
+        sg[5] = Q.sgsF[5 * n + c];
+        if (nmoist > 1) sg[6] = Q.sgsF[6 * n + c];
+      }
     }
     // base state of the buoyancy, Rayleigh and Coriolis terms
     float zc = 0.0f, ztop = 0.0f, rbsc = 0.0f;
@@ -501,74 +599,15 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     }
 
     if (phys && P.turb && active) {
-      // divergence of the SGS stresses (cuda_sgsTurbDevice.cu:447-547)
-      const float* Tt = Q.tau;
-      const long long ip = c + si, jp = c + sj, kp = c + 1;
-#define TT(m, x) Tt[(m) * n + (x)]
-      F[1] = F[1] - (dXi * (TT(0, ip) - TT(0, c)) + dYi * (TT(1, jp) - TT(1, c)) + J1 * dXi * (TT(2, ip) - TT(2, c)) +
-                     J2 * dYi * (TT(2, jp) - TT(2, c)) + J3 * dZi * (TT(2, kp) - TT(2, c)));
-      F[2] = F[2] - (dXi * (TT(1, ip) - TT(1, c)) + dYi * (TT(4, jp) - TT(4, c)) + J1 * dXi * (TT(3, ip) - TT(3, c)) +
-                     J2 * dYi * (TT(3, jp) - TT(3, c)) + J3 * dZi * (TT(3, kp) - TT(3, c)));
-      F[3] = F[3] - (dXi * (TT(2, ip) - TT(2, c)) + dYi * (TT(3, jp) - TT(3, c)) + J1 * dXi * (TT(5, ip) - TT(5, c)) +
-                     J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c)));
-      F[4] = F[4] - (dXi * (TT(6, ip) - TT(6, c)) + dYi * (TT(7, jp) - TT(7, c)) + J1 * dXi * (TT(8, ip) - TT(8, c)) +
-                     J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c)));
+      F[1] = F[1] - sg[0];
+      F[2] = F[2] - sg[1];
+      F[3] = F[3] - sg[2];
+      F[4] = F[4] - sg[3];
+      if (tke) F[SL_E] = F[SL_E] + sg[4];
       if (nmoist > 0 && P.moistSGS > 0) {
-        const float* M = Q.mtau;
-        F[SL_QV] = F[SL_QV] - (dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) +
-                               J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) + J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) +
-                               J3 * dZi * (M[2 * n + kp] - M[2 * n + c]));
-        if (nmoist > 1) {
-          const float* M1 = M + 3 * n;
-          F[SL_QL] = F[SL_QL] - (dXi * (M1[ip] - M1[c]) + dYi * (M1[n + jp] - M1[n + c]) +
-                                 J1 * dXi * (M1[2 * n + ip] - M1[2 * n + c]) + J2 * dYi * (M1[2 * n + jp] - M1[2 * n + c]) +
-                                 J3 * dZi * (M1[2 * n + kp] - M1[2 * n + c]));
-        }
+        F[SL_QV] = F[SL_QV] - sg[5];
+        if (nmoist > 1) F[SL_QL] = F[SL_QL] - sg[6];
       }
-      // SGS TKE budget (cuda_sgstkeDevice.cu:155-397)
-      if (tke) {
-        const float ri = rinv(r0);
-        const float delta = grid_scale(P, Q, c);
-        const float lsc = Q.ls[c];
-        const float mec = w[SL_E][0];
-        float Fe = F[SL_E];
-        Fe = Fe + P.g / (w[4][0] * ri) * TT(8, c);
-        const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
-        const float ec = mec * ri;
-        Fe = Fe + (-ce * mec * powf(ec, 0.5f) / lsc);
-        const float* pr = cs + own;  // rho plane
-        auto G = [&](int s, int dir, int sgn) -> float {
-          // (rho phi)/rho at a neighbour: dir 0 = x (registers), 1 = y, 2 = z (shared plane)
-          if (dir == 0) return sgn > 0 ? w[s][1] * rinv(w[0][1]) : ps[s * PLANE + own] * rinv(ps[own]);
-          const int o = dir == 1 ? sgn * PK : sgn;
-          return cs[s * PLANE + own + o] * rinv(pr[o]);
-        };
-        const float dux = 0.5f * (dXi * (G(1, 0, 1) - G(1, 0, -1)));
-        const float duy = 0.5f * (dYi * (G(1, 1, 1) - G(1, 1, -1)));
-        const float duz = 0.5f * (J1 * dXi * (G(1, 0, 1) - G(1, 0, -1)) + J2 * dYi * (G(1, 1, 1) - G(1, 1, -1)) +
-                                  J3 * dZi * (G(1, 2, 1) - G(1, 2, -1)));
-        const float dvx = 0.5f * (dXi * (G(2, 0, 1) - G(2, 0, -1)));
-        const float dvy = 0.5f * (dYi * (G(2, 1, 1) - G(2, 1, -1)));
-        const float dvz = 0.5f * (J1 * dXi * (G(2, 0, 1) - G(2, 0, -1)) + J2 * dYi * (G(2, 1, 1) - G(2, 1, -1)) +
-                                  J3 * dZi * (G(2, 2, 1) - G(2, 2, -1)));
-        const float dwx = 0.5f * (dXi * (G(3, 0, 1) - G(3, 0, -1)));
-        const float dwy = 0.5f * (dYi * (G(3, 1, 1) - G(3, 1, -1)));
-        const float dwz = 0.5f * (J1 * dXi * (G(3, 0, 1) - G(3, 0, -1)) + J2 * dYi * (G(3, 1, 1) - G(3, 1, -1)) +
-                                  J3 * dZi * (G(3, 2, 1) - G(3, 2, -1)));
-        const float shear = (-TT(0, c) * dux) + (-TT(1, c) * duy) + (-TT(2, c) * duz) + (-TT(1, c) * dvx) +
-                            (-TT(4, c) * dvy) + (-TT(3, c) * dvz) + (-TT(2, c) * dwx) + (-TT(3, c) * dwy) +
-                            (-TT(5, c) * dwz);
-        Fe = Fe + shear;
-        const float* Gq = Q.tkeQ;
-        const long long im = c - si, jm = c - sj, km = c - 1;
-        const float tx_ = -(dXi * (Gq[ip] - Gq[im]));
-        const float ty_ = -(dYi * (Gq[n + jp] - Gq[n + jm]));
-        const float tz_ = -(J1 * dXi * (Gq[2 * n + ip] - Gq[2 * n + im]) + J2 * dYi * (Gq[2 * n + jp] - Gq[2 * n + jm]) +
-                            J3 * dZi * (Gq[2 * n + kp] - Gq[2 * n + km]));
-        Fe = Fe + (-(tx_ + ty_ + tz_));
-        F[SL_E] = Fe;
-      }
-#undef TT
     }
 
     // saturation adjustment (cuda_moistureDevice.cu:80-247)
@@ -641,32 +680,37 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         const float n2 = rk(a2, F[2]);
         const float n3 = rk(a3, F[3]);
         const float n4 = rk(a4, F[4]);
-        store_images(P, nxt, i, j, k, n0, 0, false);
-        store_images(P, nxt + n, i, j, k, n1, atBot ? 3 : 0, false);
-        store_images(P, nxt + 2 * n, i, j, k, n2, atBot ? 3 : 0, false);
-        store_images(P, nxt + 3 * n, i, j, k, n3, atBot ? 3 : 0, false);
-        store_images(P, nxt + 4 * n, i, j, k, n4, 0, false);
-        float nq0 = 0.0f;
-        if (ntke) {
-          const float ne = fmaxf(rk(ae, F[SL_E]), 1e-10f);
-          store_images(P, nxt + 5 * n, i, j, k, ne, atBot ? 3 : 0, false);
-        }
-        if (nmoist > 0) {
-          nq0 = fmaxf(rk(aq0, F[SL_QV]), 0.0f);
-          store_images(P, nxt + oq, i, j, k, nq0, atBot ? 3 : 0, atTop);
-          if (nmoist > 1) {
-            const float nq1 = fmaxf(rk(aq1, F[SL_QL]), 0.0f);
-            store_images(P, nxt + oq + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
-          }
-        }
+        const float ne = ntke ? fmaxf(rk(ae, F[SL_E]), 1e-10f) : 0.0f;
+        const float nq0 = nmoist > 0 ? fmaxf(rk(aq0, F[SL_QV]), 0.0f) : 0.0f;
+        const float nq1 = nmoist > 1 ? fmaxf(rk(aq1, F[SL_QL]), 0.0f) : 0.0f;
         float pn;
         {
           float rtm = n4;
           if (nmoist > 0) rtm = (float)((double)n4 * (1.0 + (double)(P.Rv_Rg * nq0 / n0) * 1e-3));
           pn = powf(rtm * P.c1, P.cp_cv) - pbs;
         }
-        store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
-        if (atBot) store_images(P, pnxt, i, j, 0, level0_pressure(P, l0, nmoist, nq0), 0, false);
+        const float p0 = atBot ? level0_pressure(P, l0, nmoist, nq0) : 0.0f;
+        // The stores, once with the periodic images of cells within 3 of an x or y edge and once
+        // without (every other column: one store per field plus the bottom/top halo copies).
+        auto stores = [&](auto edge) {
+          auto put = [&](float* Fd, float v, int nbot, bool top) {
+            if constexpr (decltype(edge)::value) store_images(P, Fd, i, j, k, v, nbot, top);
+            else store_column(Fd, c, v, nbot, top);
+          };
+          put(nxt, n0, 0, false);
+          put(nxt + n, n1, atBot ? 3 : 0, false);
+          put(nxt + 2 * n, n2, atBot ? 3 : 0, false);
+          put(nxt + 3 * n, n3, atBot ? 3 : 0, false);
+          put(nxt + 4 * n, n4, 0, false);
+          if (ntke) put(nxt + 5 * n, ne, atBot ? 3 : 0, false);
+          if (nmoist > 0) put(nxt + oq, nq0, atBot ? 3 : 0, atTop);
+          if (nmoist > 1) put(nxt + oq + n, nq1, atBot ? 3 : 0, atTop);
+          put(pnxt, pn, atBot ? 2 : 0, atTop);
+        };
+        const bool xyEdge = (i < P.iMin + 3) || (i >= P.iMax - 3) || (j < P.jMin + 3) || (j >= P.jMax - 3);
+        if (xyEdge) stores(std::true_type{});
+        else stores(std::false_type{});
+        if (atBot) store_images(P, pnxt, i, j, 0, p0, 0, false);
       }
     }
 

@@ -574,7 +574,17 @@ static int launch_physics(const fe_domain* d, cudaStream_t s, const float* st, i
     l++;
   }
   if (d->kind == FE_KERNEL_MARCH && P.turb) {
-    fe::k_sgs_tend<<<dim3((P.Nz + 31) / 32, (P.Ny + 7) / 8, P.Nx), dim3(32, 8), 0, s>>>(P, d->Q, st);
+    const dim3 g((P.Nz + 31) / 32, (P.Ny + 7) / 8, P.Nx), b(32, 8);
+    const int nq = (P.nmoist > 0 && P.moistSGS > 0) ? std::min(P.nmoist, 2) : 0;
+    if (P.tke) {
+      if (nq == 2) fe::k_sgs_tend<true, 2><<<g, b, 0, s>>>(P, d->Q, st);
+      else if (nq == 1) fe::k_sgs_tend<true, 1><<<g, b, 0, s>>>(P, d->Q, st);
+      else fe::k_sgs_tend<true, 0><<<g, b, 0, s>>>(P, d->Q, st);
+    } else {
+      if (nq == 2) fe::k_sgs_tend<false, 2><<<g, b, 0, s>>>(P, d->Q, st);
+      else if (nq == 1) fe::k_sgs_tend<false, 1><<<g, b, 0, s>>>(P, d->Q, st);
+      else fe::k_sgs_tend<false, 0><<<g, b, 0, s>>>(P, d->Q, st);
+    }
     l++;
   }
   return l;

@@ -149,8 +149,10 @@ __device__ __forceinline__ const float* f_src(const Phys& P, const float* cur, c
 //   5, 6  divergence of the q_v and q_l SGS fluxes, subtracted
 // Each expression is the per-cell stage kernel's; the TKE terms are summed here and added to the
 // tendency once. `st` is the stage's input state; the shear production's velocity gradients use
-// central differences of phi/rho at the six neighbours.
-__global__ void __launch_bounds__(256) k_sgs_tend(Phys P, Ptrs Q, const float* __restrict__ st) {
+// central differences of phi/rho at the six neighbours. TKE (prognostic TKE) and NQ (moisture
+// species with SGS fluxes) are compile-time so that every load of a cell issues as one batch.
+template <bool TKE, int NQ>
+__global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float* __restrict__ st) {
   const int k = P.kMin + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = P.jMin + blockIdx.y * blockDim.y + threadIdx.y;
   const int i = P.iMin + blockIdx.z;
@@ -165,26 +167,22 @@ __global__ void __launch_bounds__(256) k_sgs_tend(Phys P, Ptrs Q, const float* _
 #define TT(m, x) Tt[(m) * n + (x)]
   // all loads before the first store: the compiler cannot tell the output from the inputs
   const float s0 = dXi * (TT(0, ip) - TT(0, c)) + dYi * (TT(1, jp) - TT(1, c)) + J1 * dXi * (TT(2, ip) - TT(2, c)) +
-         J2 * dYi * (TT(2, jp) - TT(2, c)) + J3 * dZi * (TT(2, kp) - TT(2, c));
+                   J2 * dYi * (TT(2, jp) - TT(2, c)) + J3 * dZi * (TT(2, kp) - TT(2, c));
   const float s1 = dXi * (TT(1, ip) - TT(1, c)) + dYi * (TT(4, jp) - TT(4, c)) + J1 * dXi * (TT(3, ip) - TT(3, c)) +
-             J2 * dYi * (TT(3, jp) - TT(3, c)) + J3 * dZi * (TT(3, kp) - TT(3, c));
+                   J2 * dYi * (TT(3, jp) - TT(3, c)) + J3 * dZi * (TT(3, kp) - TT(3, c));
   const float s2 = dXi * (TT(2, ip) - TT(2, c)) + dYi * (TT(3, jp) - TT(3, c)) + J1 * dXi * (TT(5, ip) - TT(5, c)) +
-                 J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c));
+                   J2 * dYi * (TT(5, jp) - TT(5, c)) + J3 * dZi * (TT(5, kp) - TT(5, c));
   const float s3 = dXi * (TT(6, ip) - TT(6, c)) + dYi * (TT(7, jp) - TT(7, c)) + J1 * dXi * (TT(8, ip) - TT(8, c)) +
-                 J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c));
+                   J2 * dYi * (TT(8, jp) - TT(8, c)) + J3 * dZi * (TT(8, kp) - TT(8, c));
   float sq[2] = {0.0f, 0.0f};
-  const int nq = (P.nmoist > 0 && P.moistSGS > 0) ? min(P.nmoist, 2) : 0;
-  if (nq > 0) {
 #pragma unroll
-    for (int m = 0; m < 2; m++) {
-      if (m >= nq) break;
-      const float* M = Q.mtau + 3 * m * n;
-      sq[m] = dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) + J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) +
-                           J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) + J3 * dZi * (M[2 * n + kp] - M[2 * n + c]);
-    }
+  for (int m = 0; m < NQ; m++) {
+    const float* M = Q.mtau + 3 * m * n;
+    sq[m] = dXi * (M[ip] - M[c]) + dYi * (M[n + jp] - M[n + c]) + J1 * dXi * (M[2 * n + ip] - M[2 * n + c]) +
+            J2 * dYi * (M[2 * n + jp] - M[2 * n + c]) + J3 * dZi * (M[2 * n + kp] - M[2 * n + c]);
   }
   float se = 0.0f;
-  if (P.tke) {
+  if (TKE) {
     const float r0 = st[c];
     const float ri = rinv(r0);
     const float delta = grid_scale(P, Q, c);
@@ -223,8 +221,9 @@ __global__ void __launch_bounds__(256) k_sgs_tend(Phys P, Ptrs Q, const float* _
   S[n] = s1;
   S[2 * n] = s2;
   S[3 * n] = s3;
-  if (P.tke) S[4 * n] = se;
-  for (int m = 0; m < nq; m++) S[(5 + m) * n] = sq[m];
+  if (TKE) S[4 * n] = se;
+#pragma unroll
+  for (int m = 0; m < NQ; m++) S[(5 + m) * n] = sq[m];
 }
 
 template <int STAGE, int MODE, int TJ, int FL>

@@ -153,7 +153,7 @@ struct GlobalPrims {
 // 5th/6th-order hybrid flux across the face between cells s0 (lower) and s1 (upper):
 // arguments are the stencil m2,m1,z0,p1,p2,p3 relative to the lower cell
 // (cuda_advectionDevice.cu:365-376): (37(p1+z0) - 8(p2+m1) + (p3+m2)
-//  - bfac sgn(vel) ((p3-m2) - 5(p2-m1) + 10(p1-z0))) / 60.
+//  - bfac sgn(vel) ((p3-m2) - 5(p2-m1) + 10(p1-z0))) / 60, bfac = 1 - b_hyb >= 0.
 __device__ __forceinline__ float hyb56_flux(float m2, float m1, float z0, float p1, float p2, float p3, float vel,
                                             float bfac) {
   const float sixtieth = 1.0f / 60.0f;
@@ -161,7 +161,7 @@ __device__ __forceinline__ float hyb56_flux(float m2, float m1, float z0, float 
   const float d = __fsub_rn(p3, m2), e = __fsub_rn(p2, m1), f = __fsub_rn(p1, z0);
   const float cen = __fadd_rn(__fmaf_rn(37.0f, a, __fmul_rn(-8.0f, b)), c);
   const float upw = __fmaf_rn(10.0f, f, __fmaf_rn(-5.0f, e, d));
-  const float sb = __fmul_rn(bfac, sgnf(vel));
+  const float sb = copysignf(bfac, vel);  // = bfac sgn(vel) exactly (bfac >= 0)
   return __fmul_rn(sixtieth, __fmaf_rn(-sb, upw, cen));
 }
 

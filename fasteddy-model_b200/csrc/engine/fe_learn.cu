@@ -97,10 +97,10 @@ cudaError_t fe_learn_enqueue_tau(const fe_mlp* m, const fe::Phys& P, const fe::P
   const long long cells = (long long)(P.Nx + 2) * (P.Ny + 2) * (P.Nz + 1);
   const long long tiles = (cells + fe::MLP_M - 1) / fe::MLP_M;
   if (Q.feat)
-    fe::k_mlp_infer<2><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
+    fe::k_mlp_infer<2><<<grid_for(m, tiles, 5), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
                                                                                       nullptr, 0, m->err);
   else
-    fe::k_mlp_infer<1><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
+    fe::k_mlp_infer<1><<<grid_for(m, tiles, 5), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
                                                                                       nullptr, 0, m->err);
   return cudaGetLastError();
 }
@@ -340,7 +340,7 @@ extern "C" int fe_mlp_predict(fe_mlp* m, const float* X, long long n, float* Y) 
     std::memset(&P, 0, sizeof(P));
     fe::Ptrs Q;
     std::memset(&Q, 0, sizeof(Q));
-    fe::k_mlp_infer<0><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, m->stream>>>(P, Q, nullptr, m->params, m->norm,
+    fe::k_mlp_infer<0><<<grid_for(m, tiles, 5), 128, fe::MlpInferSmem::BYTES, m->stream>>>(P, Q, nullptr, m->params, m->norm,
                                                                                             dX, dY, n, m->err);
     e = cudaGetLastError();
   }
@@ -375,7 +375,7 @@ extern "C" int fe_mlp_time(fe_mlp* m, int train, long long batch, int reps, floa
       fe::k_mlp_train<<<grid_for(m, tiles, 1), 128, fe::MlpTrainSmem::BYTES, m->stream>>>(
           m->params, m->norm, m->X, m->T, nullptr, m->n, 0, batch, m->grad, m->loss, m->err);
     else
-      fe::k_mlp_infer<0><<<grid_for(m, tiles, 4), 128, fe::MlpInferSmem::BYTES, m->stream>>>(P, Q, nullptr, m->params,
+      fe::k_mlp_infer<0><<<grid_for(m, tiles, 5), 128, fe::MlpInferSmem::BYTES, m->stream>>>(P, Q, nullptr, m->params,
                                                                                               m->norm, m->X, dY, batch, m->err);
   }
   cudaEventRecord(e1, m->stream);

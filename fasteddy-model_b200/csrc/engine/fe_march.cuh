@@ -24,8 +24,6 @@
 // of the new state -- is the cell kernel's arithmetic (fe_kernels.cuh), term by term and in the
 // same order, evaluated on the register/shared copies.
 #pragma once
-#include <type_traits>
-
 #include "fe_kernels.cuh"
 
 namespace fe {
@@ -689,26 +687,51 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
           pn = powf(rtm * P.c1, P.cp_cv) - pbs;
         }
         const float p0 = atBot ? level0_pressure(P, l0, nmoist, nq0) : 0.0f;
-        // The stores, once with the periodic images of cells within 3 of an x or y edge and once
-        // without (every other column: one store per field plus the bottom/top halo copies).
-        auto stores = [&](auto edge) {
-          auto put = [&](float* Fd, float v, int nbot, bool top) {
-            if constexpr (decltype(edge)::value) store_images(P, Fd, i, j, k, v, nbot, top);
-            else store_column(Fd, c, v, nbot, top);
-          };
-          put(nxt, n0, 0, false);
-          put(nxt + n, n1, atBot ? 3 : 0, false);
-          put(nxt + 2 * n, n2, atBot ? 3 : 0, false);
-          put(nxt + 3 * n, n3, atBot ? 3 : 0, false);
-          put(nxt + 4 * n, n4, 0, false);
-          if (ntke) put(nxt + 5 * n, ne, atBot ? 3 : 0, false);
-          if (nmoist > 0) put(nxt + oq, nq0, atBot ? 3 : 0, atTop);
-          if (nmoist > 1) put(nxt + oq + n, nq1, atBot ? 3 : 0, atTop);
-          put(pnxt, pn, atBot ? 2 : 0, atTop);
-        };
+        // The stores: cells within 3 of an x or y edge also write their periodic images (and,
+        // at the first and last level, the images' halo copies); every other cell writes one
+        // value per field and, at the first and last level, the halo copies below and above.
         const bool xyEdge = (i < P.iMin + 3) || (i >= P.iMax - 3) || (j < P.jMin + 3) || (j >= P.jMax - 3);
-        if (xyEdge) stores(std::true_type{});
-        else stores(std::false_type{});
+        if (xyEdge) {
+          store_images(P, nxt, i, j, k, n0, 0, false);
+          store_images(P, nxt + n, i, j, k, n1, atBot ? 3 : 0, false);
+          store_images(P, nxt + 2 * n, i, j, k, n2, atBot ? 3 : 0, false);
+          store_images(P, nxt + 3 * n, i, j, k, n3, atBot ? 3 : 0, false);
+          store_images(P, nxt + 4 * n, i, j, k, n4, 0, false);
+          if (ntke) store_images(P, nxt + 5 * n, i, j, k, ne, atBot ? 3 : 0, false);
+          if (nmoist > 0) store_images(P, nxt + oq, i, j, k, nq0, atBot ? 3 : 0, atTop);
+          if (nmoist > 1) store_images(P, nxt + oq + n, i, j, k, nq1, atBot ? 3 : 0, atTop);
+          store_images(P, pnxt, i, j, k, pn, atBot ? 2 : 0, atTop);
+        } else {
+          nxt[c] = n0;
+          nxt[n + c] = n1;
+          nxt[2 * n + c] = n2;
+          nxt[3 * n + c] = n3;
+          nxt[4 * n + c] = n4;
+          if (ntke) nxt[5 * n + c] = ne;
+          if (nmoist > 0) nxt[oq + c] = nq0;
+          if (nmoist > 1) nxt[oq + n + c] = nq1;
+          pnxt[c] = pn;
+          if (atBot) {
+#pragma unroll
+            for (int h = 1; h <= 3; h++) {
+              nxt[n + c - h] = n1;
+              nxt[2 * n + c - h] = n2;
+              nxt[3 * n + c - h] = n3;
+              if (ntke) nxt[5 * n + c - h] = ne;
+              if (nmoist > 0) nxt[oq + c - h] = nq0;
+              if (nmoist > 1) nxt[oq + n + c - h] = nq1;
+              if (h <= 2) pnxt[c - h] = pn;
+            }
+          }
+          if (atTop) {
+#pragma unroll
+            for (int h = 1; h <= 3; h++) {
+              if (nmoist > 0) nxt[oq + c + h] = nq0;
+              if (nmoist > 1) nxt[oq + n + c + h] = nq1;
+              pnxt[c + h] = pn;
+            }
+          }
+        }
         if (atBot) store_images(P, pnxt, i, j, 0, p0, 0, false);
       }
     }

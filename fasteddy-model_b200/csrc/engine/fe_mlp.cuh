@@ -1,8 +1,8 @@
 // fe_mlp.cuh -- the learned SGS closure on the 5th-generation tensor cores (sm_100a).
 //
-// Network: 11 -> 64 -> 64 -> 64 -> 9, tanh on the hidden layers (hardware tanh.approx, see
-// tanh_hw); inputs standardised,
-// outputs tau/rho = out_mu + out_sig * y. Every layer is one 128-row tile of tcgen05.mma
+// Network: 11 -> 64 -> 64 -> 64 -> 9, tanh on the hidden layers (hardware tanh.approx: bf16x2 on
+// the BF16-rounded pre-activations for inference, f32 for training; see epi_tanh); inputs standardised ((x - mu) times the
+// FP32 reciprocal of sig), outputs tau/rho = out_mu + out_sig * y. Every layer is one 128-row tile of tcgen05.mma
 // (kind::f16, BF16 A and B operands from shared memory, FP32 accumulators in tensor memory),
 // issued by one thread; the epilogue (tcgen05.ld, bias, tanh, BF16 pack) runs on all 128
 // threads, one tile row (one cell) per thread. Operand tiles use the canonical K-major,
@@ -119,6 +119,9 @@ __device__ __forceinline__ void st_chunk(char* base, int r, int q, int K, const 
   u.w = *reinterpret_cast<uint32_t*>(&p3);
   *reinterpret_cast<uint4*>(base + (r >> 3) * (K >> 3) * 128 + q * 128 + (r & 7) * 16) = u;
 }
+__device__ __forceinline__ void st_chunk_u(char* base, int r, int q, int K, uint4 u) {
+  *reinterpret_cast<uint4*>(base + (r >> 3) * (K >> 3) * 128 + q * 128 + (r & 7) * 16) = u;
+}
 __device__ __forceinline__ void ld_chunk(const char* base, int r, int q, int K, float* v) {
   const uint4 u = *reinterpret_cast<const uint4*>(base + (r >> 3) * (K >> 3) * 128 + q * 128 + (r & 7) * 16);
   const uint32_t w[4] = {u.x, u.y, u.z, u.w};
@@ -150,7 +153,8 @@ __device__ __forceinline__ void stage_weight(const float* __restrict__ W, int N,
 struct MlpInferSmem {
   static constexpr int W1 = 0, W2 = W1 + 64 * 16 * 2, W3 = W2 + 64 * 64 * 2, W4 = W3 + 64 * 64 * 2;
   static constexpr int X0 = W4 + 16 * 64 * 2, H = X0 + 128 * 16 * 2, BIAS = H + 128 * 64 * 2;
-  static constexpr int NORM = BIAS + (64 * 3 + 16) * 4, BAR = NORM + 64 * 4, TADDR = BAR + 8, FLAG = TADDR + 4;
+  static constexpr int NORM = BIAS + (64 * 3 + 16) * 4, ISIG = NORM + 64 * 4, BAR = ISIG + 16 * 4, TADDR = BAR + 8;
+  static constexpr int FLAG = TADDR + 4;
   static constexpr int BYTES = FLAG + 4;
 };
 // training: also the transposed weights, all forward activations and the backward tiles
@@ -159,7 +163,8 @@ struct MlpTrainSmem {
   static constexpr int W4T = W4 + 16 * 64 * 2, W3T = W4T + 64 * 16 * 2, W2T = W3T + 64 * 64 * 2;
   static constexpr int X0 = W2T + 64 * 64 * 2, H1 = X0 + 128 * 16 * 2, H2 = H1 + 128 * 64 * 2, H3 = H2 + 128 * 64 * 2;
   static constexpr int DZK = H3 + 128 * 64 * 2, DZT = DZK + 128 * 64 * 2, ATH = DZT + 64 * 128 * 2;
-  static constexpr int BIAS = ATH + 128 * 128 * 2, NORM = BIAS + (64 * 3 + 16) * 4, RED = NORM + 64 * 4;
+  static constexpr int BIAS = ATH + 128 * 128 * 2, NORM = BIAS + (64 * 3 + 16) * 4, ISIG = NORM + 64 * 4;
+  static constexpr int RED = ISIG + 16 * 4;
   static constexpr int BAR = RED + 4 * 8, TADDR = BAR + 8, FLAG = TADDR + 4;
   static constexpr int BYTES = FLAG + 4;
 };
@@ -177,35 +182,65 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
 }
 
+__device__ __forceinline__ void stage_isig(const MlpNorm* nmp, float* isig, int tid) {
+  if (tid < 16) isig[tid] = 1.0f / nmp->in_sig[tid];
+}
 // standardised input row -> 2 BF16 chunks of the X0 tile
-__device__ __forceinline__ void put_inputs(char* x0, int r, const float* x, const MlpNorm& nm, bool valid) {
+// (isig: the FP32 reciprocals of in_sig, formed once per CTA by stage_isig)
+__device__ __forceinline__ void put_inputs(char* x0, int r, const float* x, const MlpNorm& nm, const float* isig,
+                                           bool valid) {
   float v[16];
 #pragma unroll
-  for (int q = 0; q < 16; q++) v[q] = (valid && q < SGS_NIN) ? (x[q] - nm.in_mu[q]) / nm.in_sig[q] : 0.0f;
+  for (int q = 0; q < 16; q++) v[q] = (valid && q < SGS_NIN) ? (x[q] - nm.in_mu[q]) * isig[q] : 0.0f;
   st_chunk(x0, r, 0, 16, v);
   st_chunk(x0, r, 1, 16, v + 8);
 }
 
-// tanh of the hidden layers: the hardware approximation (tanh.approx.f32, relative error
-// about 2^-11), below the resolution of the BF16 activations it feeds (2^-9), at one
-// instruction instead of a library tanh
+// tanh of a hidden unit for training: the hardware tanh.approx.f32 (relative error about
+// 2^-11, below the BF16 resolution of the activation tile it feeds)
 __device__ __forceinline__ float tanh_hw(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+// tanh of two hidden units for inference: the pre-activations rounded to BF16 (the precision of
+// the activation tile they end up in) and the hardware tanh.approx.bf16x2, two values per
+// special-function instruction; the result is the packed BF16 pair of the tile
+__device__ __forceinline__ uint32_t tanh2_bf16(float a, float b) {
+  const __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+  uint32_t r;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(r) : "r"(*reinterpret_cast<const uint32_t*>(&p)));
+  return r;
+}
 
-// hidden-layer epilogue: accumulator row + bias -> tanh -> BF16 tile row
+// hidden-layer epilogue: accumulator row + bias -> tanh -> BF16 tile row. PAIRED (inference):
+// tanh2_bf16; otherwise (training, whose gradients are checked tightly) tanh_hw per unit.
+template <bool PAIRED>
 __device__ __forceinline__ void epi_tanh(uint32_t tacc, const float* bias, char* out, int r) {
 #pragma unroll
   for (int g = 0; g < 4; g++) {
     float v[16];
     tmem_ld16(tacc + g * 16, v);
     tmem_wait_ld();
+    const float* b = bias + g * 16;
+    if (PAIRED) {
+      uint4 lo, hi;
+      lo.x = tanh2_bf16(v[0] + b[0], v[1] + b[1]);
+      lo.y = tanh2_bf16(v[2] + b[2], v[3] + b[3]);
+      lo.z = tanh2_bf16(v[4] + b[4], v[5] + b[5]);
+      lo.w = tanh2_bf16(v[6] + b[6], v[7] + b[7]);
+      hi.x = tanh2_bf16(v[8] + b[8], v[9] + b[9]);
+      hi.y = tanh2_bf16(v[10] + b[10], v[11] + b[11]);
+      hi.z = tanh2_bf16(v[12] + b[12], v[13] + b[13]);
+      hi.w = tanh2_bf16(v[14] + b[14], v[15] + b[15]);
+      st_chunk_u(out, r, 2 * g, 64, lo);
+      st_chunk_u(out, r, 2 * g + 1, 64, hi);
+    } else {
 #pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = tanh_hw(v[q] + bias[g * 16 + q]);
-    st_chunk(out, r, 2 * g, 64, v);
-    st_chunk(out, r, 2 * g + 1, 64, v + 8);
+      for (int q = 0; q < 16; q++) v[q] = tanh_hw(v[q] + b[q]);
+      st_chunk(out, r, 2 * g, 64, v);
+      st_chunk(out, r, 2 * g + 1, 64, v + 8);
+    }
   }
 }
 
@@ -237,6 +272,8 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* 
   int* flag = reinterpret_cast<int*>(sm + S::FLAG);
   MlpNorm& nm = *reinterpret_cast<MlpNorm*>(sm + S::NORM);
   if (tid < 64) reinterpret_cast<float*>(&nm)[tid] = reinterpret_cast<const float*>(nmp)[tid];
+  float* isig = reinterpret_cast<float*>(sm + S::ISIG);
+  stage_isig(nmp, isig, tid);
   stage_weight(params + MP_W1, 64, 16, sm + S::W1, nullptr, tid, 128);
   stage_weight(params + MP_W2, 64, 64, sm + S::W2, nullptr, tid, 128);
   stage_weight(params + MP_W3, 64, 64, sm + S::W3, nullptr, tid, 128);
@@ -263,33 +300,52 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* 
   const long long ntiles = (ntot + MLP_M - 1) / MLP_M;
   const uint32_t id64 = umma_idesc(128, 64), id16 = umma_idesc(128, 16);
 
+  // inputs of one row of a tile (a thread's cell), loaded one tile ahead of its MMA chain
+  struct Row {
+    float x[SGS_NIN];
+    long long c;
+    float rho;
+    int i, j, k;
+    bool valid;
+  };
+  auto fetch = [&](long long tile, Row& r) {
+    const long long row = tile * MLP_M + tid;
+    r.valid = tile < ntiles && row < ntot;
+    r.c = 0;
+    r.rho = 0.0f;
+    r.i = r.j = r.k = 0;
+#pragma unroll
+    for (int q = 0; q < SGS_NIN; q++) r.x[q] = 0.0f;
+    if (!r.valid) return;
+    if (SRC == 0) {
+#pragma unroll
+      for (int q = 0; q < SGS_NIN; q++) r.x[q] = X[row * SGS_NIN + q];
+    } else {
+      r.k = P.kMin + (int)(row % rk);
+      r.j = P.jMin - 1 + (int)((row / rk) % rj);
+      r.i = P.iMin - 1 + (int)(row / ((long long)rk * rj));
+      r.c = (long long)r.i * P.si + (long long)r.j * P.sj + r.k;
+      if (SRC == 2) {
+#pragma unroll
+        for (int q = 0; q < SGS_NIN; q++) r.x[q] = Q.feat[q * P.n + r.c];
+      } else {
+        sgs_inputs(P, Q, st, r.c, r.x);
+      }
+      r.rho = st[r.c];
+    }
+  };
+  Row nxt;
+  fetch(blockIdx.x, nxt);
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long row = tile * MLP_M + tid;
-    const bool valid = row < ntot;
-    float x[SGS_NIN];
-    long long c = 0;
-    float rho = 0.0f;
-    int i = 0, j = 0, k = 0;
-    if (valid) {
-      if (SRC == 0) {
-#pragma unroll
-        for (int q = 0; q < SGS_NIN; q++) x[q] = X[row * SGS_NIN + q];
-      } else {
-        k = P.kMin + (int)(row % rk);
-        j = P.jMin - 1 + (int)((row / rk) % rj);
-        i = P.iMin - 1 + (int)(row / ((long long)rk * rj));
-        c = (long long)i * P.si + (long long)j * P.sj + k;
-        if (SRC == 2) {
-#pragma unroll
-          for (int q = 0; q < SGS_NIN; q++) x[q] = Q.feat[q * P.n + c];
-        } else {
-          sgs_inputs(P, Q, st, c, x);
-        }
-        rho = st[c];
-      }
-    }
-    put_inputs(sm + S::X0, tid, x, nm, valid);
+    const Row cur = nxt;
+    const bool valid = cur.valid;
+    const long long c = cur.c;
+    const float rho = cur.rho;
+    const int i = cur.i, j = cur.j, k = cur.k;
+    put_inputs(sm + S::X0, tid, cur.x, nm, isig, valid);
     sync_for_mma();
+    fetch(tile + gridDim.x, nxt);  // in flight while this tile's layers run
     bool ok = true;
     // layer 1
     if (tid == 0) {
@@ -300,7 +356,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* 
     ok = ok && mbar_wait(bar, phase);
     phase ^= 1;
     tc_fence_after();
-    epi_tanh(tlane + TC_DF, bias, sm + S::H, tid);
+    epi_tanh<true>(tlane + TC_DF, bias, sm + S::H, tid);
     sync_for_mma();
     // layers 2 and 3 (the MMA has finished reading H before the epilogue overwrites it)
 #pragma unroll 1
@@ -317,7 +373,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* 
       ok = ok && mbar_wait(bar, phase);
       phase ^= 1;
       tc_fence_after();
-      epi_tanh(tlane + TC_DF, bias + 64 * (l + 1), sm + S::H, tid);
+      epi_tanh<true>(tlane + TC_DF, bias + 64 * (l + 1), sm + S::H, tid);
       sync_for_mma();
     }
     // layer 4
@@ -381,6 +437,8 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
   int* flag = reinterpret_cast<int*>(sm + S::FLAG);
   MlpNorm& nm = *reinterpret_cast<MlpNorm*>(sm + S::NORM);
   if (tid < 64) reinterpret_cast<float*>(&nm)[tid] = reinterpret_cast<const float*>(nmp)[tid];
+  float* isig = reinterpret_cast<float*>(sm + S::ISIG);
+  stage_isig(nmp, isig, tid);
   stage_weight(params + MP_W1, 64, 16, sm + S::W1, nullptr, tid, 128);
   stage_weight(params + MP_W2, 64, 64, sm + S::W2, sm + S::W2T, tid, 128);
   stage_weight(params + MP_W3, 64, 64, sm + S::W3, sm + S::W3T, tid, 128);
@@ -430,7 +488,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
     float x[SGS_NIN];
 #pragma unroll
     for (int q = 0; q < SGS_NIN; q++) x[q] = valid ? X[row * SGS_NIN + q] : 0.0f;
-    put_inputs(sm + S::X0, tid, x, nm, valid);
+    put_inputs(sm + S::X0, tid, x, nm, isig, valid);
     sync_for_mma();
     // ---- forward
     if (tid == 0) {
@@ -439,7 +497,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
       umma_commit(bar);
     }
     mma_wait();
-    epi_tanh(tlane + TC_DF, bias, sm + S::H1, tid);
+    epi_tanh<false>(tlane + TC_DF, bias, sm + S::H1, tid);
     sync_for_mma();
 #pragma unroll 1
     for (int l = 0; l < 2; l++) {
@@ -453,7 +511,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(const float* __restrict__ 
         umma_commit(bar);
       }
       mma_wait();
-      epi_tanh(tlane + TC_DF, bias + 64 * (l + 1), sm + (l == 0 ? S::H2 : S::H3), tid);
+      epi_tanh<false>(tlane + TC_DF, bias + 64 * (l + 1), sm + (l == 0 ? S::H2 : S::H3), tid);
       sync_for_mma();
     }
     if (tid == 0) {

@@ -12,7 +12,8 @@ Two modes:
   exact=True   FP64 throughout (pinned against central finite differences in the tests);
   exact=False  FP64 arithmetic, but every tensor-core operand rounded to BF16 (round to
                nearest even) exactly where the device rounds it: the standardised inputs, the
-               weights, the hidden activations and the backward signals dZ. This is the
+               weights, the hidden activations (for predictions also the pre-activations,
+               the argument of the inference kernel's BF16 tanh), and the backward signals dZ. This is the
                reference the device gradients and predictions are checked against.
 """
 from __future__ import annotations
@@ -49,28 +50,34 @@ def unpack(p: np.ndarray) -> dict:
 
 
 def standardise(X: np.ndarray, norm: dict) -> np.ndarray:
-    """(x - mu)/sig in float32 as the device computes it, padded to 16 columns."""
+    """(x - mu) * (1/sig) in float32 as the device computes it (the reciprocal rounded to
+    float32 once), padded to 16 columns."""
     X = np.asarray(X, np.float32)
-    z = (X - np.asarray(norm["in_mu"], np.float32)) / np.asarray(norm["in_sig"], np.float32)
+    isig = (np.float32(1.0) / np.asarray(norm["in_sig"], np.float32)).astype(np.float32)
+    z = (X - np.asarray(norm["in_mu"], np.float32)) * isig
     out = np.zeros((X.shape[0], K0), np.float64)
     out[:, :NIN] = z.astype(np.float64)
     return out
 
 
-def forward(p: np.ndarray, X: np.ndarray, norm: dict, exact: bool = False) -> dict:
+def forward(p: np.ndarray, X: np.ndarray, norm: dict, exact: bool = False, inference: bool = False) -> dict:
+    """Forward pass. In bf16 mode the hidden activations are rounded to BF16; the inference
+    kernel also rounds the pre-activation (the argument of its BF16 tanh), the training kernel
+    does not (FP32 tanh)."""
     w = unpack(p)
     r = (lambda a: a) if exact else bf16
+    ra = r if inference else (lambda a: a)
     x0 = r(standardise(X, norm))
-    h1 = r(np.tanh(x0 @ r(w["W1"]).T + w["b1"]))
-    h2 = r(np.tanh(h1 @ r(w["W2"]).T + w["b2"]))
-    h3 = r(np.tanh(h2 @ r(w["W3"]).T + w["b3"]))
+    h1 = r(np.tanh(ra(x0 @ r(w["W1"]).T + w["b1"])))
+    h2 = r(np.tanh(ra(h1 @ r(w["W2"]).T + w["b2"])))
+    h3 = r(np.tanh(ra(h2 @ r(w["W3"]).T + w["b3"])))
     y = h3 @ r(w["W4"]).T + w["b4"]
     return {"x0": x0, "h1": h1, "h2": h2, "h3": h3, "y": y[:, :NOUT]}
 
 
 def predict(p: np.ndarray, X: np.ndarray, norm: dict, exact: bool = False) -> np.ndarray:
     """Outputs tau/rho (samples x 9)."""
-    y = forward(p, X, norm, exact)["y"]
+    y = forward(p, X, norm, exact, inference=True)["y"]
     return np.asarray(norm["out_mu"], np.float64) + np.asarray(norm["out_sig"], np.float64) * y
 
 

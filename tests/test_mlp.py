@@ -3,10 +3,11 @@ rounding, the tensor-core forward/backward kernels against the oracle, training,
 hook, and what the trained network gains over the TKE closure on coarse-grained data.
 
 Tolerances. The oracle (bf16 mode) rounds to BF16 where the kernels do, so the remaining
-differences are FP32 accumulation order and the kernels' hardware tanh (tanh.approx.f32,
-relative error about 2^-11) against numpy's tanh, which can move a BF16 activation by one unit
-(2^-8 relative) here and there: predictions are checked at relative L2 1e-2, gradients per
-parameter block at 2e-2 and the loss at 1e-3.
+differences are FP32 accumulation order and the kernels' hardware tanh (inference:
+tanh.approx.bf16x2 on the BF16 pre-activation; training: tanh.approx.f32, relative error about
+2^-11) against numpy's tanh, which can move a BF16 activation by one unit (2^-8 relative) here
+and there: predictions are checked at relative L2 1e-2, gradients per parameter block at 2e-2
+and the loss at 1e-3.
 """
 from __future__ import annotations
 

@@ -54,5 +54,6 @@ def test_single_process_defaults():
     import bench
 
     assert bench.max_over_ranks(3.5) == 3.5
-    assert bench.bytes_per_cell_stage(8, True) == 120
-    assert bench.bytes_per_cell_stage(6, False) == 72
+    # 3 N_p state fields + p' in and out + 8 grid/base-state fields, 4 bytes each
+    assert bench.bytes_per_cell_stage(8) == 136
+    assert bench.bytes_per_cell_stage(6) == 112

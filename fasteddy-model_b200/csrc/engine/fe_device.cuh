@@ -171,6 +171,9 @@ __device__ __forceinline__ float hyb56_flux(float m2, float m1, float z0, float 
 // are formed with one division: multiplying through by (q1 q2 q3)^2 gives w_k ~ g_k (q_i q_j)^2
 // (i, j != k). With q >= tol = 1e-6 the products stay normal, and they stay finite while the
 // smoothness indicators are below 1e9 (jumps of the advected field below ~3e4 across a cell).
+// FAST: the normalisation by the weight sum uses the fast division (__fdividef, 2 ulp; the sum
+// lies in [1e-25, 2e36], well inside its range) instead of the IEEE one.
+template <bool FAST = false>
 __device__ __forceinline__ float weno5_face(float a, float b, float c, float d, float e) {
   const float g1 = 1.0f / 10.0f, g2 = 3.0f / 5.0f, g3 = 3.0f / 10.0f, tol = 1e-6f;
   const float k13 = 1.0f / 3.0f, k76 = 7.0f / 6.0f, k116 = 11.0f / 6.0f, k16 = 1.0f / 6.0f, k56 = 5.0f / 6.0f;
@@ -190,15 +193,17 @@ __device__ __forceinline__ float weno5_face(float a, float b, float c, float d, 
   const float u2 = __fmul_rn(g2, __fmul_rn(a2, a2));
   const float u3 = __fmul_rn(g3, __fmul_rn(a3, a3));
   const float num = __fmaf_rn(u3, f3, __fmaf_rn(u2, f2, __fmul_rn(u1, f1)));
-  return __fdiv_rn(num, __fadd_rn(__fadd_rn(u1, u2), u3));
+  const float den = __fadd_rn(__fadd_rn(u1, u2), u3);
+  return FAST ? __fdividef(num, den) : __fdiv_rn(num, den);
 }
 
 // The reference blends both one-sided values with weights 0.5(1 +- sign(u)), which are
 // exactly 1 and 0; only the upwind value is evaluated here (same result). The upwind stencil
 // is selected value by value, so lanes of one warp with opposite velocities do not diverge.
+template <bool FAST = false>
 __device__ __forceinline__ float weno5_flux(float m2, float m1, float z0, float p1, float p2, float p3, float vel) {
   const bool up = sgnf(vel) > 0.0f;
-  return weno5_face(up ? m2 : p3, up ? m1 : p2, up ? z0 : p1, up ? p1 : z0, up ? p2 : m1);
+  return weno5_face<FAST>(up ? m2 : p3, up ? m1 : p2, up ? z0 : p1, up ? p1 : z0, up ? p2 : m1);
 }
 
 // Face velocities of a cell: lower/upper faces in x, y, z (cuda_advectionDevice.cu:54-121).

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float m2 = B1[s * PLANE + own], m1 = B2[s * PLANE + own];
       const float f = f_sel<FL>(P, s) == 3
                           ? hyb56_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev, 1.0f - slot_b(P, s))
-                          : weno5_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev);
+                          : weno5_flux<true>(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev);
       xcs[s * T::NT + tid] = __fmul_rn(upPrev, f);
     }
   }
@@ -494,6 +494,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     const float J1 = J1c, J2 = J2c, J3 = J3c;
     const float invD = ax[13 * T::NT];
     const float r0 = w[0][0];
+    // The moist PGF, Coriolis and Rayleigh terms divide by rho and rho_BS through one correctly
+    // rounded reciprocal per block (phi * (1/rho) instead of phi / rho: within an ulp).
     float F[8];
 #pragma unroll
     for (int s = 0; s < 8; s++) F[s] = 0.0f;
@@ -505,9 +507,10 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float dpy = pp[PK] - pp[-PK];
       const float dpz = pp[1] - pp[-1];
       if (nmoist > 0) {
+        const float rr0 = 1.0f / r0;
         float rmd = 1.0f;
-        rmd = (float)((double)rmd + (double)(w[SL_QV][0] / r0) * 1e-3);
-        if (nmoist > 1) rmd = (float)((double)rmd + (double)(w[SL_QL][0] / r0) * 1e-3);
+        rmd = (float)((double)rmd + (double)(w[SL_QV][0] * rr0) * 1e-3);
+        if (nmoist > 1) rmd = (float)((double)rmd + (double)(w[SL_QL][0] * rr0) * 1e-3);
         const float rdm = 1.0f / rmd;
         F[1] = (float)((double)F[1] - (double)rdm * 0.5 * (double)dXi * (double)dpx);
         F[2] = (float)((double)F[2] - (double)rdm * 0.5 * (double)dYi * (double)dpy);
@@ -543,20 +546,20 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         }
         F[s] = F[s] - invD * (Dx + Dy + Dz);
       } else {
-        const float fxp = weno5_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up);
+        const float fxp = weno5_flux<true>(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up);
         const float pxp = __fmul_rn(up, fxp);
         F[s] = F[s] - invD * __fsub_rn(pxp, xcs[s * T::NT + tid]);
         xcs[s * T::NT + tid] = pxp;
         {
           const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
-          const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, vp);
-          const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, vm);
+          const float fp = weno5_flux<true>(m2, m1, z0, p1, p2, p3, vp);
+          const float fm = weno5_flux<true>(m3, m2, m1, z0, p1, p2, vm);
           F[s] = F[s] - invD * (vp * fp - vm * fm);
         }
         {
           const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
-          const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, wp);
-          const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, wm);
+          const float fp = weno5_flux<true>(m2, m1, z0, p1, p2, p3, wp);
+          const float fm = weno5_flux<true>(m3, m2, m1, z0, p1, p2, wm);
           F[s] = F[s] - invD * (wp * fp - wm * fm);
         }
       }
@@ -565,11 +568,11 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         if (P.damp && inArr) {
           const float z = zc, zt = ztop;
           if (z >= (zt - P.dampDepth)) {
-            const float rbs = rbsc;
+            const float rbs = rbsc, rr0 = 1.0f / r0, rrb = 1.0f / rbs;
             const float wbs = momentum_bs(P, 3, z, rbs);
             const float pio2 = 1.5707963267948966f;
             const double sn = (double)sinf((float)((double)pio2 * (1.0 - (double)((zt - z) / P.dampDepth))));
-            F[3] = (float)((double)F[3] - 0.2 * (double)r0 * (sn * sn) * (double)(w[3][0] / r0 - wbs / rbs));
+            F[3] = (float)((double)F[3] - 0.2 * (double)r0 * (sn * sn) * (double)(w[3][0] * rr0 - wbs * rrb));
           }
         }
         if (P.buoy) {
@@ -590,9 +593,12 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     if (P.cor && inArr) {
       const float z = zc, rbs = rbsc;
       const float ubs = momentum_bs(P, 1, z, rbs), vbs = momentum_bs(P, 2, z, rbs), wbs = momentum_bs(P, 3, z, rbs);
-      F[1] = F[1] + (P.fHorz * (w[2][0] / r0 - P.fLS * vbs / rbs) - P.fVert * (w[3][0] / r0 - P.fLS * wbs / rbs));
-      F[2] = F[2] - (P.fHorz * (w[1][0] / r0 - P.fLS * ubs / rbs));
-      F[3] = F[3] + (P.fVert * (w[1][0] / r0 - P.fLS * ubs / rbs));
+      const float rr0 = 1.0f / r0, rrb = 1.0f / rbs;
+      const float u0 = w[1][0] * rr0, v0 = w[2][0] * rr0, w0 = w[3][0] * rr0;
+      const float ug = P.fLS * ubs * rrb, vg = P.fLS * vbs * rrb, wg = P.fLS * wbs * rrb;
+      F[1] = F[1] + (P.fHorz * (v0 - vg) - P.fVert * (w0 - wg));
+      F[2] = F[2] - (P.fHorz * (u0 - ug));
+      F[3] = F[3] + (P.fVert * (u0 - ug));
     }
 
     if (phys && P.turb && active) {

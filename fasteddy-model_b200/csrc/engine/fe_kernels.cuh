@@ -91,9 +91,9 @@ __device__ __forceinline__ float length_scale_a(const Phys& P, const Ptrs& Q, co
   const float N2 = (P.g / pr.th(0, 0, dk)) * dthdz;
   const float len2 = grid_scale(P, Q, c);
   if (N2 > 0.0f) {
-    const float tb = powf(N2, -0.5f);
+    const float tb = 1.0f / sqrtf(N2);  // N2^(-1/2): two correctly rounded operations
     const float ec = pr.ev(0, 0, dk);
-    const float len1 = (float)(0.76 * (double)powf(ec, 0.5f) * (double)tb);
+    const float len1 = (float)(0.76 * (double)sqrtf(ec) * (double)tb);
     return fmaxf(fminf(len1, len2), 1e-2f);
   }
   return len2;
@@ -284,7 +284,7 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
       const float r = pr.r(0, 0, 0);
       if (P.tke) {
         const float e0 = pr.ev(0, 0, 0);
-        const float se0 = sec >= 0.0f ? sec : powf(e0, 0.5f);  // sqrt(e/rho) of this cell (given by the tiled form)
+        const float se0 = sec >= 0.0f ? sec : sqrtf(e0);  // sqrt(e/rho) of this cell (given by the tiled form)
         Km = (float)((double)P.c_k * 0.5 * (double)(lsc * se0 + lsm * sem));
         const float invPr = 1.0f + 2.0f * lsc / delta;
         const float dev = (float)((2.0 / 3.0) * (double)r *
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
     lsc = length_scale(P, Q, rho, mth, e, c);
     if (k >= P.kMin) {
       lsm = length_scale(P, Q, rho, mth, e, c - 1);
-      sem = powf(e[c - 1] * rinv(rho[c - 1]), 0.5f);
+      sem = sqrtf(e[c - 1] * rinv(rho[c - 1]));
     }
   }
   turb_cell(P, Q, st, i, j, k, lsc, lsm, sem, stage);
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __r
         const long long c = (long long)i * P.si + (long long)j * P.sj + k;
         const TilePrims pr{tile, (li + 1) * (TP_J * TP_K) + (lj + 1) * TP_K + (lk + 1)};
         ls = length_scale_a(P, Q, pr, c, 0);
-        se = powf(pr.ev(0, 0, 0), 0.5f);
+        se = sqrtf(pr.ev(0, 0, 0));
       }
       lsT[li][lj][lk] = ls;
       seT[li][lj][lk] = se;
@@ -702,7 +702,7 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
       Fe = Fe + P.g / (mth[c] * ri) * TT(8, c);
       const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
       const float ec = me[c] * ri;
-      Fe = Fe + (-ce * me[c] * powf(ec, 0.5f) / lsc);
+      Fe = Fe + (-ce * me[c] * sqrtf(ec) / lsc);
       const long long im = c - si, jm = c - sj, km = c - 1;
 #define G_(q, x) (q[x] * rinv(rho[x]))
       const float dux = 0.5f * (dXi * (G_(mu, ip) - G_(mu, im)));

@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float
     float Se = P.g / (st[4 * n + c] * ri) * TT(8, c);
     const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
     const float ec = mec * ri;
-    Se = Se + (-ce * mec * powf(ec, 0.5f) / lsc);
+    Se = Se + (-ce * mec * sqrtf(ec) / lsc);
     // (rho phi)/rho of field f at the neighbour c + o
     auto G = [&](int f, long long o) -> float { return st[f * n + c + o] * rinv(st[c + o]); };
     const float ux = G(1, si) - G(1, -si), uy = G(1, sj) - G(1, -sj), uz = G(1, 1) - G(1, -1);

@@ -54,6 +54,8 @@ struct fe_domain {
   Ptrs Q;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;                         // second branch of a step (ring-level SGS kernel)
+  cudaEvent_t fork = nullptr, join = nullptr;          // ordering between stream and side
   float* st[3] = {nullptr, nullptr, nullptr};
   float* pr[3] = {nullptr, nullptr, nullptr};
   float* grid = nullptr;
@@ -256,6 +258,9 @@ static void free_domain(fe_domain* d) {
   cudaFree(d->feat);
   cudaFree(d->clock);
   cudaFree(d->counter);
+  if (d->fork) cudaEventDestroy(d->fork);
+  if (d->join) cudaEventDestroy(d->join);
+  if (d->side) cudaStreamDestroy(d->side);
   if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
 }
@@ -274,10 +279,13 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   d->cfg = *cfg;
   d->device = device;
   make_phys(d);
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->join, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
-    delete d;
-    return set_err(FE_ERR_CUDA, "cannot create a stream on the device");
+    free_domain(d);
+    return set_err(FE_ERR_CUDA, "cannot create streams and events on the device");
   }
   const Phys& P = d->P;
   const size_t n = (size_t)P.n, n2 = (size_t)P.n2;
@@ -552,15 +560,23 @@ static dim3 stage_grid(const fe_domain* d) {
   return dim3((P.Nz + d->tk - 1) / d->tk, (P.Ny + d->tj - 1) / d->tj, (P.Nx + d->ti - 1) / d->ti);
 }
 // Last-stage SGS physics on the +1 ring (k_turb_t: shared-memory tiles of primitives).
-// The last-stage SGS physics of the +1 ring (tiled kernel) and then the surface layer of its
-// columns; returns the number of kernels launched.
+// The last-stage SGS physics of the +1 ring (tiled kernel for the interior levels, ring-level
+// kernel for the level above) and then the surface layer of its columns; returns the number of
+// kernels launched.
 static int launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
   const Phys& P = d->P;
-  const dim3 g((P.Nz + 2 + fe::TT_K - 1) / fe::TT_K, (P.Ny + 2 + fe::TT_J - 1) / fe::TT_J, (P.Nx + 2 + fe::TT_I - 1) / fe::TT_I);
+  const dim3 g((P.Nz + fe::TT_K - 1) / fe::TT_K, (P.Ny + 2 + fe::TT_J - 1) / fe::TT_J, (P.Nx + 2 + fe::TT_I - 1) / fe::TT_I);
+  // the top ring level (latency-bound, disjoint cells) runs beside the tiled kernel on the side stream
+  const long long ring = (long long)(P.Nx + 2) * (P.Ny + 2);
+  cudaEventRecord(d->fork, s);
+  cudaStreamWaitEvent(d->side, d->fork, 0);
+  fe::k_turb_ring<<<(unsigned)((ring + 255) / 256), 256, 0, d->side>>>(P, d->Q, st, stage);
+  cudaEventRecord(d->join, d->side);
   fe::k_turb_t<<<g, dim3(fe::TT_K, fe::TT_J, fe::TT_I), 0, s>>>(P, d->Q, st, stage);
-  if (P.surf <= 0) return 1;
+  cudaStreamWaitEvent(s, d->join, 0);
+  if (P.surf <= 0) return 2;
   fe::k_surface<<<dim3((P.Ny + 1 + 127) / 128, P.Nx + 1), 128, 0, s>>>(P, d->Q, st, stage);
-  return 2;
+  return 3;
 }
 
 // Everything a physics stage needs before its stage kernel, on state st: the SGS kernel and
@@ -697,7 +713,7 @@ static int launches_per_step(const fe_domain* d) {
   const Phys& P = d->P;
   int l = 4;
   if (P.turb || P.surf > 0) {
-    const int phys = 1 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) + ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
+    const int phys = 2 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) + ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
     l += (P.oneRK ? 1 : 3) * phys;
   }
   return l;

@@ -390,7 +390,9 @@ __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __res
   turb_cell(P, Q, st, i, j, k, lsc, lsm, sem, stage);
 }
 
-// The same ring in tiles of 32 levels x 4 rows x 2 planes per block of 256 threads. The block
+// The same ring in tiles of 32 levels x 4 rows x 2 planes per block of 256 threads, over the
+// interior levels [kMin, kMax) (so a warp's 32 lanes are 32 levels of one column and columns of
+// 32k levels fill every lane); the ring level kMax goes to k_turb_ring. The block
 // first forms the primitive variables (phi * rinv(rho), the same expression the per-cell form
 // evaluates) of the tile and its stencil halo once into shared memory, then the length scale and
 // sqrt(e/rho) of every tile column including the level below the tile, then each thread runs
@@ -419,11 +421,11 @@ __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __r
   __shared__ float seT[TT_I][TT_J][TT_K + 1];  // sqrt(e/rho), same levels
   const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
   const int tid = (tz * TT_J + ty) * TT_K + tx;
-  const int k0 = P.kMin - 1 + blockIdx.x * TT_K, j0 = P.jMin - 1 + blockIdx.y * TT_J, i0 = P.iMin - 1 + blockIdx.z * TT_I;
+  const int k0 = P.kMin + blockIdx.x * TT_K, j0 = P.jMin - 1 + blockIdx.y * TT_J, i0 = P.iMin - 1 + blockIdx.z * TT_I;
   const long long n = P.n;
   for (int p = tid; p < TP_N; p += TT_K * TT_J * TT_I) {
     const int pk = p % TP_K, pj = (p / TP_K) % TP_J, pi = p / (TP_K * TP_J);
-    const int i = i0 - 1 + pi, j = j0 - 1 + pj, k = k0 - 2 + pk;  // >= 1, >= 1, >= 0
+    const int i = i0 - 1 + pi, j = j0 - 1 + pj, k = k0 - 2 + pk;  // >= 1, >= 1, >= 1
     float v[TP_F] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     if (i < P.nxh && j < P.nyh && k < P.nzh) {
       const long long c = (long long)i * P.si + (long long)j * P.sj + k;
@@ -460,11 +462,40 @@ __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __r
     __syncthreads();
   }
   const int i = i0 + tz, j = j0 + ty, k = k0 + tx;
-  if (i > P.iMax || j > P.jMax || k > P.kMax) return;
+  if (i > P.iMax || j > P.jMax || k >= P.kMax) return;
   const TilePrims pr{tile, (tz + 1) * (TP_J * TP_K) + (ty + 1) * TP_K + (tx + 2)};
   const bool below = tke && k >= P.kMin;
   turb_cell_a<TilePrims, false>(P, Q, pr, st, i, j, k, tke ? lsT[tz][ty][tx + 1] : 0.0f, below ? lsT[tz][ty][tx] : 0.0f,
               below ? seT[tz][ty][tx] : 0.0f, tke ? seT[tz][ty][tx + 1] : -1.0f, stage);
+}
+
+// The ring level above k_turb_t's columns, k = kMax, one thread per cell on the per-cell path
+// (global primitives, the length scale of the cell and of the level below recomputed; the same
+// arithmetic as the tiled form). The ring level below, k = kMin - 1, is not computed: there the
+// eddy viscosity is zero by construction, so of its outputs only the vertical TKE flux is ever
+// read (by the transport term of the first level) and it is zero, which the zero-initialised
+// scratch already holds; its moisture gradients and length scale have no reader.
+__global__ void __launch_bounds__(256) k_turb_ring(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nj = P.Ny + 2;
+  if (t >= (long long)nj * (P.Nx + 2)) return;
+  const int j = P.jMin - 1 + (int)(t % nj);
+  const int i = P.iMin - 1 + (int)(t / nj);
+  const int k = P.kMax;
+  const long long n = P.n;
+  const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+  float lsc = 0.0f, lsm = 0.0f, sem = 0.0f;
+  if (P.turb && P.tke) {
+    const float *rho = st, *mth = st + 4 * n, *e = st + 5 * n;
+    lsc = length_scale(P, Q, rho, mth, e, c);
+    if (k >= P.kMin) {
+      lsm = length_scale(P, Q, rho, mth, e, c - 1);
+      sem = sqrtf(e[c - 1] * rinv(rho[c - 1]));
+    }
+  }
+  const GlobalPrims pr{st, st + n, st + 2 * n, st + 3 * n, st + 4 * n, P.ntke ? st + 5 * n : nullptr,
+                       P.nmoist ? st + (5 + P.ntke) * n : nullptr, n, c, P.si, P.sj};
+  turb_cell_a<GlobalPrims, false>(P, Q, pr, st, i, j, k, lsc, lsm, sem, -1.0f, stage);
 }
 
 // The surface layer of the columns the tiled SGS kernel covers (i in [iMin, iMax], j in

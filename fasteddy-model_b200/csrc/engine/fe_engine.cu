@@ -619,6 +619,10 @@ static cudaError_t march_attrs_one() {
   set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_ANY>, fe::MarchTile<8>::SMEM_BYTES);
   set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_DRY>, fe::MarchTile<8>::SMEM_BYTES);
   set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST>, fe::MarchTile<8>::SMEM_BYTES);
+  if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
+    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST, 0>, fe::MarchTile<8>::SMEM_BYTES);
+    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST, 1>, fe::MarchTile<8>::SMEM_BYTES);
+  }
   set((const void*)fe::k_march<STAGE, MODE, 4, fe::FL_ANY>, fe::MarchTile<4>::SMEM_BYTES);
   return e;
 }
@@ -635,21 +639,27 @@ static int march_attrs() {
 
 // Flavour of the march kernel that matches the configuration (fe_march.cuh).
 static int march_flavor(const Phys& P) {
-  if (P.pgf && P.tke && P.ntke == 1 && P.advSel == 3 && P.tkeAdvSel == 3) {
+  if (P.pgf && P.tke && P.ntke == 1 && P.advSel == 3 && P.tkeAdvSel == 3 && P.oneRK == 1) {
     if (P.nmoist == 0) return fe::FL_DRY;
     if (P.nmoist == 2 && P.qvAdvSel == 3) return fe::FL_MOIST;
   }
   return fe::FL_ANY;
 }
 
-template <int STAGE, int MODE, int TJ, int FL>
+template <int STAGE, int MODE, int TJ, int FL, int MP = -1>
 static void launch_march(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
                          const float* pcur, float* pnxt, float* frhs) {
   const Phys& P = d->P;
   const int ni = d->mni;
   dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + TJ - 1) / TJ, (P.Nx + ni - 1) / ni);
-  fe::k_march<STAGE, MODE, TJ, FL><<<g, dim3(fe::MK, TJ), fe::MarchTile<TJ>::SMEM_BYTES, s>>>(P, d->Q, cur, base, nxt,
-                                                                                              pcur, pnxt, frhs, ni);
+  fe::k_march<STAGE, MODE, TJ, FL, MP><<<g, dim3(fe::MK, TJ), fe::MarchTile<TJ>::SMEM_BYTES, s>>>(
+      P, d->Q, cur, base, nxt, pcur, pnxt, frhs, ni);
+}
+
+// The moist flavour's last stage as a pair (k_march MP = 0 then 1): the kernel that runs in the
+// steps without saturation adjustment carries none of its code.
+static bool split_last_stage(const fe_domain* d) {
+  return d->kind == FE_KERNEL_MARCH && d->mtj == 8 && march_flavor(d->P) == fe::FL_MOIST;
 }
 
 // Launch the fused stage kernel of stage STAGE in the domain's chosen form.
@@ -663,7 +673,14 @@ static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, c
     } else {
       switch (march_flavor(P)) {
         case fe::FL_DRY: launch_march<STAGE, MODE, 8, fe::FL_DRY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
-        case fe::FL_MOIST: launch_march<STAGE, MODE, 8, fe::FL_MOIST>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
+        case fe::FL_MOIST:
+          if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
+            launch_march<STAGE, MODE, 8, fe::FL_MOIST, 0>(d, s, cur, base, nxt, pcur, pnxt, frhs);
+            launch_march<STAGE, MODE, 8, fe::FL_MOIST, 1>(d, s, cur, base, nxt, pcur, pnxt, frhs);
+          } else {
+            launch_march<STAGE, MODE, 8, fe::FL_MOIST>(d, s, cur, base, nxt, pcur, pnxt, frhs);
+          }
+          break;
         default: launch_march<STAGE, MODE, 8, fe::FL_ANY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
       }
     }
@@ -685,7 +702,7 @@ static void enqueue_step(fe_domain* d, cudaStream_t s) {
   if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2);
   launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], nullptr);
   fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
-  d->launches += 4;
+  d->launches += 4 + (split_last_stage(d) ? 1 : 0);
 }
 
 static const int kGraphSteps = 8;
@@ -711,7 +728,7 @@ static int build_graph(fe_domain* d) {
 
 static int launches_per_step(const fe_domain* d) {
   const Phys& P = d->P;
-  int l = 4;
+  int l = 4 + (split_last_stage(d) ? 1 : 0);
   if (P.turb || P.surf > 0) {
     const int phys = 2 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) + ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
     l += (P.oneRK ? 1 : 3) * phys;

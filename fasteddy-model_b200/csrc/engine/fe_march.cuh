@@ -110,8 +110,9 @@ __device__ __forceinline__ float slot_b(const Phys& P, int s) {
 
 // Compile-time configurations ("flavours") of the march kernel. FL_ANY reads every selector at
 // run time; the others fix the field set and the advection schemes of the common cases (PGF on,
-// prognostic TKE, HYB56 for the hydro fields, TKE and q_v, WENO5 for q_l), so the field loop has
-// no run-time branches. The host picks the flavour that matches the configuration.
+// prognostic TKE, HYB56 for the hydro fields, TKE and q_v, WENO5 for q_l, SGS physics in the last
+// RK stage only), so the field loop has no run-time branches and the first two stages carry no
+// physics code. The host picks the flavour that matches the configuration.
 constexpr int FL_ANY = 0;
 constexpr int FL_DRY = 1;    // rho, rho u, rho v, rho w, rho theta, rho e
 constexpr int FL_MOIST = 2;  // ... plus rho q_v and rho q_l
@@ -224,7 +225,10 @@ __global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float
   for (int m = 0; m < NQ; m++) S[(5 + m) * n] = sq[m];
 }
 
-template <int STAGE, int MODE, int TJ, int FL>
+// MP: the saturation adjustment of the last stage. -1 decides per step from the device clock;
+// 0 and 1 are the two halves of a pair launched back to back, each returning at once unless the
+// step is its kind (0: no adjustment this step, compiled without the adjustment; 1: adjustment).
+template <int STAGE, int MODE, int TJ, int FL, int MP = -1>
 __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     k_march(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base, float* __restrict__ nxt,
             const float* __restrict__ pcur, float* __restrict__ pnxt, float* __restrict__ frhs, int ni) {
@@ -232,6 +236,11 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   const int nmoist = FL == FL_ANY ? P.nmoist : (FL == FL_MOIST ? 2 : 0);
   const bool pgf = FL == FL_ANY ? (P.pgf != 0) : true;
   const bool tke = FL == FL_ANY ? (P.tke != 0) : true;
+  // physics stages: every stage without oneRK, else the last; the flavours fix oneRK = 1
+  const bool phys = FL == FL_ANY ? ((P.oneRK == 0) || (STAGE == 2)) : (STAGE == 2);
+  const bool mpNow = phys && nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
+  if ((MP == 0 && mpNow) || (MP == 1 && !mpNow)) return;  // the other half of the pair runs this step
+  const bool mpStep = MP == 0 ? false : mpNow;
   using T = MarchTile<TJ>;
   constexpr int PK = T::PK, PLANE = T::PLANE;
   extern __shared__ __align__(16) float sm[];
@@ -248,7 +257,6 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   const long long col = (long long)j * sj + k;
   const long long tile0 = (long long)j0 * sj + k0;
   const int own = (ty + 3) * PK + (tx + 3);
-  const bool phys = (P.oneRK == 0) || (STAGE == 2);
   const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
 
   // ring cells of the staged planes handled by this thread
@@ -401,7 +409,6 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   }
 
   const bool same = (base == cur);  // first stage: the commit base is the input state
-  const bool mpStep = phys && nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
 
   // ---------------------------------------------------------------- march
   float *cs = B0, *ns = B1, *ps = B2;  // planes i, i+1 (own cell: s(i-2) until refilled), i-1

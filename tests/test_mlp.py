@@ -233,3 +233,22 @@ def test_trained_network_beats_the_tke_closure_a_priori(fe):
     assert err_mlp < 0.8 * err_tke
     for x in (fine, coarse, m):
         x.close()
+
+
+@pytest.mark.gpu
+def test_a_posteriori_validation_runs_all_three_models(fe):
+    """The a-posteriori check (fine run, learned LES, TKE LES from one coarse-grained state) on a
+    tiny case: every run stays finite, the learned run is cheaper than the fine one and every
+    profile comparison is reported. The accuracy figures are measured at full size and quoted in
+    the design notes; this only exercises the path."""
+    import importlib
+
+    v = importlib.import_module("fasteddy-model_b200.validate_learned")
+    out = v.main(["--coarse", "32", "32", "32", "--spinup", "10", "--collect", "10", "--eval", "10",
+                  "--sample", "5", "--average", "10", "--train-steps", "50"])
+    assert out["finite"]
+    for name in ("learned", "tke"):
+        for q in ("resolved_tke", "heat_flux"):
+            assert np.isfinite(out["profile_rel_l2_vs_fine"][name][q])
+    cost = out["device_ms_per_model_second"]
+    assert cost["learned"] < cost["fine"]

@@ -71,6 +71,7 @@ struct fe_domain {
   int tk = 32, tj = 4, ti = 2;       // cell-kernel tiling
   int kind = FE_KERNEL_MARCH;        // stage-kernel form
   int mtj = 8, mni = 64;             // march kernel: rows per tile, planes per thread block
+  int mniDefault = 64;               // planes per block chosen for the domain size at creation
   fe_mlp* mlp = nullptr;             // learned SGS closure (nullptr: TKE closure)
   float* feat = nullptr;             // its inputs per ring cell (allocated with the first network)
   cudaGraphExec_t graph = nullptr;
@@ -289,6 +290,20 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   }
   const Phys& P = d->P;
   const size_t n = (size_t)P.n, n2 = (size_t)P.n2;
+  {
+    // default march shape: the most planes per thread block (64, 32, 16, 8) that still gives every
+    // SM two blocks of 32 levels x 8 rows, so small domains fill the GPU
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    const long long cols = (long long)((P.Nz + fe::MK - 1) / fe::MK) * ((P.Ny + 7) / 8);
+    d->mni = 8;
+    for (int ni = 64; ni >= 8; ni /= 2)
+      if (cols * ((P.Nx + ni - 1) / ni) >= 2LL * nsm) {
+        d->mni = ni;
+        break;
+      }
+    d->mniDefault = d->mni;
+  }
   rc = march_attrs();
   for (int b = 0; b < 3 && rc == FE_OK; b++) {
     rc = dev_alloc(d, &d->st[b], n * P.nf);
@@ -898,7 +913,7 @@ extern "C" int fe_set_stage_kernel(fe_domain* d, int kind, int tj, int ni) {
   if (kind != FE_KERNEL_CELL && kind != FE_KERNEL_MARCH) return set_err(FE_ERR_ARG, "unknown stage-kernel form");
   if (kind == FE_KERNEL_MARCH) {
     if (tj <= 0) tj = 8;
-    if (ni <= 0) ni = 64;
+    if (ni <= 0) ni = d->mniDefault;
     if (tj != 4 && tj != 8) return set_err(FE_ERR_ARG, "march kernel: tj must be 4 or 8");
     d->mtj = tj;
     d->mni = ni;

@@ -175,7 +175,8 @@ int fe_set_tiling(fe_domain *d, int tk, int tj, int ti);
 /* Form of the fused stage kernel. FE_KERNEL_MARCH (the default): thread blocks of 32 levels
  * by tj rows (4 or 8) march ni planes along i with the x stencil in registers and the y/z
  * stencils in shared memory. FE_KERNEL_CELL: one thread per cell, tiled by fe_set_tiling.
- * tj/ni <= 0 select the defaults (8, 64). */
+ * tj/ni <= 0 select the defaults: tj = 8 and the ni chosen at creation (the most of 64, 32, 16, 8
+ * planes per block that still gives every SM two thread blocks). */
 #define FE_KERNEL_CELL 0
 #define FE_KERNEL_MARCH 1
 int fe_set_stage_kernel(fe_domain *d, int kind, int tj, int ni);

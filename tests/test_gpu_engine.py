@@ -160,7 +160,8 @@ def test_tiling_and_autotune_do_not_change_results(fe):
     host, inp, cfg = _setup(fe, "cbl_dry")
     a = fe.Domain(cfg)
     a.set_inputs(inp)
-    assert a.stage_kernel() == ("march", 8, 64)
+    kind, tj, ni = a.stage_kernel()  # default: tiles of 8 rows, planes per block chosen for the size
+    assert (kind, tj) == ("march", 8) and ni in (8, 16, 32, 64)
     a.advance(3)
     b = fe.Domain(cfg)
     b.set_inputs(inp)

@@ -291,6 +291,7 @@ def run_ours(args, rank: int, world: int, local: int) -> dict | None:
     cells = nx * ny * nz
     warm = graph_warmup(args.warmup)
     dom.advance(warm)
+    shape = list(dom.stage_kernel())  # form, rows per tile, planes per block
     stream = torch.cuda.ExternalStream(dom.stream(), device=device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -352,7 +353,7 @@ def run_ours(args, rank: int, world: int, local: int) -> dict | None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": desc, "cells": cells, "prognostic_fields": nprog, "dt_s": float(cfg.dt),
                    "parallelism": f"replicas{world}", "l2": "state 4*8*N bytes >> 126 MB L2, no flush needed",
-                   "warmup_steps_run": warm},
+                   "warmup_steps_run": warm, "stage_kernel": shape},
         "e2e": {"value": whole_job_rate(cells, args.steps, e2e_s, world), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "path": "cuda_timeIntCommence (drop-in C ABI), host buffers, one batch of K steps"},

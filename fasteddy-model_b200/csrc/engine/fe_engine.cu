@@ -291,14 +291,16 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   const Phys& P = d->P;
   const size_t n = (size_t)P.n, n2 = (size_t)P.n2;
   {
-    // default march shape: the most planes per thread block (64, 32, 16, 8) that still gives every
-    // SM two blocks of 32 levels x 8 rows, so small domains fill the GPU
+    // default march shape: the most planes per thread block of 32 levels x 8 rows (64, 32, 16, 8)
+    // that still leaves 20 waves of two blocks per SM (many blocks balance the SMs, long blocks
+    // amortise each block's first plane: 16 at 512x512x128, 64 at 1024x1024x256, as the
+    // autotuner finds), else 8
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     const long long cols = (long long)((P.Nz + fe::MK - 1) / fe::MK) * ((P.Ny + 7) / 8);
     d->mni = 8;
     for (int ni = 64; ni >= 8; ni /= 2)
-      if (cols * ((P.Nx + ni - 1) / ni) >= 2LL * nsm) {
+      if (cols * ((P.Nx + ni - 1) / ni) >= 40LL * nsm) {
         d->mni = ni;
         break;
       }

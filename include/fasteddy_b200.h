@@ -176,7 +176,7 @@ int fe_set_tiling(fe_domain *d, int tk, int tj, int ti);
  * by tj rows (4 or 8) march ni planes along i with the x stencil in registers and the y/z
  * stencils in shared memory. FE_KERNEL_CELL: one thread per cell, tiled by fe_set_tiling.
  * tj/ni <= 0 select the defaults: tj = 8 and the ni chosen at creation (the most of 64, 32, 16, 8
- * planes per block that still gives every SM two thread blocks). */
+ * planes per block that leaves 20 waves of two thread blocks per SM, else 8). */
 #define FE_KERNEL_CELL 0
 #define FE_KERNEL_MARCH 1
 int fe_set_stage_kernel(fe_domain *d, int kind, int tj, int ni);

@@ -577,23 +577,22 @@ static dim3 stage_grid(const fe_domain* d) {
   return dim3((P.Nz + d->tk - 1) / d->tk, (P.Ny + d->tj - 1) / d->tj, (P.Nx + d->ti - 1) / d->ti);
 }
 // Last-stage SGS physics on the +1 ring (k_turb_t: shared-memory tiles of primitives).
-// The last-stage SGS physics of the +1 ring (tiled kernel for the interior levels, ring-level
-// kernel for the level above) and then the surface layer of its columns; returns the number of
-// kernels launched.
+// The last-stage SGS physics of the +1 ring: the tiled kernel for the interior levels on stream s
+// and, beside it on the side stream, the surface layer of the ring's columns (first-level tau31,
+// tau32, tauTH3 and q_v flux, which the tiled kernel leaves alone) and the ring-level kernel for
+// the level above; the three write disjoint values. Returns the number of kernels launched.
 static int launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
   const Phys& P = d->P;
   const dim3 g((P.Nz + fe::TT_K - 1) / fe::TT_K, (P.Ny + 2 + fe::TT_J - 1) / fe::TT_J, (P.Nx + 2 + fe::TT_I - 1) / fe::TT_I);
-  // the top ring level (latency-bound, disjoint cells) runs beside the tiled kernel on the side stream
   const long long ring = (long long)(P.Nx + 2) * (P.Ny + 2);
   cudaEventRecord(d->fork, s);
   cudaStreamWaitEvent(d->side, d->fork, 0);
+  if (P.surf > 0) fe::k_surface<<<dim3((P.Ny + 1 + 127) / 128, P.Nx + 1), 128, 0, d->side>>>(P, d->Q, st, stage);
   fe::k_turb_ring<<<(unsigned)((ring + 255) / 256), 256, 0, d->side>>>(P, d->Q, st, stage);
   cudaEventRecord(d->join, d->side);
   fe::k_turb_t<<<g, dim3(fe::TT_K, fe::TT_J, fe::TT_I), 0, s>>>(P, d->Q, st, stage);
   cudaStreamWaitEvent(s, d->join, 0);
-  if (P.surf <= 0) return 2;
-  fe::k_surface<<<dim3((P.Ny + 1 + 127) / 128, P.Nx + 1), 128, 0, s>>>(P, d->Q, st, stage);
-  return 3;
+  return P.surf > 0 ? 3 : 2;
 }
 
 // Everything a physics stage needs before its stage kernel, on state st: the SGS kernel and

@@ -253,6 +253,9 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
                                             int j, int k, float lsc, float lsm, float sem, float sec, int stage) {
   const long long n = P.n;
   const long long c = (long long)i * P.si + (long long)j * P.sj + k;
+  // with the surface layer in its own kernel (not SURF), the first-level tau31, tau32, tauTH3 and
+  // q_v flux of its columns are that kernel's: this cell leaves them alone
+  const bool surfCell = !SURF && P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin;
   if (P.turb) {
     float* T = Q.tau;
     float Km = 0.0f;
@@ -293,13 +296,15 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
                                            e0));
         T[c] = -2.0f * r * Km * S11 + dev;
         T[n + c] = -2.0f * r * Km * S21;
-        T[2 * n + c] = -2.0f * r * Km * S31;
-        T[3 * n + c] = -2.0f * r * Km * S32;
         T[4 * n + c] = -2.0f * r * Km * S22 + dev;
         T[5 * n + c] = -2.0f * r * Km * S33 + dev;
         T[6 * n + c] = -r * Km * invPr * ST1;
         T[7 * n + c] = -r * Km * invPr * ST2;
-        T[8 * n + c] = -r * Km * invPr * ST3;
+        if (!surfCell) {
+          T[2 * n + c] = -2.0f * r * Km * S31;
+          T[3 * n + c] = -2.0f * r * Km * S32;
+          T[8 * n + c] = -r * Km * invPr * ST3;
+        }
       } else {
         const float t1 = 0.5f * (S11 * S11 + S22 * S22 + S33 * S33) + S21 * S21 + S31 * S31 + S32 * S32;
         const float N2 = P.g / thc * ST3;
@@ -308,13 +313,15 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
         const float invPr = 1.0f + 2.0f * delta / delta;
         T[c] = -2.0f * r * Km * S11;
         T[n + c] = -2.0f * r * Km * S21;
-        T[2 * n + c] = -2.0f * r * Km * S31;
-        T[3 * n + c] = -2.0f * r * Km * S32;
         T[4 * n + c] = -2.0f * r * Km * S22;
         T[5 * n + c] = -2.0f * r * Km * S33;
         T[6 * n + c] = -r * Km * invPr * ST1;
         T[7 * n + c] = -r * Km * invPr * ST2;
-        T[8 * n + c] = -r * Km * invPr * ST3;
+        if (!surfCell) {
+          T[2 * n + c] = -2.0f * r * Km * S31;
+          T[3 * n + c] = -2.0f * r * Km * S32;
+          T[8 * n + c] = -r * Km * invPr * ST3;
+        }
       }
     }
     if (Q.feat && k >= P.kMin) {
@@ -354,7 +361,7 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
         }
         Q.mtau[(3 * m + 0) * n + c] = g1;
         Q.mtau[(3 * m + 1) * n + c] = g2;
-        Q.mtau[(3 * m + 2) * n + c] = g3;
+        if (!(surfCell && m == 0)) Q.mtau[(3 * m + 2) * n + c] = g3;
       }
     }
   }

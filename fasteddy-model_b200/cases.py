@@ -12,6 +12,7 @@ input. Sizes can be shrunk for tests; the physics settings stay those of the cas
 from __future__ import annotations
 
 import math
+import re
 
 # Coriolis parameter f = 1e-4 s^-1: FastEddy takes a latitude, f = 2*Omega*sin(lat)
 F_CORIOLIS = 1.0e-4
@@ -138,12 +139,15 @@ def exact_tb(ny: int, nz: int, max_threads: int = 256) -> tuple[int, int]:
 
 
 def param_text(case: str, nx: int, ny: int, nz: int, *, dx: float = 20.0, dz: float = 10.0, dt: float = DT_STABLE,
-               nt: int = 100, topo: str = "", ug: float = 10.0, z0: float = 0.05, tb: tuple[int, int] | None = None) -> str:
+               nt: int = 100, topo: str = "", ug: float = 10.0, z0: float = 0.05, tb: tuple[int, int] | None = None,
+               params: dict | None = None) -> str:
     """Parameter file text of `case` at the given size.
 
     tb = (tBy, tBz) sets the reference build's thread-block shape; by default the
     tutorials' (4, 64). A shape that divides the halo-inclusive extents exactly avoids
-    the reference's out-of-range threads (see oracle/refrun.py)."""
+    the reference's out-of-range threads (see oracle/refrun.py).
+    params = {key: value} overrides keys of the case (e.g. advectionSelector, filterSelector);
+    every key must already be in the file."""
     tby, tbz = tb if tb is not None else (4, 64)
     ztop = nz * dz - 0.5 * dz
     if case == "cbl_dry":
@@ -159,8 +163,13 @@ def param_text(case: str, nx: int, ny: int, nz: int, *, dx: float = 20.0, dz: fl
                   zsb=round(0.8 * ztop, 3), pert=1)
     else:
         raise ValueError(f"unknown case {case}")
-    return _BASE.format(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, dt=dt, nt=nt, topo=topo, lat=LAT_F1EM4, ug=ug,
+    text = _BASE.format(nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dz, dt=dt, nt=nt, topo=topo, lat=LAT_F1EM4, ug=ug,
                         z0=z0, tby=tby, tbz=tbz, **kw)
+    for key, value in (params or {}).items():
+        text, n = re.subn(rf"^{re.escape(key)} = .*$", f"{key} = {value}", text, flags=re.M)
+        if n != 1:
+            raise ValueError(f"{key} is not a key of the {case} parameter file")
+    return text
 
 
 # Gaussian hill of the terrain cases: height 200 m, half-width 1 km (h = 200 * 2^-(r/1km)^2)

@@ -28,7 +28,10 @@ struct Phys {
   int itRestart;
   int ntke, nmoist, nf;      // prognostic field counts (nf = 5 + ntke + nmoist)
   int pgf, buoy, cor, turb, tke, advSel, tkeAdvSel, qvAdvSel, qiAdvSel;
+  int qlSch;                 // q_l's scheme as an ADV_* id (from qiAdvSel: 0 upwind, 1 WENO3, 2 WENO5)
   float bHyb, tkeBHyb, qvB;
+  int filt;                  // 6th-order vertical filter of rho w on (filterSelector = 1)
+  float filtCoef;            // 0.015625 filter_6th_coeff / dt
   float c_s, c_k;
   int surf, surfStab, idealSine, qskinInput;
   float z0, z0t, wth, tr, wq, qr, idealTs, idealTe, idealAmp, idealQts, idealQte, idealQamp;
@@ -204,6 +207,90 @@ template <bool FAST = false>
 __device__ __forceinline__ float weno5_flux(float m2, float m1, float z0, float p1, float p2, float p3, float vel) {
   const bool up = sgnf(vel) > 0.0f;
   return weno5_face<FAST>(up ? m2 : p3, up ? m1 : p2, up ? z0 : p1, up ? p1 : z0, up ? p2 : m1);
+}
+
+// Advection schemes by the reference's selector value (advectionSelector, TKEAdvSelector,
+// moistureAdvSelectorQv; cuda_hydroCoreDevice.cu:635-654). q_l's selector (0 upwind, 1 WENO3,
+// 2 WENO5, cuda_hydroCoreDevice.cu:726-736) is mapped onto these ids by the host.
+constexpr int ADV_UPWIND = 0, ADV_QUICK = 1, ADV_HYB34 = 2, ADV_HYB56 = 3, ADV_WENO3 = 4, ADV_WENO5 = 5,
+              ADV_CEN2 = 6;
+// The WENO schemes update the tendency direction by direction (three updates, x then y then
+// z); the others subtract the divergence summed over the three directions in one update.
+__host__ __device__ constexpr bool adv_split(int sel) { return sel == ADV_WENO3 || sel == ADV_WENO5; }
+
+// WENO3 face value from the upwind side (cuda_advectionDevice.cu:382-623): a = second cell
+// upwind, b = upwind cell, c = downwind cell. Candidates -a/2 + 3b/2 and (b + c)/2, smoothness
+// (b - a)^2 and (c - b)^2, linear weights 1/3 and 2/3, tol 1e-6. As in weno5_face the two
+// normalised weights come from one division: w_k ~ g_k q_j^2 (j != k), q = tol + beta.
+template <bool FAST = false>
+__device__ __forceinline__ float weno3_face(float a, float b, float c) {
+  const float g1 = 1.0f / 3.0f, g2 = 2.0f / 3.0f, tol = 1e-6f;
+  const float f1 = __fmaf_rn(1.5f, b, __fmul_rn(-0.5f, a));
+  const float f2 = __fmaf_rn(0.5f, b, __fmul_rn(0.5f, c));
+  const float d1 = __fsub_rn(b, a), d2 = __fsub_rn(c, b);
+  const float q1 = __fadd_rn(tol, __fmul_rn(d1, d1)), q2 = __fadd_rn(tol, __fmul_rn(d2, d2));
+  const float u1 = __fmul_rn(g1, __fmul_rn(q2, q2)), u2 = __fmul_rn(g2, __fmul_rn(q1, q1));
+  const float num = __fmaf_rn(u2, f2, __fmul_rn(u1, f1));
+  const float den = __fadd_rn(u1, u2);
+  return FAST ? __fdividef(num, den) : __fdiv_rn(num, den);
+}
+
+// Face value of scheme `sel` across the face between cells z0 (lower) and p1 (upper), stencil
+// m2..p3 as for hyb56_flux; the flux through the face is vel times this value. bfac = 1 - b
+// for the hybrid schemes.
+//   upwind  z0 if vel > 0 else p1        (cuda_advectionDevice.cu:126-158, fmaxf/fminf form)
+//   QUICK   (6 z0 + 3 p1 - m1)/8 if vel > 0 else (6 p1 + 3 z0 - p2)/8       (:206-254)
+//   HYB34   (7(p1+z0) - (p2+m1) + bfac sgn(vel) ((p2-m1) - 3(p1-z0)))/12   (:260-312)
+//   centred (z0 + p1)/2                                                    (:162-200)
+template <bool FAST = false>
+__device__ __forceinline__ float adv_face(int sel, float m2, float m1, float z0, float p1, float p2, float p3,
+                                          float vel, float bfac) {
+  switch (sel) {
+    case ADV_UPWIND:
+      return vel > 0.0f ? z0 : p1;
+    case ADV_QUICK: {
+      const bool up = vel > 0.0f;
+      const float a = up ? z0 : p1, b = up ? p1 : z0, c = up ? m1 : p2;
+      return __fmul_rn(0.125f, __fsub_rn(__fmaf_rn(6.0f, a, __fmul_rn(3.0f, b)), c));
+    }
+    case ADV_HYB34: {
+      const float twelfth = 1.0f / 12.0f;
+      const float cen = __fsub_rn(__fmul_rn(7.0f, __fadd_rn(p1, z0)), __fadd_rn(p2, m1));
+      const float upw = __fmaf_rn(-3.0f, __fsub_rn(p1, z0), __fsub_rn(p2, m1));
+      return __fmul_rn(twelfth, __fmaf_rn(copysignf(bfac, vel), upw, cen));
+    }
+    case ADV_HYB56:
+      return hyb56_flux(m2, m1, z0, p1, p2, p3, vel, bfac);
+    case ADV_WENO3: {
+      const bool up = sgnf(vel) > 0.0f;
+      return weno3_face<FAST>(up ? m1 : p2, up ? z0 : p1, up ? p1 : z0);
+    }
+    case ADV_WENO5:
+      return weno5_flux<FAST>(m2, m1, z0, p1, p2, p3, vel);
+    default:
+      return __fmul_rn(0.5f, __fadd_rn(z0, p1));
+  }
+}
+
+// q_l's selector (moistureAdvSelectorQi) as a scheme id.
+__host__ __device__ constexpr int ql_scheme(int qi) { return qi == 0 ? ADV_UPWIND : (qi == 1 ? ADV_WENO3 : ADV_WENO5); }
+// The filter's factor as the reference forms it (cuda_filtersDevice.cu:86): the literal
+// 0.015625 is double, so the quotient is taken in double and stored as float.
+__host__ __device__ inline float filter_coef(float coeff, float dt) { return (float)(0.015625 * (double)coeff / (double)(1.0f * dt)); }
+
+// 6th-order vertical filter of rho w (cuda_filtersDevice.cu:73-122; Xue 2000, Knievel et al.
+// 2007), stencil s[k-3..k+3] as m3..p3: face fluxes 10 d1 - 5 d3 + d5 at k-1/2 and k+1/2, each
+// kept only where its product with the face's first difference is not negative (the reference's
+// fmaxf(copysign(1, grad), 0): a product of -0 also drops it), scaled by `coef` =
+// 0.015625 filter_6th_coeff / dt.
+__device__ __forceinline__ float filter6_tend(float m3, float m2, float m1, float z0, float p1, float p2, float p3,
+                                              float coef) {
+  const float dm = __fsub_rn(z0, m1), dp = __fsub_rn(p1, z0);
+  float fm = __fadd_rn(__fmaf_rn(-5.0f, __fsub_rn(p1, m2), __fmul_rn(10.0f, dm)), __fsub_rn(p2, m3));
+  float fp = __fadd_rn(__fmaf_rn(-5.0f, __fsub_rn(p2, m1), __fmul_rn(10.0f, dp)), __fsub_rn(p3, m2));
+  if (signbit(__fmul_rn(dm, fm))) fm = 0.0f;
+  if (signbit(__fmul_rn(dp, fp))) fp = 0.0f;
+  return __fmul_rn(coef, __fsub_rn(fp, fm));
 }
 
 // Face velocities of a cell: lower/upper faces in x, y, z (cuda_advectionDevice.cu:54-121).

@@ -156,18 +156,27 @@ static int check_config(const fe_config* c) {
   if (c->Nh != 3) return set_err(FE_ERR_CONFIG, "Nh must be 3");
   if (c->Nx < 3 || c->Ny < 3 || c->Nz < 2) return set_err(FE_ERR_CONFIG, "need Nx,Ny >= 3 and Nz >= 2");
   if (c->hydroBCs != 2) return set_err(FE_ERR_CONFIG, "only hydroBCs = 2 (periodic horizontal, ABL vertical)");
-  if (c->advectionSelector != 3 && c->advectionSelector != 5)
-    return set_err(FE_ERR_CONFIG, "advectionSelector must be 3 (HYB56) or 5 (WENO5)");
-  if (c->turbulenceSelector > 0 && c->TKESelector > 0 && c->TKEAdvSelector != 3 && c->TKEAdvSelector != 5)
-    return set_err(FE_ERR_CONFIG, "TKEAdvSelector must be 3 or 5");
-  if (c->diffusionSelector != 0 || c->filterSelector != 0 || c->lsfSelector != 0)
-    return set_err(FE_ERR_CONFIG, "diffusion, explicit filter and large-scale forcing are not on this path");
+  // selector ranges as the reference's parameter reader checks them (hydro_core.c:221-349)
+  if (c->advectionSelector < 0 || c->advectionSelector > 6) return set_err(FE_ERR_CONFIG, "advectionSelector must be 0..6");
+  if (!(c->b_hyb >= 0.0f && c->b_hyb <= 1.0f)) return set_err(FE_ERR_CONFIG, "b_hyb must be in [0, 1]");
+  if (c->turbulenceSelector > 0 && c->TKESelector > 0) {
+    if (c->TKEAdvSelector < 0 || c->TKEAdvSelector > 6) return set_err(FE_ERR_CONFIG, "TKEAdvSelector must be 0..6");
+    if (!(c->TKEAdvSelector_b_hyb >= 0.0f && c->TKEAdvSelector_b_hyb <= 1.0f))
+      return set_err(FE_ERR_CONFIG, "TKEAdvSelector_b_hyb must be in [0, 1]");
+  }
+  if (c->diffusionSelector != 0 || c->lsfSelector != 0)
+    return set_err(FE_ERR_CONFIG, "molecular diffusion and large-scale forcing are not on this path");
+  if (c->filterSelector < 0 || c->filterSelector > 1) return set_err(FE_ERR_CONFIG, "filterSelector must be 0 or 1");
+  if (c->filterSelector > 0 && !(c->filter_6th_coeff >= 0.0f && c->filter_6th_coeff <= 1.0f))
+    return set_err(FE_ERR_CONFIG, "filter_6th_coeff must be in [0, 1]");
   if (c->moistureSelector > 0) {
     if (c->moistureNvars < 1 || c->moistureNvars > 2) return set_err(FE_ERR_CONFIG, "moistureNvars must be 1 or 2");
-    if (c->moistureAdvSelectorQv != 3 && c->moistureAdvSelectorQv != 5)
-      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQv must be 3 or 5");
-    if (c->moistureNvars > 1 && c->moistureAdvSelectorQi != 2)
-      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQi must be 2 (WENO5)");
+    if (c->moistureAdvSelectorQv < 0 || c->moistureAdvSelectorQv > 6)
+      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQv must be 0..6");
+    if (!(c->moistureAdvSelectorQv_b >= 0.0f && c->moistureAdvSelectorQv_b <= 1.0f))
+      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQv_b must be in [0, 1]");
+    if (c->moistureNvars > 1 && (c->moistureAdvSelectorQi < 0 || c->moistureAdvSelectorQi > 2))
+      return set_err(FE_ERR_CONFIG, "moistureAdvSelectorQi must be 0..2");
   }
   if (c->surflayerSelector < 0 || c->surflayerSelector > 2) return set_err(FE_ERR_CONFIG, "surflayerSelector 0..2");
   if (c->TKESelector > 1) return set_err(FE_ERR_CONFIG, "TKESelector must be 0 or 1");
@@ -205,7 +214,10 @@ static void make_phys(fe_domain* d) {
   P.tkeAdvSel = c.TKEAdvSelector;
   P.qvAdvSel = c.moistureAdvSelectorQv;
   P.qiAdvSel = c.moistureAdvSelectorQi;
+  P.qlSch = fe::ql_scheme(c.moistureAdvSelectorQi);
   P.bHyb = c.b_hyb; P.tkeBHyb = c.TKEAdvSelector_b_hyb; P.qvB = c.moistureAdvSelectorQv_b;
+  P.filt = c.filterSelector > 0;
+  P.filtCoef = fe::filter_coef(c.filter_6th_coeff, c.dt);
   P.c_s = c.c_s; P.c_k = c.c_k;
   P.surf = c.surflayerSelector;
   P.surfStab = c.surflayer_stab;
@@ -657,7 +669,7 @@ static int march_attrs() {
 static int march_flavor(const Phys& P) {
   if (P.pgf && P.tke && P.ntke == 1 && P.advSel == 3 && P.tkeAdvSel == 3 && P.oneRK == 1) {
     if (P.nmoist == 0) return fe::FL_DRY;
-    if (P.nmoist == 2 && P.qvAdvSel == 3) return fe::FL_MOIST;
+    if (P.nmoist == 2 && P.qvAdvSel == 3 && P.qlSch == fe::ADV_WENO5) return fe::FL_MOIST;
   }
   return fe::FL_ANY;
 }

@@ -612,59 +612,59 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
   }
   const float invD = Q.invD[c];
 
-  auto adv56 = [&](const float* __restrict__ s, float b) -> float {
+  // Summed schemes: F -= invD (Dx + Dy + Dz) in one update; D = u+ f+ - u- f- per direction.
+  auto advSum = [&](const float* __restrict__ s, int sel, float b) -> float {
     const float bf = 1.0f - b;
     float fxp, fxm, fyp, fym, fzp, fzm;
     {
       const float m3 = s[c - 3 * si], m2 = s[c - 2 * si], m1 = s[c - si], z0 = s[c], p1 = s[c + si], p2 = s[c + 2 * si],
                   p3 = s[c + 3 * si];
-      fxp = hyb56_flux(m2, m1, z0, p1, p2, p3, fv.up, bf);
-      fxm = hyb56_flux(m3, m2, m1, z0, p1, p2, fv.um, bf);
+      fxp = adv_face(sel, m2, m1, z0, p1, p2, p3, fv.up, bf);
+      fxm = adv_face(sel, m3, m2, m1, z0, p1, p2, fv.um, bf);
     }
     {
       const float m3 = s[c - 3 * sj], m2 = s[c - 2 * sj], m1 = s[c - sj], z0 = s[c], p1 = s[c + sj], p2 = s[c + 2 * sj],
                   p3 = s[c + 3 * sj];
-      fyp = hyb56_flux(m2, m1, z0, p1, p2, p3, fv.vp, bf);
-      fym = hyb56_flux(m3, m2, m1, z0, p1, p2, fv.vm, bf);
+      fyp = adv_face(sel, m2, m1, z0, p1, p2, p3, fv.vp, bf);
+      fym = adv_face(sel, m3, m2, m1, z0, p1, p2, fv.vm, bf);
     }
     {
       const float m3 = s[c - 3], m2 = s[c - 2], m1 = s[c - 1], z0 = s[c], p1 = s[c + 1], p2 = s[c + 2], p3 = s[c + 3];
-      fzp = hyb56_flux(m2, m1, z0, p1, p2, p3, fv.wp, bf);
-      fzm = hyb56_flux(m3, m2, m1, z0, p1, p2, fv.wm, bf);
+      fzp = adv_face(sel, m2, m1, z0, p1, p2, p3, fv.wp, bf);
+      fzm = adv_face(sel, m3, m2, m1, z0, p1, p2, fv.wm, bf);
     }
     const float Dx = fv.up * fxp - fv.um * fxm;
     const float Dy = fv.vp * fyp - fv.vm * fym;
     const float Dz = fv.wp * fzp - fv.wm * fzm;
     return invD * (Dx + Dy + Dz);
   };
-  // WENO5 applies x, y, z as three separate updates (cuda_hydroCoreDevice.cu:646-648)
-  auto advW5 = [&](float Facc, const float* __restrict__ s) -> float {
+  // WENO3/WENO5 apply x, y, z as three separate updates (cuda_hydroCoreDevice.cu:641-648)
+  auto advSplit = [&](float Facc, const float* __restrict__ s, int sel) -> float {
     {
       const float m3 = s[c - 3 * si], m2 = s[c - 2 * si], m1 = s[c - si], z0 = s[c], p1 = s[c + si], p2 = s[c + 2 * si],
                   p3 = s[c + 3 * si];
-      const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, fv.up);
-      const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, fv.um);
+      const float fp = adv_face(sel, m2, m1, z0, p1, p2, p3, fv.up, 1.0f);
+      const float fm = adv_face(sel, m3, m2, m1, z0, p1, p2, fv.um, 1.0f);
       Facc = Facc - invD * (fv.up * fp - fv.um * fm);
     }
     {
       const float m3 = s[c - 3 * sj], m2 = s[c - 2 * sj], m1 = s[c - sj], z0 = s[c], p1 = s[c + sj], p2 = s[c + 2 * sj],
                   p3 = s[c + 3 * sj];
-      const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, fv.vp);
-      const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, fv.vm);
+      const float fp = adv_face(sel, m2, m1, z0, p1, p2, p3, fv.vp, 1.0f);
+      const float fm = adv_face(sel, m3, m2, m1, z0, p1, p2, fv.vm, 1.0f);
       Facc = Facc - invD * (fv.vp * fp - fv.vm * fm);
     }
     {
       const float m3 = s[c - 3], m2 = s[c - 2], m1 = s[c - 1], z0 = s[c], p1 = s[c + 1], p2 = s[c + 2], p3 = s[c + 3];
-      const float fp = weno5_flux(m2, m1, z0, p1, p2, p3, fv.wp);
-      const float fm = weno5_flux(m3, m2, m1, z0, p1, p2, fv.wm);
+      const float fp = adv_face(sel, m2, m1, z0, p1, p2, p3, fv.wp, 1.0f);
+      const float fm = adv_face(sel, m3, m2, m1, z0, p1, p2, fv.wm, 1.0f);
       Facc = Facc - invD * (fv.wp * fp - fv.wm * fm);
     }
     return Facc;
   };
   auto advect = [&](float Facc, const float* __restrict__ s, int sel, float b) -> float {
-    if (sel == 3) return Facc - adv56(s, b);
-    if (sel == 5) return advW5(Facc, s);
-    return Facc;
+    if (adv_split(sel)) return advSplit(Facc, s, sel);
+    return Facc - advSum(s, sel, b);
   };
 
   // advection of the hydro fields, Rayleigh damping and buoyancy on w (cuda_hydroCoreDevice.cu:631-672)
@@ -697,7 +697,7 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
   F4 = advect(F4, mth, P.advSel, P.bHyb);
   if (P.ntke) Fe = advect(Fe, me, P.tkeAdvSel, P.tkeBHyb);
   if (P.nmoist > 0) Fq0 = advect(Fq0, mq0, P.qvAdvSel, P.qvB);
-  if (P.nmoist > 1 && P.qiAdvSel == 2) Fq1 = advW5(Fq1, mq1);
+  if (P.nmoist > 1) Fq1 = advect(Fq1, mq1, P.qlSch, 0.0f);
 
   // Coriolis (cuda_coriolisDevice.cu:50-58)
   if (P.cor) {
@@ -808,6 +808,10 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
       F4 = F4 + ((thd * P.L_v) / (Td2 * P.cp_gas)) * fc;
     }
   }
+
+  // explicit filter of rho w, every stage, after all other terms (cuda_hydroCoreDevice.cu:414-416)
+  if (P.filt)
+    F3 = __fadd_rn(F3, filter6_tend(mw[c - 3], mw[c - 2], mw[c - 1], mw[c], mw[c + 1], mw[c + 2], mw[c + 3], P.filtCoef));
 
   if (MODE == MODE_FRHS) {
     frhs[c] = F0;

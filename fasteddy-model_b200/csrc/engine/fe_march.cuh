@@ -94,12 +94,12 @@ __device__ __forceinline__ const float* slot_src(const Phys& P, const float* cur
   if (s == SL_QL) return cur + (long long)(6 + P.ntke) * P.n;
   return pcur;
 }
-// advection scheme of a slot: 3 = HYB56, 5 = WENO5 (q_l always WENO5: moistureAdvSelectorQi = 2)
+// advection scheme of a slot as an ADV_* id (q_l's from moistureAdvSelectorQi)
 __device__ __forceinline__ int slot_sel(const Phys& P, int s) {
   if (s < 5) return P.advSel;
   if (s == SL_E) return P.tkeAdvSel;
   if (s == SL_QV) return P.qvAdvSel;
-  return 5;
+  return P.qlSch;
 }
 __device__ __forceinline__ float slot_b(const Phys& P, int s) {
   if (s < 5) return P.bHyb;
@@ -385,9 +385,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float* src = f_src<FL>(P, cur, pcur, s);
       const float m3 = inArr ? src[cA - 3 * (long long)si] : 0.0f;
       const float m2 = B1[s * PLANE + own], m1 = B2[s * PLANE + own];
-      const float f = f_sel<FL>(P, s) == 3
-                          ? hyb56_flux(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev, 1.0f - slot_b(P, s))
-                          : weno5_flux<true>(m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev);
+      const float f = adv_face<true>(f_sel<FL>(P, s), m3, m2, m1, w[s][0], w[s][1], w[s][2], upPrev, 1.0f - slot_b(P, s));
       xcs[s * T::NT + tid] = __fmul_rn(upPrev, f);
     }
   }
@@ -504,6 +502,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     // The moist PGF, Coriolis and Rayleigh terms divide by rho and rho_BS through one correctly
     // rounded reciprocal per block (phi * (1/rho) instead of phi / rho: within an ulp).
     float F[8];
+    float fw = 0.0f;  // explicit filter of rho w (filterSelector = 1)
 #pragma unroll
     for (int s = 0; s < 8; s++) F[s] = 0.0f;
 
@@ -529,46 +528,37 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       }
     }
 
-    // advection of every field (cuda_hydroCoreDevice.cu:631-672; WENO5 as x, y, z updates)
+    // advection of every field (cuda_hydroCoreDevice.cu:631-736; WENO3/WENO5 as x, y, z updates)
 #pragma unroll
     for (int s = 0; s < 8; s++) {
       if (!f_on<FL>(P, s)) continue;
       const float* pl = cs + s * PLANE + own;
       const float z0 = w[s][0];
       const float xm2 = ns[s * PLANE + own], xm1 = ps[s * PLANE + own];
-      if (f_sel<FL>(P, s) == 3) {
-        const float bf = 1.0f - slot_b(P, s);
-        const float fxp = hyb56_flux(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
-        const float pxp = __fmul_rn(up, fxp);
-        const float Dx = __fsub_rn(pxp, xcs[s * T::NT + tid]);
-        xcs[s * T::NT + tid] = pxp;
-        float Dy, Dz;
-        {
-          const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
-          Dy = vp * hyb56_flux(m2, m1, z0, p1, p2, p3, vp, bf) - vm * hyb56_flux(m3, m2, m1, z0, p1, p2, vm, bf);
-        }
-        {
-          const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
-          Dz = wp * hyb56_flux(m2, m1, z0, p1, p2, p3, wp, bf) - wm * hyb56_flux(m3, m2, m1, z0, p1, p2, wm, bf);
-        }
-        F[s] = F[s] - invD * (Dx + Dy + Dz);
+      const int sel = f_sel<FL>(P, s);
+      const float bf = adv_split(sel) ? 1.0f : 1.0f - slot_b(P, s);
+      const float fxp = adv_face<true>(sel, xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
+      const float pxp = __fmul_rn(up, fxp);
+      const float Dx = __fsub_rn(pxp, xcs[s * T::NT + tid]);
+      xcs[s * T::NT + tid] = pxp;
+      float Dy, Dz;
+      {
+        const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
+        Dy = vp * adv_face<true>(sel, m2, m1, z0, p1, p2, p3, vp, bf) - vm * adv_face<true>(sel, m3, m2, m1, z0, p1, p2, vm, bf);
+      }
+      {
+        const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
+        Dz = wp * adv_face<true>(sel, m2, m1, z0, p1, p2, p3, wp, bf) - wm * adv_face<true>(sel, m3, m2, m1, z0, p1, p2, wm, bf);
+        // the explicit filter of rho w reads the same column; it is added after every other term
+        if (s == 3 && P.filt) fw = filter6_tend(m3, m2, m1, z0, p1, p2, p3, P.filtCoef);
+      }
+      if (adv_split(sel)) {
+        // WENO: x, y and z as three separate updates
+        F[s] = F[s] - invD * Dx;
+        F[s] = F[s] - invD * Dy;
+        F[s] = F[s] - invD * Dz;
       } else {
-        const float fxp = weno5_flux<true>(xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up);
-        const float pxp = __fmul_rn(up, fxp);
-        F[s] = F[s] - invD * __fsub_rn(pxp, xcs[s * T::NT + tid]);
-        xcs[s * T::NT + tid] = pxp;
-        {
-          const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
-          const float fp = weno5_flux<true>(m2, m1, z0, p1, p2, p3, vp);
-          const float fm = weno5_flux<true>(m3, m2, m1, z0, p1, p2, vm);
-          F[s] = F[s] - invD * (vp * fp - vm * fm);
-        }
-        {
-          const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
-          const float fp = weno5_flux<true>(m2, m1, z0, p1, p2, p3, wp);
-          const float fm = weno5_flux<true>(m3, m2, m1, z0, p1, p2, wm);
-          F[s] = F[s] - invD * (wp * fp - wm * fm);
-        }
+        F[s] = F[s] - invD * (Dx + Dy + Dz);
       }
       if (s == 3) {
         // Rayleigh damping and buoyancy act on F_w right after its advection
@@ -658,6 +648,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float Td2 = thd * powf(prd2 / P.p0, P.R_cp);
       F[4] = F[4] + ((thd * P.L_v) / (Td2 * P.cp_gas)) * fc;
     }
+    // explicit filter of rho w, every stage, after all other terms (cuda_hydroCoreDevice.cu:414-416)
+    if (P.filt) F[3] = __fadd_rn(F[3], fw);
 
     if (active) {
       if (MODE == MODE_FRHS) {

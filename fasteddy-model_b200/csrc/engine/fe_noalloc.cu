@@ -81,6 +81,7 @@ void make_phys(const fe_config& c, Phys& P) {
   P.tkeAdvSel = c.TKEAdvSelector;
   P.qvAdvSel = c.moistureAdvSelectorQv;
   P.qiAdvSel = c.moistureAdvSelectorQi;
+  P.qlSch = K::ql_scheme(c.moistureAdvSelectorQi);
   P.bHyb = c.b_hyb; P.tkeBHyb = c.TKEAdvSelector_b_hyb; P.qvB = c.moistureAdvSelectorQv_b;
   P.c_s = c.c_s; P.c_k = c.c_k;
   P.surf = c.surflayerSelector;

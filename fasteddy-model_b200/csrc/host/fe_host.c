@@ -70,6 +70,7 @@ float moistureCondTscale;
 int moistureCondBasePres;
 float moistureMPcallTscale;
 int filterSelector;
+float filter_6th_coeff;
 int dampingLayerSelector;
 float dampingLayerDepth;
 float temp_grnd, pres_grnd;
@@ -87,7 +88,7 @@ static int stabilityScheme;
 static float zStableBottom, stableGradient, zStableBottom2, stableGradient2, zStableBottom3, stableGradient3;
 static int thetaPerturbationSwitch;
 static float thetaHeight, thetaAmplitude;
-static float nu_0, filter_6th_coeff;
+static float nu_0;
 static char g_topoFile[1024];
 static char g_inFile[1024];
 static int ioOutputMode, frqOutput;

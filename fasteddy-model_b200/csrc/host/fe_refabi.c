@@ -58,6 +58,7 @@ static void fill_config(fe_config *c) {
   c->TKEAdvSelector_b_hyb = TKEAdvSelector_b_hyb; c->c_s = c_s; c->c_k = c_k;
   c->advectionSelector = advectionSelector; c->b_hyb = b_hyb;
   c->diffusionSelector = diffusionSelector; c->filterSelector = filterSelector; c->lsfSelector = lsfSelector;
+  c->filter_6th_coeff = filter_6th_coeff;
   c->surflayerSelector = surflayerSelector;
   c->surflayer_z0 = surflayer_z0; c->surflayer_z0t = surflayer_z0t; c->surflayer_wth = surflayer_wth;
   c->surflayer_tr = surflayer_tr; c->surflayer_wq = surflayer_wq; c->surflayer_qr = surflayer_qr;

@@ -60,6 +60,7 @@ extern float moistureCondTscale;
 extern int moistureCondBasePres;
 extern float moistureMPcallTscale;
 extern int filterSelector;
+extern float filter_6th_coeff;
 extern int dampingLayerSelector;
 extern float dampingLayerDepth;
 extern float temp_grnd, pres_grnd;

@@ -64,6 +64,7 @@ class FeConfig(ctypes.Structure):
         ("R_gas", ctypes.c_float), ("R_vapor", ctypes.c_float), ("Rv_Rg", ctypes.c_float), ("cp_gas", ctypes.c_float),
         ("cv_gas", ctypes.c_float), ("accel_g", ctypes.c_float), ("R_cp", ctypes.c_float), ("cp_R", ctypes.c_float),
         ("cp_cv", ctypes.c_float), ("refPressure", ctypes.c_float), ("kappa", ctypes.c_float), ("L_v", ctypes.c_float),
+        ("filter_6th_coeff", ctypes.c_float),
     ]
 
     def as_dict(self) -> dict:

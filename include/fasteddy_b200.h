@@ -96,9 +96,9 @@ typedef struct fe_config {
   int pgfSelector, buoyancySelector, coriolisSelector;
   int turbulenceSelector, TKESelector, TKEAdvSelector;
   float TKEAdvSelector_b_hyb, c_s, c_k;
-  int advectionSelector;              /* 3 = HYB56, 5 = WENO5 */
+  int advectionSelector;              /* 0 upwind, 1 QUICK, 2 HYB34, 3 HYB56, 4 WENO3, 5 WENO5, 6 centred 2nd */
   float b_hyb;
-  int diffusionSelector, filterSelector, lsfSelector;   /* must be 0 */
+  int diffusionSelector, filterSelector, lsfSelector;   /* diffusion and lsf must be 0; filter 0 or 1 */
   int surflayerSelector;              /* 0, 1 (heat flux) or 2 (skin temperature) */
   float surflayer_z0, surflayer_z0t, surflayer_wth, surflayer_tr, surflayer_wq, surflayer_qr;
   int surflayer_qskin_input, surflayer_stab, surflayer_idealsine;
@@ -117,6 +117,7 @@ typedef struct fe_config {
   int physics_oneRKonly;
   float temp_grnd, pres_grnd;
   float R_gas, R_vapor, Rv_Rg, cp_gas, cv_gas, accel_g, R_cp, cp_R, cp_cv, refPressure, kappa, L_v;
+  float filter_6th_coeff;             /* 6th-order vertical filter factor on rho w (filterSelector = 1) */
 } fe_config;
 
 /* Reference defaults (hydro_core.c:197-395 defaults, hydro_core.c:941-952 constants). */

@@ -251,10 +251,70 @@ static double weno5(const ora_domain *o, const double *s, int i, int j, int k) {
   return tot;
 }
 
+/* Face value of the lower-order schemes on the face between cells z0 (lower) and p1 (upper),
+ * stencil m1..p2; u = face velocity (cuda_advectionDevice.cu:126-312, 382-623):
+ *   0 upwind  max(0,u) z0 + min(0,u) p1 (returned divided by u: the flux is u times the value)
+ *   1 QUICK   [max(0,u)(6 z0 + 3 p1 - m1) + min(0,u)(6 p1 + 3 z0 - p2)] / 8, likewise
+ *   2 HYB34   (7(p1+z0) - (p2+m1) + (1-b) sgn(u) ((p2-m1) - 3(p1-z0))) / 12
+ *   4 WENO3   two-candidate WENO on the upwind side, weights g/(tol+beta)^2, g = 1/3, 2/3
+ *   6 centred (z0 + p1) / 2 */
+static double weno3_side(double a, double b, double c) {
+  double g1 = 1.0 / 3.0, g2 = 2.0 / 3.0, tol = 1e-6;
+  double f1 = -0.5 * a + 1.5 * b, f2 = 0.5 * b + 0.5 * c;
+  double w1 = g1 / pow(tol + pow(b - a, 2.0), 2.0), w2 = g2 / pow(tol + pow(c - b, 2.0), 2.0);
+  return (w1 / (w1 + w2)) * f1 + (w2 / (w1 + w2)) * f2;
+}
+
+static double low_order_face(int sel, double m1, double z0, double p1, double p2, double u, double b) {
+  double up = u > 0.0;
+  switch (sel) {
+    case 0: return up ? z0 : p1;
+    case 1: return up ? (6.0 * z0 + 3.0 * p1 - m1) / 8.0 : (6.0 * p1 + 3.0 * z0 - p2) / 8.0;
+    case 2: return (7.0 * (p1 + z0) - (p2 + m1) + (1.0 - b) * sgn1(u) * ((p2 - m1) - 3.0 * (p1 - z0))) / 12.0;
+    case 4: return sgn1(u) > 0.0 ? weno3_side(m1, z0, p1) : weno3_side(p2, p1, z0);
+    default: return 0.5 * (z0 + p1);
+  }
+}
+
+/* Flux divergence of a lower-order scheme: -invD sum_d (u+ f+ - u- f-). */
+static double low_order(const ora_domain *o, const double *s, int i, int j, int k, int sel, double b) {
+  size_t c = IX(o, i, j, k);
+  size_t st[3] = {(size_t)o->nyh * o->nzh, (size_t)o->nzh, 1};
+  const double *vel[3] = {o->ucf, o->vcf, o->wcf};
+  double div = 0.0;
+  int d;
+  for (d = 0; d < 3; d++) {
+    size_t q = st[d];
+    double m2 = s[c - 2 * q], m1 = s[c - q], z0 = s[c], p1 = s[c + q], p2 = s[c + 2 * q];
+    double fp = low_order_face(sel, m1, z0, p1, p2, vel[d][c + q], b);
+    double fm = low_order_face(sel, m2, m1, z0, p1, vel[d][c], b);
+    div += vel[d][c + q] * fp - vel[d][c] * fm;
+  }
+  return -o->invD[c] * div;
+}
+
 static double advect(const ora_domain *o, const double *s, int i, int j, int k, int sel, double b) {
   if (sel == 3) return hyb56(o, s, i, j, k, b);
   if (sel == 5) return weno5(o, s, i, j, k);
-  return 0.0; /* other schemes are rejected at configuration time */
+  return low_order(o, s, i, j, k, sel, b);
+}
+
+/* q_l's scheme (moistureAdvSelectorQi: 0 upwind, 1 WENO3, 2 WENO5; cuda_hydroCoreDevice.cu:725-736). */
+static double advect_ql(const ora_domain *o, const double *s, int i, int j, int k, int qi) {
+  if (qi == 2) return weno5(o, s, i, j, k);
+  return low_order(o, s, i, j, k, qi == 1 ? 4 : 0, 0.0);
+}
+
+/* 6th-order vertical filter of rho w (cuda_filtersDevice.cu:73-122): flux-limited so that it
+ * only diffuses down-gradient; coefficient 0.015625 filter_6th_coeff / dt. */
+static double filter6(const ora_domain *o, const double *s, int i, int j, int k) {
+  size_t c = IX(o, i, j, k);
+  double coef = 0.015625 * o->c.filter_6th_coeff / o->c.dt;
+  double fm = 10.0 * (s[c] - s[c - 1]) - 5.0 * (s[c + 1] - s[c - 2]) + (s[c + 2] - s[c - 3]);
+  double fp = 10.0 * (s[c + 1] - s[c]) - 5.0 * (s[c + 2] - s[c - 1]) + (s[c + 3] - s[c - 2]);
+  if (signbit((s[c] - s[c - 1]) * fm)) fm = 0.0;
+  if (signbit((s[c + 1] - s[c]) * fp)) fp = 0.0;
+  return coef * (fp - fm);
 }
 
 /* ------------------------------------------------------------------ surface layer */
@@ -650,7 +710,7 @@ int ora_build_frhs(ora_domain *o, int stage) {
         if (o->ntke) o->Ftke[c] += advect(o, o->tke, i, j, k, C->TKEAdvSelector, C->TKEAdvSelector_b_hyb);
         for (f = 0; f < o->nmoist; f++) {
           if (f == 0) o->Fmoist[0][c] += advect(o, o->moist[0], i, j, k, C->moistureAdvSelectorQv, C->moistureAdvSelectorQv_b);
-          else if (C->moistureAdvSelectorQi == 2) o->Fmoist[f][c] += weno5(o, o->moist[f], i, j, k);
+          else o->Fmoist[f][c] += advect_ql(o, o->moist[f], i, j, k, C->moistureAdvSelectorQi);
         }
         if (C->coriolisSelector > 0) {
           double z = o->zPos[c], rb = o->rhoBS[c], r = rho[c];
@@ -775,6 +835,12 @@ int ora_build_frhs(ora_domain *o, int stage) {
           }
     }
   }
+
+  /* 7. explicit filter of rho w, every stage (cuda_hydroCoreDevice.cu:414-416) */
+  if (C->filterSelector > 0)
+    for (i = iMin; i < iMax; i++)
+      for (j = jMin; j < jMax; j++)
+        for (k = kMin; k < kMax; k++) o->F[3][IX(o, i, j, k)] += filter6(o, w, i, j, k);
   return FE_OK;
 }
 

@@ -6,7 +6,7 @@ RK3 steps, so the FP64 oracle and the engine are checked against the reference's
 outputs. The reference runs with a thread-block shape that divides the halo-inclusive
 extents (no out-of-range threads), twice, and the run-to-run difference is stored too.
 
-usage: python tests/golden/make_reference_golden.py OUTDIR
+usage: python tests/golden/make_reference_golden.py OUTDIR [CASE ...]
 """
 from __future__ import annotations
 
@@ -22,10 +22,27 @@ sys.path.insert(0, ROOT)
 fe = importlib.import_module("fasteddy-model_b200")
 from oracle import refrun  # noqa: E402
 
+MOIST_HILL = dict(hill_halfwidth=60.0, hill_height=15.0, qv=(24.0, 8.0, 300.0))
 CASES = {
     "cbl_dry": dict(case="cbl_dry", nx=16, ny=12, nz=12, kw={}),
-    "moist_hill": dict(case="cbl_moist_hill", nx=16, ny=12, nz=12,
-                       kw=dict(hill_halfwidth=60.0, hill_height=15.0, qv=(24.0, 8.0, 300.0))),
+    "moist_hill": dict(case="cbl_moist_hill", nx=16, ny=12, nz=12, kw=MOIST_HILL),
+    # the other advection schemes and the explicit filter, by the reference's parameter keys
+    "dry_quick_filter": dict(case="cbl_dry", nx=16, ny=12, nz=12,
+                             kw=dict(params=dict(advectionSelector=1, TKEAdvSelector=2, TKEAdvSelector_b_hyb=0.5,
+                                                 filterSelector=1, filter_6th_coeff=0.12))),
+    "moist_weno3_filter": dict(case="cbl_moist_hill", nx=16, ny=12, nz=12,
+                               kw=dict(MOIST_HILL, params=dict(advectionSelector=4, TKEAdvSelector=6,
+                                                               moistureAdvSelectorQv=0, moistureAdvSelectorQi=1,
+                                                               filterSelector=1))),
+    "dry_hyb34": dict(case="cbl_dry", nx=16, ny=12, nz=12,
+                      kw=dict(params=dict(advectionSelector=2, b_hyb=0.3, TKEAdvSelector=4))),
+    "moist_centred_filter": dict(case="cbl_moist_hill", nx=16, ny=12, nz=12,
+                                 kw=dict(MOIST_HILL, params=dict(advectionSelector=6, TKEAdvSelector=0,
+                                                                 moistureAdvSelectorQv=1, moistureAdvSelectorQi=0,
+                                                                 filterSelector=1, filter_6th_coeff=0.12))),
+    "dry_upwind_filter": dict(case="cbl_dry", nx=16, ny=12, nz=12,
+                              kw=dict(params=dict(advectionSelector=0, TKEAdvSelector=1, filterSelector=1,
+                                                  filter_6th_coeff=0.12))),
 }
 
 
@@ -44,12 +61,14 @@ def make_inputs(name: str):
     return host, host.inputs()
 
 
-def main(out: str) -> None:
+def main(out: str, names=None) -> None:
     os.makedirs(out, exist_ok=True)
-    for name, c in CASES.items():
+    for name in names or list(CASES):
+        c = CASES[name]
         host, inp = make_inputs(name)
         ntke, nm = host.nfields()
-        text = fe.cases.param_text(c["case"], c["nx"], c["ny"], c["nz"], tb=fe.cases.exact_tb(c["ny"], c["nz"]))
+        text = fe.cases.param_text(c["case"], c["nx"], c["ny"], c["nz"], tb=fe.cases.exact_tb(c["ny"], c["nz"]),
+                                   params=c["kw"].get("params"))
         res = {"input_sha256": np.array(input_digest(inp))}
         for n in (1, 10):
             a = refrun.run(text, inp, n, host.shape, ntke, nm)
@@ -67,4 +86,4 @@ def main(out: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"), sys.argv[2:] or None)

@@ -31,6 +31,9 @@ def _load(name):
     return mk, np.load(path)
 
 
+GOLDEN_CASES = ["cbl_dry", "moist_hill", "dry_quick_filter", "moist_weno3_filter", "dry_hyb34", "moist_centred_filter",
+                "dry_upwind_filter"]
+
 TOL = {1: [1e-6, 1e-5, 2e-3, 2e-3, 1e-6], 10: [2e-6, 2e-5, 5e-3, 5e-3, 2e-6]}
 
 
@@ -39,11 +42,16 @@ def _compare(state, gold, n, spread):
         ref = gold[f"hydro_{n}"][f]
         bound = TOL[n][f] + 4 * spread[f] / max(np.abs(ref).max(), 1e-30)
         assert rel_l2(interior(state["hydroFlds"][f]), ref) < bound, (n, f)
+    # TKE and q_l: FP32 noise against the reference is ~3e-5; a wrong advection scheme for either
+    # field moves it by 1e-3 to 1e-2 in 10 steps
+    if f"tke_{n}" in gold:
+        assert rel_l2(interior(state["sgstke"][0]), gold[f"tke_{n}"][0]) < 2e-4, (n, "tke")
     if f"moist_{n}" in gold:
         assert rel_l2(interior(state["moist"][0]), gold[f"moist_{n}"][0]) < 2e-6
+        assert rel_l2(interior(state["moist"][1]), gold[f"moist_{n}"][1]) < 2e-4, (n, "q_l")
 
 
-@pytest.mark.parametrize("name", ["cbl_dry", "moist_hill"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
 def test_oracle_matches_reference_build(fe, name):
     mk, gold = _load(name)
     host, inp = mk.make_inputs(name)
@@ -57,8 +65,31 @@ def test_oracle_matches_reference_build(fe, name):
     host.cleanup()
 
 
+# Mistakes planted in the oracle (a scheme or the filter switched): each must fail the
+# comparison with the reference build's vectors, so the vectors pin the option they exercise.
+PLANTED = [("dry_quick_filter", "advectionSelector", 3), ("dry_quick_filter", "filterSelector", 0),
+           ("moist_weno3_filter", "advectionSelector", 5), ("moist_weno3_filter", "moistureAdvSelectorQi", 2),
+           ("dry_hyb34", "b_hyb", 0.0), ("dry_hyb34", "TKEAdvSelector", 3),
+           ("moist_centred_filter", "moistureAdvSelectorQv", 3), ("moist_centred_filter", "filterSelector", 0),
+           ("dry_upwind_filter", "TKEAdvSelector", 3), ("dry_upwind_filter", "advectionSelector", 1)]
+
+
+@pytest.mark.parametrize("name,key,value", PLANTED)
+def test_golden_vectors_reject_a_wrong_option(fe, name, key, value):
+    mk, gold = _load(name)
+    host, inp = mk.make_inputs(name)
+    cfg = host.config()
+    setattr(cfg, key, value)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    o.step(10)
+    with pytest.raises(AssertionError):
+        _compare(o.get_state(), gold, 10, gold["self_absdiff_10"])
+    host.cleanup()
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["cbl_dry", "moist_hill"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
 def test_engine_matches_reference_build(fe, name):
     mk, gold = _load(name)
     host, inp = mk.make_inputs(name)

@@ -352,7 +352,107 @@ def test_ensemble_of_uneven_domains_matches_members(fe):
 
 def test_unsupported_configuration_is_rejected(fe):
     host, inp, cfg = _setup(fe, "cbl_dry")
-    cfg.advectionSelector = 1
-    with pytest.raises(fe.FeError, match="advectionSelector"):
-        fe.Domain(cfg)
+    for key, value, msg in (("advectionSelector", 7, "advectionSelector"), ("diffusionSelector", 1, "diffusion"),
+                            ("lsfSelector", 1, "large-scale"), ("filterSelector", 2, "filterSelector")):
+        bad = type(cfg).from_buffer_copy(cfg)
+        setattr(bad, key, value)
+        with pytest.raises(fe.FeError, match=msg):
+            fe.Domain(bad)
+    host.cleanup()
+
+
+# The other advection schemes (upwind, QUICK, HYB34, WENO3, centred 2nd) on every advected field
+# and the explicit 6th-order filter of rho w, by the reference's own parameter keys. The last
+# case keeps the default schemes and adds the filter, so the compile-time moist form of the
+# march kernel carries it.
+SCHEME_CASES = {
+    "dry_quick_upwind_filter": ("cbl_dry", dict(advectionSelector=1, TKEAdvSelector=0, filterSelector=1)),
+    "dry_hyb34_centred_filter": ("cbl_dry", dict(advectionSelector=2, b_hyb=0.4, TKEAdvSelector=6, filterSelector=1,
+                                                 filter_6th_coeff=0.12)),
+    "hill_weno3_quick": ("hill_dry", dict(advectionSelector=4, TKEAdvSelector=1, filterSelector=1)),
+    "moist_centred_weno3": ("moist_hill", dict(advectionSelector=6, TKEAdvSelector=4, moistureAdvSelectorQv=2,
+                                               moistureAdvSelectorQv_b=0.3, moistureAdvSelectorQi=1, filterSelector=1)),
+    "moist_upwind_quick": ("moist_hill", dict(advectionSelector=0, TKEAdvSelector=2, TKEAdvSelector_b_hyb=0.5,
+                                              moistureAdvSelectorQv=1, moistureAdvSelectorQi=0)),
+    "moist_default_filter": ("moist_hill", dict(filterSelector=1, filter_6th_coeff=0.12)),
+}
+
+
+def _scheme_setup(fe, name):
+    base, params = SCHEME_CASES[name]
+    c = CASES[base]
+    host = fe.cases.setup_host(c["case"], c["nx"], c["ny"], c["nz"], params=params, **c["kw"])
+    return host, host.inputs(), host.config()
+
+
+@pytest.mark.parametrize("name", list(SCHEME_CASES))
+def test_advection_schemes_and_filter_match_oracle(fe, name):
+    """Stage tendencies of both kernel forms (stages 1 and 3) and the state after 4 steps
+    against the FP64 oracle, at the tolerances of the default schemes."""
+    host, inp, cfg = _scheme_setup(fe, name)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    ref = {stage: o.build_frhs(stage) for stage in (0, 2)}
+    for kind in ("march", "cell"):
+        dom = fe.Domain(cfg)
+        dom.set_inputs(inp)
+        dom.set_stage_kernel(kind, 8 if kind == "march" else 0, 0)
+        for stage in (0, 2):
+            g, r = dom.build_frhs(stage), ref[stage]
+            for f in range(5):
+                if np.abs(interior(r["hydroFrhs"][f])).max() == 0.0:
+                    assert np.abs(interior(g["hydroFrhs"][f])).max() < 1e-6
+                    continue
+                assert rel_l2(interior(g["hydroFrhs"][f]), interior(r["hydroFrhs"][f])) < 1e-3, (kind, stage, f)
+            if r["sgstkeFrhs"] is not None and stage == 2:
+                assert rel_l2(interior(g["sgstkeFrhs"][0]), interior(r["sgstkeFrhs"][0])) < 1e-3, kind
+            if r["moistFrhs"] is not None:
+                for m in range(r["moistFrhs"].shape[0]):
+                    if np.abs(interior(r["moistFrhs"][m])).max() > 0:
+                        assert rel_l2(interior(g["moistFrhs"][m]), interior(r["moistFrhs"][m])) < 1e-3, (kind, stage, m)
+        dom.close()
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    dom.advance(4)
+    o.step(4)
+    g, r = dom.get_state(), o.get_state()
+    for f in range(5):
+        assert rel_l2(interior(g["hydroFlds"][f]), interior(r["hydroFlds"][f])) < STATE_TOL[f], f
+    if r["sgstke"] is not None:
+        assert rel_l2(interior(g["sgstke"][0]), interior(r["sgstke"][0])) < 2e-3
+    if r["moist"] is not None:
+        assert rel_l2(interior(g["moist"][0]), interior(r["moist"][0])) < 1e-6
+        if np.abs(interior(r["moist"][1])).max() > 0:
+            assert rel_l2(interior(g["moist"][1]), interior(r["moist"][1])) < 2e-3
+    assert dom.nonfinite() == 0
+    dom.close()
+    host.cleanup()
+
+
+def test_filter_changes_only_rho_w(fe):
+    """With the filter on, the engine's tendency differs from the unfiltered one in rho w only,
+    by the oracle's filter term. The initial state is at rest in w, so the comparison starts from
+    the state after 20 steps."""
+    host, inp, cfg = _scheme_setup(fe, "moist_default_filter")
+    d = fe.Domain(cfg)
+    d.set_inputs(inp)
+    d.advance(20)
+    st = d.get_state()
+    d.close()
+    inp = dict(inp, hydroFlds=st["hydroFlds"], sgstke=st["sgstke"], moist=st["moist"])
+    out = {}
+    for filt in (0, 1):
+        cfg.filterSelector = filt
+        d = fe.Domain(cfg)
+        d.set_inputs(inp)
+        o = Oracle(cfg)
+        o.set_inputs(inp)
+        out[filt] = (d.build_frhs(0)["hydroFrhs"], o.build_frhs(0)["hydroFrhs"])
+        d.close()
+    for f in (0, 1, 2, 4):
+        np.testing.assert_array_equal(interior(out[1][0][f]), interior(out[0][0][f]))
+    dg = interior(out[1][0][3]).astype(np.float64) - interior(out[0][0][3])
+    dr = interior(out[1][1][3]) - interior(out[0][1][3])
+    assert np.abs(dr).max() > 0
+    assert rel_l2(dg, dr) < 1e-3
     host.cleanup()

@@ -70,31 +70,46 @@ def test_mass_is_conserved(fe):
     host.cleanup()
 
 
-def _advective_tendency_error(fe, n):
-    """Relative max error of the rho*theta advective tendency of one sine wave per domain
-    (n cells per wavelength) advected by a uniform wind."""
-    edits = (("stabilityScheme = 1", "stabilityScheme = 0"), ("thetaPerturbationSwitch = 1", "thetaPerturbationSwitch = 0"),
-             ("surflayerSelector = 1", "surflayerSelector = 0"), ("turbulenceSelector = 1", "turbulenceSelector = 0"),
-             ("TKESelector = 1", "TKESelector = 0"), ("coriolisSelector = 1", "coriolisSelector = 0"),
-             ("U_g = 10.0", "U_g = 5.0"))
+ADVECTION_ONLY = (("stabilityScheme = 1", "stabilityScheme = 0"), ("thetaPerturbationSwitch = 1", "thetaPerturbationSwitch = 0"),
+                  ("surflayerSelector = 1", "surflayerSelector = 0"), ("turbulenceSelector = 1", "turbulenceSelector = 0"),
+                  ("TKESelector = 1", "TKESelector = 0"), ("coriolisSelector = 1", "coriolisSelector = 0"),
+                  ("U_g = 10.0", "U_g = 5.0"))
+
+
+def _theta_advection(fe, n, profile, sel=3, b=0.0):
+    """rho*theta tendency and its exact value -u d(rho theta)/dx for theta = 300 + profile(x/L)
+    on one periodic wavelength of n cells, advected by a uniform 5 m/s wind with scheme `sel`.
+    profile returns (value, derivative in x/L)."""
+    edits = ADVECTION_ONLY + (("advectionSelector = 3", f"advectionSelector = {sel}"), ("b_hyb = 0.0", f"b_hyb = {b}"))
     host = _host(fe, "cbl_dry", n, 4, 4, edits)
     host.init(1)
     inp = host.inputs()
     H = inp["hydroFlds"].astype(np.float64)
     dx = 20.0
     L = n * dx
-    x = (np.arange(n + 6) - 3 + 0.5) * dx
+    x = ((np.arange(n + 6) - 3 + 0.5) * dx) / L
+    val, der = profile(x)
     rho = H[0]
-    H[4] = rho * (300.0 + np.sin(2 * np.pi * x / L))[:, None, None]
+    H[4] = rho * (300.0 + val)[:, None, None]
     o = Oracle(host.config())
     o.set_inputs(inp)
     o.lib.ora_set_state_f64(o.h, np.ascontiguousarray(H).ctypes.data_as(o.lib.ora_set_state_f64.argtypes[1]), None, None)
     F = o.build_frhs(0)["hydroFrhs"][4]
-    exact = -5.0 * rho * (2 * np.pi / L) * np.cos(2 * np.pi * x / L)[:, None, None]
-    # relative to the exact tendency: the grid spacing is fixed, so kh = 2 pi / n
-    err = np.abs(interior(F - exact)).max() / np.abs(interior(exact)).max()
+    exact = -5.0 * rho * (der / L)[:, None, None]
     host.cleanup()
-    return err
+    return interior(F), interior(exact)
+
+
+def _sine(x):
+    return np.sin(2 * np.pi * x), 2 * np.pi * np.cos(2 * np.pi * x)
+
+
+def _advective_tendency_error(fe, n, sel=3, b=0.0):
+    """Relative max error of the rho*theta advective tendency of one sine wave per domain
+    (n cells per wavelength) advected by a uniform wind."""
+    F, exact = _theta_advection(fe, n, _sine, sel, b)
+    # relative to the exact tendency: the grid spacing is fixed, so kh = 2 pi / n
+    return np.abs(F - exact).max() / np.abs(exact).max()
 
 
 def test_hyb56_advection_is_fifth_order(fe):
@@ -102,6 +117,57 @@ def test_hyb56_advection_is_fifth_order(fe):
     e2 = _advective_tendency_error(fe, 32)
     order = np.log2(e1 / e2)
     assert 4.6 < order < 5.4, order
+
+
+# Orders of the other schemes' tendency in the max norm on point values: upwind 1; QUICK 2
+# (its face value is third-order, but the difference of two face values of point data leaves a
+# (kh)^2/24 term); HYB34 3 with full upwinding (b = 0) and 4 centred (b = 1); centred 2nd 2.
+@pytest.mark.parametrize("sel,b,order", [(0, 0.0, 1.0), (1, 0.0, 2.0), (2, 0.0, 3.0), (2, 1.0, 4.0), (6, 0.0, 2.0)])
+def test_advection_scheme_orders(fe, sel, b, order):
+    e1 = _advective_tendency_error(fe, 32, sel, b)
+    e2 = _advective_tendency_error(fe, 64, sel, b)
+    assert abs(np.log2(e1 / e2) - order) < 0.3, (sel, b, np.log2(e1 / e2))
+
+
+@pytest.mark.parametrize("sel", range(7))
+def test_every_scheme_is_exact_on_linear_data(fe, sel):
+    """theta = 300 + |x/L - 1/2|: away from the two kinks every stencil sees linear data, where
+    each scheme's face value is exact (WENO3/WENO5: the smoothness indicators are equal, so the
+    weights reduce to the linear ones) and the tendency is -u rho dtheta/dx."""
+    n = 32
+    F, exact = _theta_advection(fe, n, lambda x: (np.abs(x - 0.5), np.sign(x - 0.5)), sel, 0.5)
+    away = np.r_[3:13, 19:29]  # cells whose +-3 stencil lies on one linear segment
+    np.testing.assert_allclose(F[away], exact[away], rtol=1e-9)
+
+
+def test_filter_damps_the_two_grid_mode_at_coeff_over_dt(fe):
+    """The 6th-order filter on rho w (cuda_filtersDevice.cu:73-122): for w = a(-1)^k both face
+    fluxes are +-32 a and pass the limiter, so the tendency is -64 a (0.015625 c/dt) = -(c/dt) a;
+    a profile linear in z has zero filtered flux. Checked on levels whose +-3 stencil is interior."""
+    coeff = 0.03
+    edits = REST + (("filterSelector = 0", "filterSelector = 1"), ("filter_6th_coeff = 0.03", f"filter_6th_coeff = {coeff}"))
+    host = _host(fe, "cbl_dry", 8, 8, 24, edits)
+    host.init(1)
+    inp = host.inputs()
+    cfg = host.config()
+    dt = float(np.float32(cfg.dt))
+    H = inp["hydroFlds"].astype(np.float64)
+    k = np.arange(H.shape[3])
+    lv = slice(6, H.shape[3] - 6)
+    rate = float(np.float32(coeff)) / dt  # filter_6th_coeff and dt are float parameters
+    for w, expect in ((0.01 * (-1.0) ** k, -rate * 0.01 * (-1.0) ** k), (1e-3 * k, 0.0 * k)):
+        H[3] = w[None, None, :] * np.ones(H.shape[1:3])[:, :, None]
+        tend = []
+        for filt in (0, 1):
+            cfg.filterSelector = filt
+            o = Oracle(cfg)
+            o.set_inputs(inp)
+            o.lib.ora_set_state_f64(o.h, np.ascontiguousarray(H).ctypes.data_as(o.lib.ora_set_state_f64.argtypes[1]),
+                                    None, None)
+            tend.append(o.build_frhs(0)["hydroFrhs"][3])
+        diff = (tend[1] - tend[0])[3:-3, 3:-3, lv]
+        np.testing.assert_allclose(diff, np.broadcast_to(expect[lv], diff.shape), rtol=1e-9, atol=1e-12)
+    host.cleanup()
 
 
 def test_neutral_surface_layer_log_law(fe):

@@ -105,6 +105,21 @@ Vg_grad = 0.0
 lsfSelector = 0
 lsf_horMnSubTerms = 0
 lsf_freq = 1.0
+lsf_w_surf = 0.0
+lsf_w_lev1 = 0.0
+lsf_w_lev2 = 0.0
+lsf_w_zlev1 = 100.0
+lsf_w_zlev2 = 200.0
+lsf_th_surf = 0.0
+lsf_th_lev1 = 0.0
+lsf_th_lev2 = 0.0
+lsf_th_zlev1 = 100.0
+lsf_th_zlev2 = 200.0
+lsf_qv_surf = 0.0
+lsf_qv_lev1 = 0.0
+lsf_qv_lev2 = 0.0
+lsf_qv_zlev1 = 100.0
+lsf_qv_zlev2 = 200.0
 physics_oneRKonly = 1
 """
 

@@ -32,6 +32,10 @@ struct Phys {
   float bHyb, tkeBHyb, qvB;
   int filt;                  // 6th-order vertical filter of rho w on (filterSelector = 1)
   float filtCoef;            // 0.015625 filter_6th_coeff / dt
+  int lsf, lsfSub;           // large-scale forcing; its subsidence terms (lsf_horMnSubTerms)
+  int lsfN;                  // steps between applications, roundf(lsf_freq/dt)
+  float lsfFac;              // the same as a float factor of the per-hour rates
+  float lsfW[5], lsfTh[5], lsfQv[5];  // surface value, values at zlev1 and zlev2, zlev1, zlev2
   float c_s, c_k;
   int surf, surfStab, idealSine, qskinInput;
   float z0, z0t, wth, tr, wq, qr, idealTs, idealTe, idealAmp, idealQts, idealQte, idealQamp;
@@ -63,6 +67,8 @@ struct Ptrs {
   const float* delta;          // grid scale (dx dy dz D)^(1/3) per cell, or nullptr (evaluated inline)
   float* feat;                 // inputs of the learned closure per ring cell (11 fields), or nullptr
   float* sgsF;                 // SGS tendencies for the march kernel's physics stages (7 fields), or nullptr
+  float* lsfProf;              // slab means of rho, rho u, rho v, rho theta, rho q_v (nzh levels each), or nullptr
+  double* lsfPart;             // per-block FP64 partial sums of the slab means
   int *clockIt;                // simTime_it of the step being computed
   float *clockTime;            // simTime of the step being computed
 };
@@ -277,6 +283,49 @@ __host__ __device__ constexpr int ql_scheme(int qi) { return qi == 0 ? ADV_UPWIN
 // The filter's factor as the reference forms it (cuda_filtersDevice.cu:86): the literal
 // 0.015625 is double, so the quotient is taken in double and stored as float.
 __host__ __device__ inline float filter_coef(float coeff, float dt) { return (float)(0.015625 * (double)coeff / (double)(1.0f * dt)); }
+
+// ---------------------------------------------------------------- large-scale forcing
+// Step `it` applies the forcing in its last RK stage and takes the slab means at its start
+// (cuda_hydroCoreDevice.cu:401-406, cuda_timeIntDevice.cu:125-127): every lsfN steps after
+// the restart step (the forcing also needs lsfN steps since the restart).
+__device__ __forceinline__ bool lsf_step(const Phys& P, int it) {
+  return P.lsf && it > P.itRestart && (it - P.itRestart) >= P.lsfN && it % P.lsfN == 0;
+}
+__device__ __forceinline__ bool lsf_means_step(const Phys& P, int it) {
+  return P.lsf && P.lsfSub && it > P.itRestart && it % P.lsfN == 0;
+}
+// Piecewise-linear forcing profile times rho (cuda_largeScaleForcingsDevice.cu:177-212): linear
+// from the surface value to lev1 at zlev1, to lev2 at zlev2, constant lev2 above.
+__device__ __forceinline__ float lsf_profile(const float (&p)[5], float z, float rho) {
+  if (z <= p[3]) return (p[0] + ((p[1] - p[0]) / p[3]) * z) * rho;
+  if (z <= p[4]) return (p[1] + ((p[2] - p[1]) / (p[4] - p[3])) * (z - p[3])) * rho;
+  return p[2] * rho;
+}
+// The per-hour rates times the application interval in steps (the double literal 3600.0 makes
+// the division double, as in the reference).
+__device__ __forceinline__ float lsf_rate(const Phys& P, float f) { return (float)((double)(f * P.lsfFac) / 3600.0); }
+// Vertical difference of the slab-mean ratio <rho phi>/<rho> between levels k+1 and k-1.
+__device__ __forceinline__ float lsf_dmean(const float* prof, int nzh, int f, int k) {
+  return prof[f * nzh + k + 1] / prof[k + 1] - prof[f * nzh + k - 1] / prof[k - 1];
+}
+// Large-scale forcing of one interior cell (cuda_largeScaleForcingsDevice.cu:155-252): theta and
+// q_v tendencies, then the subsidence terms -w_ls rho d<phi>/dz of u, v, theta and q_v from the
+// slab means (w_ls already carries rho, so rho enters twice, as in the reference).
+// Fu/Fv/Fth/Fqv are the cell's tendencies of rho u, rho v, rho theta, rho q_v.
+__device__ __forceinline__ void lsf_tend(const Phys& P, const Ptrs& Q, long long c, int k, float z, float rho,
+                                         float& Fu, float& Fv, float& Fth, float& Fqv) {
+  Fth = Fth + lsf_rate(P, lsf_profile(P.lsfTh, z, rho));
+  if (P.moist) Fqv = Fqv + lsf_rate(P, lsf_profile(P.lsfQv, z, rho));
+  if (P.lsfSub) {
+    const float fw = lsf_rate(P, lsf_profile(P.lsfW, z, rho));
+    const float dz = Q.zPos[c + 1] - Q.zPos[c - 1];
+    const float* pr = Q.lsfProf;
+    Fu = Fu - fw * rho * lsf_dmean(pr, P.nzh, 1, k) / dz;
+    Fv = Fv - fw * rho * lsf_dmean(pr, P.nzh, 2, k) / dz;
+    Fth = Fth - fw * rho * lsf_dmean(pr, P.nzh, 3, k) / dz;
+    if (P.moist) Fqv = Fqv - fw * rho * lsf_dmean(pr, P.nzh, 4, k) / dz;
+  }
+}
 
 // 6th-order vertical filter of rho w (cuda_filtersDevice.cu:73-122; Xue 2000, Knievel et al.
 // 2007), stencil s[k-3..k+3] as m3..p3: face fluxes 10 d1 - 5 d3 + d5 at k-1/2 and k+1/2, each

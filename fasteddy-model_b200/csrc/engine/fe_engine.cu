@@ -63,6 +63,8 @@ struct fe_domain {
   float* scratch = nullptr;
   float* surf = nullptr;
   float* frhs = nullptr;
+  void* lsfMem = nullptr;                              // slab means and their per-block partial sums
+  int lsfBlocks = 0;                                   // blocks of the slab-mean kernel
   void* clock = nullptr;
   unsigned long long* counter = nullptr;
   float simTime = 0.0f;
@@ -126,6 +128,10 @@ extern "C" void fe_config_defaults(fe_config* c) {
   c->dX = c->dY = c->dZ = 1.0f;
   c->surflayer_ideal_amp = 0.1f;
   c->surflayer_ideal_qamp = 0.1f;
+  c->filter_6th_coeff = 0.12f;
+  c->lsf_freq = 1.0f;
+  c->lsf_w_zlev1 = c->lsf_th_zlev1 = c->lsf_qv_zlev1 = 100.0f;
+  c->lsf_w_zlev2 = c->lsf_th_zlev2 = c->lsf_qv_zlev2 = 200.0f;
   fe_config_derive(c, 54.0f);
 }
 
@@ -164,8 +170,13 @@ static int check_config(const fe_config* c) {
     if (!(c->TKEAdvSelector_b_hyb >= 0.0f && c->TKEAdvSelector_b_hyb <= 1.0f))
       return set_err(FE_ERR_CONFIG, "TKEAdvSelector_b_hyb must be in [0, 1]");
   }
-  if (c->diffusionSelector != 0 || c->lsfSelector != 0)
-    return set_err(FE_ERR_CONFIG, "molecular diffusion and large-scale forcing are not on this path");
+  if (c->diffusionSelector != 0) return set_err(FE_ERR_CONFIG, "molecular diffusion is not on this path");
+  if (c->lsfSelector < 0 || c->lsfSelector > 1) return set_err(FE_ERR_CONFIG, "lsfSelector must be 0 or 1");
+  if (c->lsfSelector > 0) {
+    if (!(c->lsf_freq >= 1e-3f && c->lsf_freq <= 1e3f)) return set_err(FE_ERR_CONFIG, "lsf_freq must be in [1e-3, 1e3]");
+    if ((int)roundf(c->lsf_freq / c->dt) < 1) return set_err(FE_ERR_CONFIG, "lsf_freq must be at least dt/2");
+    if (c->lsf_horMnSubTerms < 0 || c->lsf_horMnSubTerms > 1) return set_err(FE_ERR_CONFIG, "lsf_horMnSubTerms must be 0 or 1");
+  }
   if (c->filterSelector < 0 || c->filterSelector > 1) return set_err(FE_ERR_CONFIG, "filterSelector must be 0 or 1");
   if (c->filterSelector > 0 && !(c->filter_6th_coeff >= 0.0f && c->filter_6th_coeff <= 1.0f))
     return set_err(FE_ERR_CONFIG, "filter_6th_coeff must be in [0, 1]");
@@ -218,6 +229,16 @@ static void make_phys(fe_domain* d) {
   P.bHyb = c.b_hyb; P.tkeBHyb = c.TKEAdvSelector_b_hyb; P.qvB = c.moistureAdvSelectorQv_b;
   P.filt = c.filterSelector > 0;
   P.filtCoef = fe::filter_coef(c.filter_6th_coeff, c.dt);
+  P.lsf = c.lsfSelector > 0;
+  P.lsfSub = P.lsf && c.lsf_horMnSubTerms == 1;
+  P.lsfN = P.lsf ? (int)roundf(c.lsf_freq / c.dt) : 1;  // as the reference rounds it (cuda_hydroCoreDevice.cu:402-404)
+  P.lsfFac = (float)P.lsfN;
+  {
+    const float w[5] = {c.lsf_w_surf, c.lsf_w_lev1, c.lsf_w_lev2, c.lsf_w_zlev1, c.lsf_w_zlev2};
+    const float th[5] = {c.lsf_th_surf, c.lsf_th_lev1, c.lsf_th_lev2, c.lsf_th_zlev1, c.lsf_th_zlev2};
+    const float qv[5] = {c.lsf_qv_surf, c.lsf_qv_lev1, c.lsf_qv_lev2, c.lsf_qv_zlev1, c.lsf_qv_zlev2};
+    for (int m = 0; m < 5; m++) { P.lsfW[m] = w[m]; P.lsfTh[m] = th[m]; P.lsfQv[m] = qv[m]; }
+  }
   P.c_s = c.c_s; P.c_k = c.c_k;
   P.surf = c.surflayerSelector;
   P.surfStab = c.surflayer_stab;
@@ -268,6 +289,7 @@ static void free_domain(fe_domain* d) {
   cudaFree(d->scratch);
   cudaFree(d->surf);
   cudaFree(d->frhs);
+  cudaFree(d->lsfMem);
   cudaFree(d->feat);
   cudaFree(d->clock);
   cudaFree(d->counter);
@@ -317,6 +339,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
         break;
       }
     d->mniDefault = d->mni;
+    d->lsfBlocks = P.lsfSub ? 2 * nsm : 0;
   }
   rc = march_attrs();
   for (int b = 0; b < 3 && rc == FE_OK; b++) {
@@ -329,6 +352,16 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   if (rc == FE_OK) rc = dev_alloc(d, &d->base, n * 3);
   if (rc == FE_OK) rc = dev_alloc(d, &d->scratch, n * nscr);
   if (rc == FE_OK) rc = dev_alloc(d, &d->surf, n2 * 11);
+  const size_t lsfProfBytes = ((size_t)5 * P.nzh * sizeof(float) + 255) / 256 * 256;
+  if (rc == FE_OK && P.lsfSub) {
+    const size_t bytes = lsfProfBytes + (size_t)d->lsfBlocks * 5 * P.nzh * sizeof(double);
+    if (cudaMalloc(&d->lsfMem, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      rc = set_err(FE_ERR_NOMEM, "slab-mean buffer allocation failed");
+    } else {
+      cudaMemsetAsync(d->lsfMem, 0, bytes, d->stream);
+    }
+  }
   if (rc == FE_OK) {
     cudaError_t e = cudaMalloc(&d->clock, 64);
     if (e == cudaSuccess) e = cudaMalloc(&d->counter, sizeof(unsigned long long));
@@ -355,6 +388,8 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   Q.ls = d->scratch + 12 * n;
   Q.mtau = d->scratch + 13 * n;
   Q.sgsF = P.turb ? d->scratch + nsgs * n : nullptr;
+  Q.lsfProf = P.lsfSub ? (float*)d->lsfMem : nullptr;
+  Q.lsfPart = P.lsfSub ? (double*)((char*)d->lsfMem + lsfProfBytes) : nullptr;
   float* s = d->surf;
   Q.cd = s; Q.ch = s + n2; Q.cq = s + 2 * n2; Q.fricVel = s + 3 * n2; Q.htFlux = s + 4 * n2; Q.tskin = s + 5 * n2;
   Q.invOblen = s + 6 * n2; Q.z0m = s + 7 * n2; Q.z0t = s + 8 * n2; Q.qFlux = s + 9 * n2; Q.qskin = s + 10 * n2;
@@ -717,12 +752,24 @@ static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, c
   }
 }
 
+// Slab means of the large-scale subsidence terms; the kernels return at once unless the device
+// clock says the step takes them (or `force`). Returns the number of kernels launched.
+static int launch_slab_means(const fe_domain* d, cudaStream_t s, const float* cur, const float* halo, bool force) {
+  const Phys& P = d->P;
+  fe::k_slab_partial<<<d->lsfBlocks, std::min(256, (P.nzh + 31) / 32 * 32), 0, s>>>(P, d->Q, cur, halo, force ? 1 : 0);
+  fe::k_slab_final<<<(5 * P.nzh + 127) / 128, 128, 0, s>>>(P, d->Q, d->lsfBlocks, force ? 1 : 0);
+  return 2;
+}
+
 // Enqueue one RK3 step on stream s (no host synchronisation; graph-capturable).
 static void enqueue_step(fe_domain* d, cudaStream_t s) {
   const Phys& P = d->P;
   const Ptrs& Q = d->Q;
   float *A = d->st[0], *B = d->st[1], *C = d->st[2];
   const bool physPrep = (P.turb || P.surf > 0);
+  // slab means of the subsidence terms at the start of a forcing step (phi^n in A; C still holds
+  // the previous step's phi** with its boundary images, the reference's halo values at this point)
+  if (P.lsfSub) d->launches += launch_slab_means(d, s, A, C, false);
   if (physPrep && stage_has_physics(d, 0)) d->launches += launch_physics(d, s, A, 0);
   launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
   if (physPrep && stage_has_physics(d, 1)) d->launches += launch_physics(d, s, B, 1);
@@ -756,7 +803,7 @@ static int build_graph(fe_domain* d) {
 
 static int launches_per_step(const fe_domain* d) {
   const Phys& P = d->P;
-  int l = 4 + (split_last_stage(d) ? 1 : 0);
+  int l = 4 + (split_last_stage(d) ? 1 : 0) + (P.lsfSub ? 2 : 0);
   if (P.turb || P.surf > 0) {
     const int phys = 2 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) + ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
     l += (P.oneRK ? 1 : 3) * phys;
@@ -847,6 +894,8 @@ extern "C" int fe_build_frhs(fe_domain* d, int stage) {
     if (rc) return rc;
   }
   float* A = d->st[0];
+  // the last stage's large-scale forcing on a forcing step uses the slab means of this state
+  if (stage == 2 && P.lsfSub) d->launches += launch_slab_means(d, d->stream, A, A, false);
   if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
     d->launches += launch_physics(d, d->stream, A, stage);
     CU(cudaGetLastError());

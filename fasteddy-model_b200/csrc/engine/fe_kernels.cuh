@@ -11,6 +11,7 @@
 //                 writes the tendency only)
 //   k_clock       advance the device simulation clock after the last stage
 //   k_nonfinite, k_means   device reductions (NaN/Inf count, FP64 domain means)
+//   k_slab_partial, k_slab_final   FP64 slab means of the large-scale subsidence terms
 #pragma once
 #include "fe_device.cuh"
 #include "fe_sgs.cuh"
@@ -809,6 +810,8 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
     }
   }
 
+  // large-scale forcing in the last stage (cuda_hydroCoreDevice.cu:401-406)
+  if (STAGE == 2 && lsf_step(P, *Q.clockIt)) lsf_tend(P, Q, c, k, Q.zPos[c], rho[c], F1, F2, F4, Fq0);
   // explicit filter of rho w, every stage, after all other terms (cuda_hydroCoreDevice.cu:414-416)
   if (P.filt)
     F3 = __fadd_rn(F3, filter6_tend(mw[c - 3], mw[c - 2], mw[c - 1], mw[c], mw[c + 1], mw[c + 2], mw[c + 3], P.filtCoef));
@@ -886,6 +889,48 @@ __global__ void k_nonfinite(Phys P, const float* __restrict__ st, unsigned long 
   }
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, (unsigned long long)cnt);
+}
+
+// Slab means for the large-scale subsidence terms (cuda_largeScaleForcingsDevice.cu:96-138 with
+// fecuda_PlugIns.cu:25-45): the mean over every column of the halo-inclusive plane (weight
+// 1/(nxh nyh)) of rho, rho u, rho v, rho theta and rho q_v at every level. The reference's RK
+// commit writes interior cells only, so when it takes the means at the start of a step its halo
+// cells still hold the boundary values of the previous step's last-stage input phi**: interior
+// cells are read from `cur` (phi^n) and halo cells from `halo` (the buffer holding phi** with its
+// boundary images). Sums are FP64: each block accumulates its columns (thread = level) into
+// lsfPart[block][field][level]; k_slab_final adds the blocks in a fixed order.
+__global__ void k_slab_partial(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ halo,
+                               int force) {
+  if (!force && !lsf_means_step(P, *Q.clockIt)) return;
+  const long long cols = (long long)P.nxh * P.nyh;
+  const long long qv = (long long)(5 + P.ntke) * P.n;
+  for (int k = threadIdx.x; k < P.nzh; k += blockDim.x) {
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const bool kin = k >= P.kMin && k < P.kMax;
+    for (long long col = blockIdx.x; col < cols; col += gridDim.x) {
+      const int i = (int)(col / P.nyh), j = (int)(col % P.nyh);
+      const bool in = kin && i >= P.iMin && i < P.iMax && j >= P.jMin && j < P.jMax;
+      const float* src = in ? cur : halo;
+      const long long c = col * P.nzh + k;
+      acc[0] += (double)src[c];
+      acc[1] += (double)src[P.n + c];
+      acc[2] += (double)src[2 * P.n + c];
+      acc[3] += (double)src[4 * P.n + c];
+      if (P.moist) acc[4] += (double)src[qv + c];
+    }
+    double* out = Q.lsfPart + (long long)blockIdx.x * 5 * P.nzh;
+#pragma unroll
+    for (int f = 0; f < 5; f++) out[f * P.nzh + k] = acc[f];
+  }
+}
+
+__global__ void k_slab_final(Phys P, Ptrs Q, int nblocks, int force) {
+  if (!force && !lsf_means_step(P, *Q.clockIt)) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 5 * P.nzh) return;
+  double sum = 0.0;
+  for (int b = 0; b < nblocks; b++) sum += Q.lsfPart[(long long)b * 5 * P.nzh + t];
+  Q.lsfProf[t] = (float)(sum / ((double)P.nxh * (double)P.nyh));
 }
 
 // FP64 sums of the interior fields: warp shuffle, then one atomic per warp and field.

@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   const bool mpNow = phys && nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
   if ((MP == 0 && mpNow) || (MP == 1 && !mpNow)) return;  // the other half of the pair runs this step
   const bool mpStep = MP == 0 ? false : mpNow;
+  const bool lsfNow = STAGE == 2 && lsf_step(P, *Q.clockIt);
   using T = MarchTile<TJ>;
   constexpr int PK = T::PK, PLANE = T::PLANE;
   extern __shared__ __align__(16) float sm[];
@@ -648,6 +649,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float Td2 = thd * powf(prd2 / P.p0, P.R_cp);
       F[4] = F[4] + ((thd * P.L_v) / (Td2 * P.cp_gas)) * fc;
     }
+    // large-scale forcing in the last stage (cuda_hydroCoreDevice.cu:401-406)
+    if (lsfNow && active) lsf_tend(P, Q, c, k, Q.zPos[c], r0, F[1], F[2], F[4], F[SL_QV]);
     // explicit filter of rho w, every stage, after all other terms (cuda_hydroCoreDevice.cu:414-416)
     if (P.filt) F[3] = __fadd_rn(F[3], fw);
 

@@ -61,6 +61,11 @@ int surflayer_idealsine;
 float surflayer_ideal_ts, surflayer_ideal_te, surflayer_ideal_amp;
 float surflayer_ideal_qts, surflayer_ideal_qte, surflayer_ideal_qamp;
 int lsfSelector;
+int lsf_horMnSubTerms;
+float lsf_freq;
+float lsf_w_surf, lsf_w_lev1, lsf_w_lev2, lsf_w_zlev1, lsf_w_zlev2;
+float lsf_th_surf, lsf_th_lev1, lsf_th_lev2, lsf_th_zlev1, lsf_th_zlev2;
+float lsf_qv_surf, lsf_qv_lev1, lsf_qv_lev2, lsf_qv_zlev1, lsf_qv_zlev2;
 int moistureSelector, moistureNvars, moistureAdvSelectorQv;
 float moistureAdvSelectorQv_b;
 int moistureSGSturb, moistureCond;
@@ -212,6 +217,31 @@ static int query_all(void) {
   Q(rc, fe_params_query_int("surflayer_stab", &surflayer_stab, 0, 1, FE_PARAM_OPTIONAL));
   lsfSelector = 0;
   Q(rc, fe_params_query_int("lsfSelector", &lsfSelector, 0, 1, FE_PARAM_MANDATORY));
+  /* large-scale forcing: defaults, then the keys read under lsfSelector > 0 (hydro_core.c:267-311) */
+  lsf_w_surf = lsf_w_lev1 = lsf_w_lev2 = 0.0f; lsf_w_zlev1 = 100.0f; lsf_w_zlev2 = 200.0f;
+  lsf_th_surf = lsf_th_lev1 = lsf_th_lev2 = 0.0f; lsf_th_zlev1 = 100.0f; lsf_th_zlev2 = 200.0f;
+  lsf_qv_surf = lsf_qv_lev1 = lsf_qv_lev2 = 0.0f; lsf_qv_zlev1 = 100.0f; lsf_qv_zlev2 = 200.0f;
+  lsf_horMnSubTerms = 0;
+  lsf_freq = 1.0f;
+  if (lsfSelector > 0) {
+    Q(rc, fe_params_query_float("lsf_w_surf", &lsf_w_surf, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_w_lev1", &lsf_w_lev1, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_w_lev2", &lsf_w_lev2, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_w_zlev1", &lsf_w_zlev1, 0.0f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_w_zlev2", &lsf_w_zlev2, 0.0f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_th_surf", &lsf_th_surf, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_th_lev1", &lsf_th_lev1, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_th_lev2", &lsf_th_lev2, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_th_zlev1", &lsf_th_zlev1, 0.0f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_th_zlev2", &lsf_th_zlev2, 0.0f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_qv_surf", &lsf_qv_surf, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_qv_lev1", &lsf_qv_lev1, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_qv_lev2", &lsf_qv_lev2, -1e+4f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_qv_zlev1", &lsf_qv_zlev1, 0.0f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_qv_zlev2", &lsf_qv_zlev2, 0.0f, 1e+4f, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_int("lsf_horMnSubTerms", &lsf_horMnSubTerms, 0, 1, FE_PARAM_MANDATORY));
+    Q(rc, fe_params_query_float("lsf_freq", &lsf_freq, 1e-3f, 1e+3f, FE_PARAM_MANDATORY));
+  }
   moistureSelector = 0;
   Q(rc, fe_params_query_int("moistureSelector", &moistureSelector, 0, 1, FE_PARAM_MANDATORY));
   moistureNvars = 0; moistureAdvSelectorQv = 0; moistureAdvSelectorQv_b = 0.0f;

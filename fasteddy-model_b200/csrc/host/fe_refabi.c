@@ -59,6 +59,13 @@ static void fill_config(fe_config *c) {
   c->advectionSelector = advectionSelector; c->b_hyb = b_hyb;
   c->diffusionSelector = diffusionSelector; c->filterSelector = filterSelector; c->lsfSelector = lsfSelector;
   c->filter_6th_coeff = filter_6th_coeff;
+  c->lsf_horMnSubTerms = lsf_horMnSubTerms; c->lsf_freq = lsf_freq;
+  c->lsf_w_surf = lsf_w_surf; c->lsf_w_lev1 = lsf_w_lev1; c->lsf_w_lev2 = lsf_w_lev2;
+  c->lsf_w_zlev1 = lsf_w_zlev1; c->lsf_w_zlev2 = lsf_w_zlev2;
+  c->lsf_th_surf = lsf_th_surf; c->lsf_th_lev1 = lsf_th_lev1; c->lsf_th_lev2 = lsf_th_lev2;
+  c->lsf_th_zlev1 = lsf_th_zlev1; c->lsf_th_zlev2 = lsf_th_zlev2;
+  c->lsf_qv_surf = lsf_qv_surf; c->lsf_qv_lev1 = lsf_qv_lev1; c->lsf_qv_lev2 = lsf_qv_lev2;
+  c->lsf_qv_zlev1 = lsf_qv_zlev1; c->lsf_qv_zlev2 = lsf_qv_zlev2;
   c->surflayerSelector = surflayerSelector;
   c->surflayer_z0 = surflayer_z0; c->surflayer_z0t = surflayer_z0t; c->surflayer_wth = surflayer_wth;
   c->surflayer_tr = surflayer_tr; c->surflayer_wq = surflayer_wq; c->surflayer_qr = surflayer_qr;

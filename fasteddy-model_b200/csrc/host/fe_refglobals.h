@@ -51,6 +51,11 @@ extern int surflayer_idealsine;
 extern float surflayer_ideal_ts, surflayer_ideal_te, surflayer_ideal_amp;
 extern float surflayer_ideal_qts, surflayer_ideal_qte, surflayer_ideal_qamp;
 extern int lsfSelector;
+extern int lsf_horMnSubTerms;
+extern float lsf_freq;
+extern float lsf_w_surf, lsf_w_lev1, lsf_w_lev2, lsf_w_zlev1, lsf_w_zlev2;
+extern float lsf_th_surf, lsf_th_lev1, lsf_th_lev2, lsf_th_zlev1, lsf_th_zlev2;
+extern float lsf_qv_surf, lsf_qv_lev1, lsf_qv_lev2, lsf_qv_zlev1, lsf_qv_zlev2;
 extern int moistureSelector, moistureNvars, moistureAdvSelectorQv;
 extern float moistureAdvSelectorQv_b;
 extern int moistureSGSturb, moistureCond;

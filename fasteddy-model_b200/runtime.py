@@ -65,6 +65,8 @@ class FeConfig(ctypes.Structure):
         ("cv_gas", ctypes.c_float), ("accel_g", ctypes.c_float), ("R_cp", ctypes.c_float), ("cp_R", ctypes.c_float),
         ("cp_cv", ctypes.c_float), ("refPressure", ctypes.c_float), ("kappa", ctypes.c_float), ("L_v", ctypes.c_float),
         ("filter_6th_coeff", ctypes.c_float),
+        ("lsf_horMnSubTerms", ctypes.c_int), ("lsf_freq", ctypes.c_float),
+        *[(f"lsf_{v}_{p}", ctypes.c_float) for v in ("w", "th", "qv") for p in ("surf", "lev1", "lev2", "zlev1", "zlev2")],
     ]
 
     def as_dict(self) -> dict:

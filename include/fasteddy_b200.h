@@ -98,7 +98,7 @@ typedef struct fe_config {
   float TKEAdvSelector_b_hyb, c_s, c_k;
   int advectionSelector;              /* 0 upwind, 1 QUICK, 2 HYB34, 3 HYB56, 4 WENO3, 5 WENO5, 6 centred 2nd */
   float b_hyb;
-  int diffusionSelector, filterSelector, lsfSelector;   /* diffusion and lsf must be 0; filter 0 or 1 */
+  int diffusionSelector, filterSelector, lsfSelector;   /* diffusion must be 0; filter and lsf 0 or 1 */
   int surflayerSelector;              /* 0, 1 (heat flux) or 2 (skin temperature) */
   float surflayer_z0, surflayer_z0t, surflayer_wth, surflayer_tr, surflayer_wq, surflayer_qr;
   int surflayer_qskin_input, surflayer_stab, surflayer_idealsine;
@@ -118,6 +118,13 @@ typedef struct fe_config {
   float temp_grnd, pres_grnd;
   float R_gas, R_vapor, Rv_Rg, cp_gas, cv_gas, accel_g, R_cp, cp_R, cp_cv, refPressure, kappa, L_v;
   float filter_6th_coeff;             /* 6th-order vertical filter factor on rho w (filterSelector = 1) */
+  /* large-scale forcing (lsfSelector = 1): piecewise-linear profiles in z (surface value, values
+   * at zlev1 and zlev2, constant above), per hour; w drives the subsidence terms */
+  int lsf_horMnSubTerms;              /* 1: subsidence of the slab-mean u, v, theta, q_v */
+  float lsf_freq;                     /* seconds between applications */
+  float lsf_w_surf, lsf_w_lev1, lsf_w_lev2, lsf_w_zlev1, lsf_w_zlev2;
+  float lsf_th_surf, lsf_th_lev1, lsf_th_lev2, lsf_th_zlev1, lsf_th_zlev2;
+  float lsf_qv_surf, lsf_qv_lev1, lsf_qv_lev2, lsf_qv_zlev1, lsf_qv_zlev2;
 } fe_config;
 
 /* Reference defaults (hydro_core.c:197-395 defaults, hydro_core.c:941-952 constants). */

@@ -35,6 +35,9 @@ struct ora_domain {
   double *tau[9], *Km, *ls, *dedx[3], *mtau[6], *fcond;
   /* surface */
   double *cd, *ch, *cq, *fricVel, *htFlux, *tskin, *invOblen, *z0m, *z0t, *qFlux, *qskin;
+  /* large-scale forcing: slab means of rho, rho u, rho v, rho theta, rho q_v per level */
+  double *lsfProf;
+  int lsfN;
 };
 
 #define IX(o, i, j, k) (((size_t)(i) * (size_t)(o)->nyh + (size_t)(j)) * (size_t)(o)->nzh + (size_t)(k))
@@ -73,7 +76,10 @@ int ora_create(const fe_config *cfg, ora_domain **out) {
   o->cd = dalloc(o->n2); o->ch = dalloc(o->n2); o->cq = dalloc(o->n2); o->fricVel = dalloc(o->n2);
   o->htFlux = dalloc(o->n2); o->tskin = dalloc(o->n2); o->invOblen = dalloc(o->n2); o->z0m = dalloc(o->n2);
   o->z0t = dalloc(o->n2); o->qFlux = dalloc(o->n2); o->qskin = dalloc(o->n2);
-  if (!o->fcond || !o->qskin) { ora_destroy(o); return FE_ERR_NOMEM; }
+  o->lsfProf = dalloc((size_t)5 * o->nzh);
+  o->lsfN = cfg->lsfSelector > 0 ? (int)lroundf(cfg->lsf_freq / cfg->dt) : 1;
+  if (o->lsfN < 1) o->lsfN = 1;
+  if (!o->fcond || !o->qskin || !o->lsfProf) { ora_destroy(o); return FE_ERR_NOMEM; }
   *out = o;
   return FE_OK;
 }
@@ -94,6 +100,7 @@ void ora_destroy(ora_domain *o) {
   free(o->fcond);
   free(o->cd); free(o->ch); free(o->cq); free(o->fricVel); free(o->htFlux); free(o->tskin); free(o->invOblen);
   free(o->z0m); free(o->z0t); free(o->qFlux); free(o->qskin);
+  free(o->lsfProf);
   free(o);
 }
 
@@ -449,7 +456,53 @@ static void surface_most(ora_domain *o, int i, int j) {
 }
 
 /* ------------------------------------------------------------------ one tendency */
-int ora_build_frhs(ora_domain *o, int stage) {
+/* ------------------------------------------------------------------ large-scale forcing */
+/* Steps that take the slab means and apply the forcing (cuda_timeIntDevice.cu:125-127,
+ * cuda_hydroCoreDevice.cu:401-406). */
+static int lsf_means_step(const ora_domain *o) {
+  return o->c.lsfSelector > 0 && o->c.lsf_horMnSubTerms == 1 && o->simTime_it > o->c.simTime_itRestart &&
+         o->simTime_it % o->lsfN == 0;
+}
+static int lsf_force_step(const ora_domain *o) {
+  int d = o->simTime_it - o->c.simTime_itRestart;
+  return o->c.lsfSelector > 0 && d > 0 && d >= o->lsfN && o->simTime_it % o->lsfN == 0;
+}
+
+/* Slab means over every column of the halo-inclusive plane (cuda_largeScaleForcingsDevice.cu:96-138,
+ * fecuda_PlugIns.cu:25-45) of the arrays as they are: at the start of a step their halo cells
+ * hold the boundary values of the previous step's last-stage input, as the reference's do. */
+static void lsf_slab_means(ora_domain *o) {
+  const double *src[5] = {o->fld[0], o->fld[1], o->fld[2], o->fld[4], o->nmoist > 0 ? o->moist[0] : NULL};
+  double inv = 1.0 / ((double)o->nxh * (double)o->nyh);
+  int f, i, j, k;
+  for (f = 0; f < 5; f++)
+    for (k = 0; k < o->nzh; k++) {
+      double sum = 0.0;
+      if (src[f])
+        for (i = 0; i < o->nxh; i++)
+          for (j = 0; j < o->nyh; j++) sum += src[f][IX(o, i, j, k)];
+      o->lsfProf[f * o->nzh + k] = sum * inv;
+    }
+}
+
+/* Piecewise-linear forcing profile (surface, lev1 at zlev1, lev2 at zlev2, constant above)
+ * times rho, per second over the application interval (cuda_largeScaleForcingsDevice.cu:177-230). */
+static double lsf_profile(double surf, double lev1, double lev2, double z1, double z2, double z, double rho,
+                          int nsteps) {
+  double f;
+  if (z <= z1) f = (surf + (lev1 - surf) / z1 * z) * rho;
+  else if (z <= z2) f = (lev1 + (lev2 - lev1) / (z2 - z1) * (z - z1)) * rho;
+  else f = lev2 * rho;
+  return f * nsteps / 3600.0;
+}
+
+static int build_frhs(ora_domain *o, int stage, int fresh_means);
+
+int ora_build_frhs(ora_domain *o, int stage) { return build_frhs(o, stage, 1); }
+
+/* fresh_means: a tendency evaluated on its own takes the slab means of its input state (after
+ * its boundary values are set); inside a step they were taken at the step's start. */
+static int build_frhs(ora_domain *o, int stage, int fresh_means) {
   const fe_config *C = &o->c;
   int i, j, k, f;
   int iMin = o->iMin, iMax = o->iMax, jMin = o->jMin, jMax = o->jMax, kMin = o->kMin, kMax = o->kMax;
@@ -836,7 +889,34 @@ int ora_build_frhs(ora_domain *o, int stage) {
     }
   }
 
-  /* 7. explicit filter of rho w, every stage (cuda_hydroCoreDevice.cu:414-416) */
+  /* 7. large-scale forcing in the last stage (cuda_largeScaleForcingsDevice.cu:155-252); the
+   * subsidence terms multiply the rho-weighted w_ls by rho once more, as the reference does */
+  if (stage == 2 && lsf_force_step(o)) {
+    double *P = o->lsfProf;
+    int nz = o->nzh, ns = o->lsfN;
+    if (fresh_means && C->lsf_horMnSubTerms == 1) lsf_slab_means(o);
+    for (i = iMin; i < iMax; i++)
+      for (j = jMin; j < jMax; j++)
+        for (k = kMin; k < kMax; k++) {
+          size_t c = IX(o, i, j, k);
+          double z = o->zPos[c], r = rho[c];
+          o->F[4][c] += lsf_profile(C->lsf_th_surf, C->lsf_th_lev1, C->lsf_th_lev2, C->lsf_th_zlev1, C->lsf_th_zlev2, z, r, ns);
+          if (moistOn)
+            o->Fmoist[0][c] += lsf_profile(C->lsf_qv_surf, C->lsf_qv_lev1, C->lsf_qv_lev2, C->lsf_qv_zlev1, C->lsf_qv_zlev2, z, r, ns);
+          if (C->lsf_horMnSubTerms == 1) {
+            double fw = lsf_profile(C->lsf_w_surf, C->lsf_w_lev1, C->lsf_w_lev2, C->lsf_w_zlev1, C->lsf_w_zlev2, z, r, ns);
+            double dz = o->zPos[c + 1] - o->zPos[c - 1];
+#define DMEAN(q) (P[(q) * nz + k + 1] / P[k + 1] - P[(q) * nz + k - 1] / P[k - 1])
+            o->F[1][c] -= fw * r * DMEAN(1) / dz;
+            o->F[2][c] -= fw * r * DMEAN(2) / dz;
+            o->F[4][c] -= fw * r * DMEAN(3) / dz;
+            if (moistOn) o->Fmoist[0][c] -= fw * r * DMEAN(4) / dz;
+#undef DMEAN
+          }
+        }
+  }
+
+  /* 8. explicit filter of rho w, every stage (cuda_hydroCoreDevice.cu:414-416) */
   if (C->filterSelector > 0)
     for (i = iMin; i < iMax; i++)
       for (j = jMin; j < jMax; j++)
@@ -869,7 +949,7 @@ static void commit(ora_domain *o, int stage) {
 }
 
 int ora_rk_stage(ora_domain *o, int stage) {
-  int rc = ora_build_frhs(o, stage);
+  int rc = build_frhs(o, stage, 0);
   if (rc != FE_OK) return rc;
   commit(o, stage);
   return FE_OK;
@@ -878,6 +958,7 @@ int ora_rk_stage(ora_domain *o, int stage) {
 int ora_step(ora_domain *o, int nsteps) {
   int s, st;
   for (s = 0; s < nsteps; s++) {
+    if (lsf_means_step(o)) lsf_slab_means(o);
     for (st = 0; st < 3; st++) ora_rk_stage(o, st);
     o->simTime = (double)(float)((float)o->simTime + (float)o->c.dt);
     o->simTime_it += 1;

@@ -22,6 +22,10 @@ sys.path.insert(0, ROOT)
 fe = importlib.import_module("fasteddy-model_b200")
 from oracle import refrun  # noqa: E402
 
+LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-40.0, lsf_w_lev2=0.0,
+           lsf_w_zlev1=50.0, lsf_w_zlev2=100.0, lsf_th_surf=-2.0, lsf_th_lev1=-1.0, lsf_th_lev2=0.5,
+           lsf_th_zlev1=40.0, lsf_th_zlev2=90.0, lsf_qv_surf=-0.5, lsf_qv_lev1=-0.5, lsf_qv_lev2=0.0,
+           lsf_qv_zlev1=30.0, lsf_qv_zlev2=70.0)
 MOIST_HILL = dict(hill_halfwidth=60.0, hill_height=15.0, qv=(24.0, 8.0, 300.0))
 CASES = {
     "cbl_dry": dict(case="cbl_dry", nx=16, ny=12, nz=12, kw={}),
@@ -43,6 +47,13 @@ CASES = {
     "dry_upwind_filter": dict(case="cbl_dry", nx=16, ny=12, nz=12,
                               kw=dict(params=dict(advectionSelector=0, TKEAdvSelector=1, filterSelector=1,
                                                   filter_6th_coeff=0.12))),
+    # large-scale forcing every 2 steps (BOMEX-type profiles scaled to the 120 m column); the
+    # reference's slab-mean reduction tiles the halo-inclusive plane with 2 x 8 blocks, so the
+    # plane is 22 x 16 columns here (ny = 10), and its subsidence terms need moisture on
+    "moist_lsf": dict(case="cbl_moist_hill", nx=16, ny=10, nz=12,
+                      kw=dict(MOIST_HILL, params=dict(LSF, filterSelector=1))),
+    "dry_lsf_no_subsidence": dict(case="cbl_dry", nx=16, ny=10, nz=12,
+                                  kw=dict(params=dict(LSF, lsf_horMnSubTerms=0))),
 }
 
 

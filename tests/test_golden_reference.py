@@ -32,7 +32,7 @@ def _load(name):
 
 
 GOLDEN_CASES = ["cbl_dry", "moist_hill", "dry_quick_filter", "moist_weno3_filter", "dry_hyb34", "moist_centred_filter",
-                "dry_upwind_filter"]
+                "dry_upwind_filter", "moist_lsf", "dry_lsf_no_subsidence"]
 
 TOL = {1: [1e-6, 1e-5, 2e-3, 2e-3, 1e-6], 10: [2e-6, 2e-5, 5e-3, 5e-3, 2e-6]}
 

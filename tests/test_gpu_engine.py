@@ -456,3 +456,58 @@ def test_filter_changes_only_rho_w(fe):
     assert np.abs(dr).max() > 0
     assert rel_l2(dg, dr) < 1e-3
     host.cleanup()
+
+
+# Large-scale forcing as in the BOMEX tutorial (theta and q_v forcing, subsidence of the slab-mean
+# u, v, theta, q_v), heights scaled to the 160 m test column, applied every 2 steps.
+LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-40.0, lsf_w_lev2=0.0,
+           lsf_w_zlev1=60.0, lsf_w_zlev2=120.0, lsf_th_surf=-2.0, lsf_th_lev1=-1.0, lsf_th_lev2=0.5,
+           lsf_th_zlev1=50.0, lsf_th_zlev2=110.0, lsf_qv_surf=-0.5, lsf_qv_lev1=-0.5, lsf_qv_lev2=0.0,
+           lsf_qv_zlev1=40.0, lsf_qv_zlev2=90.0)
+
+
+@pytest.mark.parametrize("kind", ["march", "cell"])
+def test_large_scale_forcing_matches_oracle(fe, kind):
+    """The forcing's own tendency (last stage on a forcing step, with minus without) from the
+    state after 8 steps, and the state after 6 forced steps (forcing at steps 2 and 4; the slab
+    means taken at their start from phi^n inside and the previous phi** in the halo cells)."""
+    c = CASES["moist_hill"]
+    host = fe.cases.setup_host(c["case"], c["nx"], c["ny"], c["nz"], params=LSF, **c["kw"])
+    inp, cfg = host.inputs(), host.config()
+    d = fe.Domain(cfg)
+    d.set_inputs(inp)
+    d.advance(8)
+    st = d.get_state()
+    d.close()
+    moved = dict(inp, hydroFlds=st["hydroFlds"], sgstke=st["sgstke"], moist=st["moist"])
+    diff = {}
+    for on in (0, 1):
+        cfg.lsfSelector = on
+        dom = fe.Domain(cfg)
+        dom.set_inputs(moved, 0.2, 8)
+        dom.set_stage_kernel(kind, 8 if kind == "march" else 0, 0)
+        o = Oracle(cfg)
+        o.set_inputs(moved, 0.2, 8)
+        diff[on] = (dom.build_frhs(2), o.build_frhs(2))
+        dom.close()
+    for key, fields in (("hydroFrhs", (1, 2, 4)), ("moistFrhs", (0,))):
+        for f in fields:
+            dg = interior(diff[1][0][key][f]).astype(np.float64) - interior(diff[0][0][key][f])
+            dr = interior(diff[1][1][key][f]) - interior(diff[0][1][key][f])
+            assert np.abs(dr).max() > 0, (key, f)
+            assert rel_l2(dg, dr) < 1e-3, (kind, key, f, rel_l2(dg, dr))
+    cfg.lsfSelector = 1
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    dom.set_stage_kernel(kind, 8 if kind == "march" else 0, 0)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    dom.advance(6)
+    o.step(6)
+    g, r = dom.get_state(), o.get_state()
+    for f in range(5):
+        assert rel_l2(interior(g["hydroFlds"][f]), interior(r["hydroFlds"][f])) < STATE_TOL[f], f
+    assert rel_l2(interior(g["moist"][0]), interior(r["moist"][0])) < 1e-6
+    assert dom.nonfinite() == 0
+    dom.close()
+    host.cleanup()

@@ -204,3 +204,81 @@ def test_rk3_stage_weights(fe):
     dt = float(np.float32(0.025))  # dt is a float parameter (time_integration.h:26)
     np.testing.assert_allclose(interior(phi1), interior(phi0 + dt / 3.0 * F0), rtol=0, atol=1e-12)
     host.cleanup()
+
+
+LSF = dict(lsfSelector=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-40.0, lsf_w_lev2=0.0, lsf_w_zlev1=60.0,
+           lsf_w_zlev2=120.0, lsf_th_surf=-2.0, lsf_th_lev1=-1.0, lsf_th_lev2=0.5, lsf_th_zlev1=50.0,
+           lsf_th_zlev2=110.0, lsf_qv_surf=-0.5, lsf_qv_lev1=-0.5, lsf_qv_lev2=0.0, lsf_qv_zlev1=40.0, lsf_qv_zlev2=90.0)
+
+
+def _lsf_profile(p, z):
+    s_, l1, l2, z1, z2 = [float(np.float32(x)) for x in p]  # the parameters are floats
+    return np.where(z <= z1, s_ + (l1 - s_) / z1 * z, np.where(z <= z2, l1 + (l2 - l1) / (z2 - z1) * (z - z1), l2))
+
+
+def _lsf_tendency_difference(fe, params, state_edit=None):
+    """Last-stage tendency with the forcing minus without it, at a forcing step (it = 2 with
+    lsf_freq = 2 dt), from the same state."""
+    host = fe.Host()
+    host.load_params_text(fe.cases.param_text("cbl_moist_hill", 10, 8, 16, params=params))
+    host.init(3)
+    host.set_qv_profile(14.0, 4.0, 1500.0)
+    inp = host.inputs()
+    cfg = host.config()
+    out = []
+    for on in (0, 1):
+        cfg.lsfSelector = on
+        o = Oracle(cfg)
+        o.set_inputs(inp, 0.05, 2)
+        if state_edit is not None:
+            state_edit(o, inp)
+        r = o.build_frhs(2)
+        out.append((r["hydroFrhs"], r["moistFrhs"]))
+    host.cleanup()
+    return inp, (out[1][0] - out[0][0]), (out[1][1] - out[0][1])
+
+
+def test_lsf_forcing_follows_the_piecewise_linear_profiles(fe):
+    """theta and q_v forcing (cuda_largeScaleForcingsDevice.cu:177-230): rate(z) rho n / 3600
+    with n = lsf_freq/dt steps per application; no subsidence terms without lsf_horMnSubTerms."""
+    inp, dH, dM = _lsf_tendency_difference(fe, dict(LSF, lsf_horMnSubTerms=0))
+    z = inp["zPos"].astype(np.float64)
+    rho = inp["hydroFlds"][0].astype(np.float64)
+    th = _lsf_profile((-2.0, -1.0, 0.5, 50.0, 110.0), z) * rho * 2 / 3600.0
+    qv = _lsf_profile((-0.5, -0.5, 0.0, 40.0, 90.0), z) * rho * 2 / 3600.0
+    np.testing.assert_allclose(interior(dH[4]), interior(th), rtol=1e-9, atol=1e-15)
+    np.testing.assert_allclose(interior(dM[0]), interior(qv), rtol=1e-9, atol=1e-15)
+    for f in (0, 1, 2, 3):
+        assert np.abs(interior(dH[f])).max() == 0.0
+
+
+def test_lsf_subsidence_of_a_linear_wind_profile(fe):
+    """With a horizontally uniform state the slab means are the profiles themselves, so the
+    subsidence term of u = a z on the uniform grid is -w_ls rho rho a (the reference multiplies
+    the rho-weighted w_ls by rho once more) on levels whose k+-1 neighbours are interior."""
+    a = 0.02
+
+    def edit(o, inp):
+        H = inp["hydroFlds"].astype(np.float64).copy()
+        rho = H[0].mean(axis=(0, 1), keepdims=True) * np.ones_like(H[0])
+        H[0] = rho
+        H[1] = rho * a * inp["zPos"].astype(np.float64)
+        H[2] = 0.0
+        H[3] = 0.0
+        H[4] = rho * 300.0
+        M = inp["moist"].astype(np.float64).copy()
+        M[0] = rho * 10.0
+        M[1] = 0.0
+        o.lib.ora_set_state_f64(o.h, *(np.ascontiguousarray(x).ctypes.data_as(o.lib.ora_set_state_f64.argtypes[1])
+                                       for x in (H, inp["sgstke"].astype(np.float64), M)))
+
+    inp, dH, dM = _lsf_tendency_difference(fe, dict(LSF, lsf_horMnSubTerms=1), edit)
+    z = inp["zPos"].astype(np.float64)
+    rho = inp["hydroFlds"][0].astype(np.float64).mean(axis=(0, 1), keepdims=True) * np.ones_like(z)
+    fw = _lsf_profile((0.0, -40.0, 0.0, 60.0, 120.0), z) * rho * 2 / 3600.0
+    lv = slice(4, -4)
+    np.testing.assert_allclose(interior(dH[1])[..., lv], interior(-fw * rho * a)[..., lv], rtol=1e-7)
+    # v = 0, theta and q_v/rho uniform: only the large-scale forcing of theta and q_v remains
+    assert np.abs(interior(dH[2])).max() == 0.0
+    th = _lsf_profile((-2.0, -1.0, 0.5, 50.0, 110.0), z) * rho * 2 / 3600.0
+    np.testing.assert_allclose(interior(dH[4])[..., lv], interior(th)[..., lv], rtol=1e-7, atol=1e-12)

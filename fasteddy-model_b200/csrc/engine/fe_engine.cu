@@ -656,13 +656,13 @@ static int launch_physics(const fe_domain* d, cudaStream_t s, const float* st, i
     const dim3 g((P.Nz + 31) / 32, (P.Ny + 7) / 8, P.Nx), b(32, 8);
     const int nq = (P.nmoist > 0 && P.moistSGS > 0) ? std::min(P.nmoist, 2) : 0;
     if (P.tke) {
-      if (nq == 2) fe::k_sgs_tend<true, 2><<<g, b, 0, s>>>(P, d->Q, st);
-      else if (nq == 1) fe::k_sgs_tend<true, 1><<<g, b, 0, s>>>(P, d->Q, st);
-      else fe::k_sgs_tend<true, 0><<<g, b, 0, s>>>(P, d->Q, st);
+      if (nq == 2) fe::k_sgs_tend<true, 2><<<g, b, 0, s>>>(P, d->Q, st, stage);
+      else if (nq == 1) fe::k_sgs_tend<true, 1><<<g, b, 0, s>>>(P, d->Q, st, stage);
+      else fe::k_sgs_tend<true, 0><<<g, b, 0, s>>>(P, d->Q, st, stage);
     } else {
-      if (nq == 2) fe::k_sgs_tend<false, 2><<<g, b, 0, s>>>(P, d->Q, st);
-      else if (nq == 1) fe::k_sgs_tend<false, 1><<<g, b, 0, s>>>(P, d->Q, st);
-      else fe::k_sgs_tend<false, 0><<<g, b, 0, s>>>(P, d->Q, st);
+      if (nq == 2) fe::k_sgs_tend<false, 2><<<g, b, 0, s>>>(P, d->Q, st, stage);
+      else if (nq == 1) fe::k_sgs_tend<false, 1><<<g, b, 0, s>>>(P, d->Q, st, stage);
+      else fe::k_sgs_tend<false, 0><<<g, b, 0, s>>>(P, d->Q, st, stage);
     }
     l++;
   }

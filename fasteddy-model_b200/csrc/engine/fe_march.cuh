@@ -150,8 +150,13 @@ __device__ __forceinline__ const float* f_src(const Phys& P, const float* cur, c
 // tendency once. `st` is the stage's input state; the shear production's velocity gradients use
 // central differences of phi/rho at the six neighbours. TKE (prognostic TKE) and NQ (moisture
 // species with SGS fluxes) are compile-time so that every load of a cell issues as one batch.
+//
+// On a large-scale forcing step (last stage) the forcing's tendencies of rho u, rho v, rho theta
+// and rho q_v are folded into fields 0, 1, 3 and 5 (subtracted, as those fields are), so the march
+// kernel carries no forcing code of its own; with moisture but no moisture SGS fluxes, field 5
+// then holds only the forcing (zero on other steps).
 template <bool TKE, int NQ>
-__global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float* __restrict__ st) {
+__global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
   const int k = P.kMin + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = P.jMin + blockIdx.y * blockDim.y + threadIdx.y;
   const int i = P.iMin + blockIdx.z;
@@ -215,14 +220,19 @@ __global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float
     se = Se;
   }
 #undef TT
+  // large-scale forcing of the last stage (cuda_hydroCoreDevice.cu:401-406)
+  float lu = 0.0f, lv = 0.0f, lth = 0.0f, lqv = 0.0f;
+  if (stage == 2 && lsf_step(P, *Q.clockIt)) lsf_tend(P, Q, c, k, Q.zPos[c], st[c], lu, lv, lth, lqv);
   float* S = Q.sgsF + c;
-  S[0] = s0;
-  S[n] = s1;
+  S[0] = s0 - lu;
+  S[n] = s1 - lv;
   S[2 * n] = s2;
-  S[3 * n] = s3;
+  S[3 * n] = s3 - lth;
   if (TKE) S[4 * n] = se;
+  if (NQ > 0) S[5 * n] = sq[0] - lqv;
+  else if (P.lsf && P.moist) S[5 * n] = -lqv;
 #pragma unroll
-  for (int m = 0; m < NQ; m++) S[(5 + m) * n] = sq[m];
+  for (int m = 1; m < NQ; m++) S[(5 + m) * n] = sq[m];
 }
 
 // MP: the saturation adjustment of the last stage. -1 decides per step from the device clock;
@@ -241,7 +251,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   const bool mpNow = phys && nmoist > 1 && P.moist && P.moistCond > 0 && ((*Q.clockIt) % P.mpFreq == 0);
   if ((MP == 0 && mpNow) || (MP == 1 && !mpNow)) return;  // the other half of the pair runs this step
   const bool mpStep = MP == 0 ? false : mpNow;
-  const bool lsfNow = STAGE == 2 && lsf_step(P, *Q.clockIt);
+  // large-scale forcing inline only without the SGS kernel (which otherwise carries it)
+  const bool lsfNow = STAGE == 2 && FL == FL_ANY && !P.turb && lsf_step(P, *Q.clockIt);
   using T = MarchTile<TJ>;
   constexpr int PK = T::PK, PLANE = T::PLANE;
   extern __shared__ __align__(16) float sm[];
@@ -464,9 +475,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
 #pragma unroll
       for (int m = 0; m < 4; m++) sg[m] = Q.sgsF[m * n + c];
       if (tke) sg[4] = Q.sgsF[4 * n + c];
-      if (nmoist > 0 && P.moistSGS > 0) {
+      if (nmoist > 0 && (P.moistSGS > 0 || P.lsf)) {
         sg[5] = Q.sgsF[5 * n + c];
-        if (nmoist > 1) sg[6] = Q.sgsF[6 * n + c];
+        if (nmoist > 1 && P.moistSGS > 0) sg[6] = Q.sgsF[6 * n + c];
       }
     }
     // base state of the buoyancy, Rayleigh and Coriolis terms
@@ -605,9 +616,9 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       F[3] = F[3] - sg[2];
       F[4] = F[4] - sg[3];
       if (tke) F[SL_E] = F[SL_E] + sg[4];
-      if (nmoist > 0 && P.moistSGS > 0) {
+      if (nmoist > 0 && (P.moistSGS > 0 || P.lsf)) {
         F[SL_QV] = F[SL_QV] - sg[5];
-        if (nmoist > 1) F[SL_QL] = F[SL_QL] - sg[6];
+        if (nmoist > 1 && P.moistSGS > 0) F[SL_QL] = F[SL_QL] - sg[6];
       }
     }
 

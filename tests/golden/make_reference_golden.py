@@ -22,9 +22,11 @@ sys.path.insert(0, ROOT)
 fe = importlib.import_module("fasteddy-model_b200")
 from oracle import refrun  # noqa: E402
 
-LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-40.0, lsf_w_lev2=0.0,
-           lsf_w_zlev1=50.0, lsf_w_zlev2=100.0, lsf_th_surf=-2.0, lsf_th_lev1=-1.0, lsf_th_lev2=0.5,
-           lsf_th_zlev1=40.0, lsf_th_zlev2=90.0, lsf_qv_surf=-0.5, lsf_qv_lev1=-0.5, lsf_qv_lev2=0.0,
+# BOMEX-shaped large-scale forcing with rates ~50 times the tutorial's, so that 10 steps of it move
+# the state well beyond FP32 noise (the reference accepts rates up to 1e4 per hour)
+LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-2000.0, lsf_w_lev2=0.0,
+           lsf_w_zlev1=50.0, lsf_w_zlev2=100.0, lsf_th_surf=-100.0, lsf_th_lev1=-50.0, lsf_th_lev2=25.0,
+           lsf_th_zlev1=40.0, lsf_th_zlev2=90.0, lsf_qv_surf=-20.0, lsf_qv_lev1=-20.0, lsf_qv_lev2=0.0,
            lsf_qv_zlev1=30.0, lsf_qv_zlev2=70.0)
 MOIST_HILL = dict(hill_halfwidth=60.0, hill_height=15.0, qv=(24.0, 8.0, 300.0))
 CASES = {
@@ -53,7 +55,8 @@ CASES = {
     "moist_lsf": dict(case="cbl_moist_hill", nx=16, ny=10, nz=12,
                       kw=dict(MOIST_HILL, params=dict(LSF, filterSelector=1))),
     "dry_lsf_no_subsidence": dict(case="cbl_dry", nx=16, ny=10, nz=12,
-                                  kw=dict(params=dict(LSF, lsf_horMnSubTerms=0))),
+                                  kw=dict(params=dict(LSF, lsf_horMnSubTerms=0, lsf_th_surf=-1000.0,
+                                                      lsf_th_lev1=-500.0, lsf_th_lev2=250.0))),
 }
 
 

@@ -71,7 +71,9 @@ PLANTED = [("dry_quick_filter", "advectionSelector", 3), ("dry_quick_filter", "f
            ("moist_weno3_filter", "advectionSelector", 5), ("moist_weno3_filter", "moistureAdvSelectorQi", 2),
            ("dry_hyb34", "b_hyb", 0.0), ("dry_hyb34", "TKEAdvSelector", 3),
            ("moist_centred_filter", "moistureAdvSelectorQv", 3), ("moist_centred_filter", "filterSelector", 0),
-           ("dry_upwind_filter", "TKEAdvSelector", 3), ("dry_upwind_filter", "advectionSelector", 1)]
+           ("dry_upwind_filter", "TKEAdvSelector", 3), ("dry_upwind_filter", "advectionSelector", 1),
+           ("moist_lsf", "lsfSelector", 0), ("moist_lsf", "lsf_horMnSubTerms", 0), ("moist_lsf", "lsf_freq", 0.075),
+           ("dry_lsf_no_subsidence", "lsfSelector", 0), ("dry_lsf_no_subsidence", "lsf_freq", 0.075)]
 
 
 @pytest.mark.parametrize("name,key,value", PLANTED)

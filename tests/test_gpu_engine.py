@@ -353,7 +353,7 @@ def test_ensemble_of_uneven_domains_matches_members(fe):
 def test_unsupported_configuration_is_rejected(fe):
     host, inp, cfg = _setup(fe, "cbl_dry")
     for key, value, msg in (("advectionSelector", 7, "advectionSelector"), ("diffusionSelector", 1, "diffusion"),
-                            ("lsfSelector", 1, "large-scale"), ("filterSelector", 2, "filterSelector")):
+                            ("lsfSelector", 2, "lsfSelector"), ("filterSelector", 2, "filterSelector")):
         bad = type(cfg).from_buffer_copy(cfg)
         setattr(bad, key, value)
         with pytest.raises(fe.FeError, match=msg):
@@ -459,8 +459,10 @@ def test_filter_changes_only_rho_w(fe):
 
 
 # Large-scale forcing as in the BOMEX tutorial (theta and q_v forcing, subsidence of the slab-mean
-# u, v, theta, q_v), heights scaled to the 160 m test column, applied every 2 steps.
-LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-40.0, lsf_w_lev2=0.0,
+# u, v, theta, q_v), heights scaled to the 160 m test column, applied every 2 steps. The subsidence
+# rate is 200 times BOMEX's so that its term on rho u (otherwise ~1e-5 against O(1) tendencies)
+# is resolved by the difference of two FP32 tendencies.
+LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, lsf_w_lev1=-8000.0, lsf_w_lev2=0.0,
            lsf_w_zlev1=60.0, lsf_w_zlev2=120.0, lsf_th_surf=-2.0, lsf_th_lev1=-1.0, lsf_th_lev2=0.5,
            lsf_th_zlev1=50.0, lsf_th_zlev2=110.0, lsf_qv_surf=-0.5, lsf_qv_lev1=-0.5, lsf_qv_lev2=0.0,
            lsf_qv_zlev1=40.0, lsf_qv_zlev2=90.0)
@@ -470,7 +472,15 @@ LSF = dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=0.05, lsf_w_surf=0.0, ls
 def test_large_scale_forcing_matches_oracle(fe, kind):
     """The forcing's own tendency (last stage on a forcing step, with minus without) from the
     state after 8 steps, and the state after 6 forced steps (forcing at steps 2 and 4; the slab
-    means taken at their start from phi^n inside and the previous phi** in the halo cells)."""
+    means taken at their start from phi^n inside and the previous phi** in the halo cells).
+
+    The forcing is small against the O(1) tendencies it is added to, so the engine's value of it
+    (the difference of two FP32 tendencies that share every other term) is known to a few ulps of
+    those tendencies: each cell is checked to 4 ulps of the larger tendency plus 1e-4 of the
+    largest forcing term. The subsidence terms are checked on u and v. On theta (and q_v) the
+    reference's formula differences two FP32 slab-mean ratios <rho theta>/<rho> ~ 300 across two
+    levels, which carries ~1e-7 relative noise of theta itself; there the theta and q_v forcing is
+    checked without subsidence, and the subsidence through the forced state below."""
     c = CASES["moist_hill"]
     host = fe.cases.setup_host(c["case"], c["nx"], c["ny"], c["nz"], params=LSF, **c["kw"])
     inp, cfg = host.inputs(), host.config()
@@ -480,22 +490,26 @@ def test_large_scale_forcing_matches_oracle(fe, kind):
     st = d.get_state()
     d.close()
     moved = dict(inp, hydroFlds=st["hydroFlds"], sgstke=st["sgstke"], moist=st["moist"])
-    diff = {}
-    for on in (0, 1):
-        cfg.lsfSelector = on
-        dom = fe.Domain(cfg)
-        dom.set_inputs(moved, 0.2, 8)
-        dom.set_stage_kernel(kind, 8 if kind == "march" else 0, 0)
-        o = Oracle(cfg)
-        o.set_inputs(moved, 0.2, 8)
-        diff[on] = (dom.build_frhs(2), o.build_frhs(2))
-        dom.close()
-    for key, fields in (("hydroFrhs", (1, 2, 4)), ("moistFrhs", (0,))):
-        for f in fields:
-            dg = interior(diff[1][0][key][f]).astype(np.float64) - interior(diff[0][0][key][f])
+    for sub, checks in ((1, (("hydroFrhs", 1), ("hydroFrhs", 2))), (0, (("hydroFrhs", 4), ("moistFrhs", 0)))):
+        cfg.lsf_horMnSubTerms = sub
+        diff = {}
+        for on in (0, 1):
+            cfg.lsfSelector = on
+            dom = fe.Domain(cfg)
+            dom.set_inputs(moved, 0.2, 8)
+            dom.set_stage_kernel(kind, 8 if kind == "march" else 0, 0)
+            o = Oracle(cfg)
+            o.set_inputs(moved, 0.2, 8)
+            diff[on] = (dom.build_frhs(2), o.build_frhs(2))
+            dom.close()
+        for key, f in checks:
+            on, off = interior(diff[1][0][key][f]), interior(diff[0][0][key][f])
+            dg = on.astype(np.float64) - off
             dr = interior(diff[1][1][key][f]) - interior(diff[0][1][key][f])
             assert np.abs(dr).max() > 0, (key, f)
-            assert rel_l2(dg, dr) < 1e-3, (kind, key, f, rel_l2(dg, dr))
+            tol = 4 * np.spacing(np.maximum(np.abs(on), np.abs(off))) + 1e-4 * np.abs(dr).max()
+            assert (np.abs(dg - dr) <= tol).all(), (kind, sub, key, f, float((np.abs(dg - dr) / tol).max()))
+    cfg.lsf_horMnSubTerms = 1
     cfg.lsfSelector = 1
     dom = fe.Domain(cfg)
     dom.set_inputs(inp)

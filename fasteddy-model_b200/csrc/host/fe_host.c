@@ -98,6 +98,7 @@ static char g_topoFile[1024];
 static char g_inFile[1024];
 static int ioOutputMode, frqOutput;
 static char g_msg[512];
+static char g_outPath[1024], g_outFileBase[256];
 static double *g_topoGlobal; /* Nx*Ny, i-major, set by fe_host_set_topography */
 
 const char *fe_host_last_message(void) { return g_msg[0] ? g_msg : fe_params_last_message(); }
@@ -120,8 +121,11 @@ static int query_all(void) {
   g_inFile[0] = 0;
   Q(rc, fe_params_query_string("inFile", &s, FE_PARAM_OPTIONAL));
   if (s) snprintf(g_inFile, sizeof(g_inFile), "%s", s);
+  g_outPath[0] = g_outFileBase[0] = 0;
   Q(rc, fe_params_query_string("outPath", &s, FE_PARAM_MANDATORY));
+  if (s) snprintf(g_outPath, sizeof(g_outPath), "%s", s);
   Q(rc, fe_params_query_string("outFileBase", &s, FE_PARAM_MANDATORY));
+  if (s) snprintf(g_outFileBase, sizeof(g_outFileBase), "%s", s);
   Q(rc, fe_params_query_int("frqOutput", &frqOutput, 0, INT_MAX, FE_PARAM_MANDATORY));
   /* FECUDA (fecuda.c:35-44) */
   Q(rc, fe_params_query_int("tBx", &tBx, 1, INT_MAX, FE_PARAM_MANDATORY));
@@ -808,3 +812,110 @@ int fe_host_set_qv_profile(float q_sfc, float q_top, float z_top) {
 }
 
 const char *fe_host_topofile(void) { return g_topoFile; }
+
+
+/* ------------------------------------------------------------------ binary output */
+/* The reference's raw binary output (io_binary.c:19-132): one file per rank and output step,
+ * <outPath><outFileBase>_rank_<rank>.<step>, holding every variable registered for output in
+ * registration order. A record is the name length (int), the name bytes, the number of
+ * dimensions (int, 3 or 2) and the halo-inclusive extents (int each), then the float values in
+ * the halo-inclusive layout. u, v, w, theta, TKE and moisture are written divided by rho (the
+ * reference divides its host arrays in place; this writer divides into a scratch buffer and leaves
+ * the host state as it is). */
+static int put_record(FILE *f, const char *name, int nd, const float *v, const float *rho, float *tmp) {
+  static const char *divided[] = {"u", "v", "w", "theta", "TKE_0", "TKE_1", "qv", "ql", "qr", NULL};
+  int len = (int)strlen(name), ext[3] = {Nxp + 2 * Nh, Nyp + 2 * Nh, Nzp + 2 * Nh};
+  size_t n = (size_t)ext[0] * ext[1] * (nd == 3 ? (size_t)ext[2] : 1), m;
+  int a, div = 0;
+  if (nd == 3)
+    for (a = 0; divided[a]; a++) div |= !strcmp(name, divided[a]);
+  if (div) {
+    for (m = 0; m < n; m++) tmp[m] = v[m] / rho[m];
+    v = tmp;
+  }
+  if (fwrite(&len, sizeof(int), 1, f) != 1 || fwrite(name, 1, (size_t)len, f) != (size_t)len ||
+      fwrite(&nd, sizeof(int), 1, f) != 1 || fwrite(ext, sizeof(int), (size_t)nd, f) != (size_t)nd ||
+      fwrite(v, sizeof(float), n, f) != n)
+    return -1;
+  return 0;
+}
+
+/* Registration order and conditions of the reference's output list (grid.c:229-232,
+ * hydro_core.c:632-930) without its DEBUG and BASE_STATE_IO_DUMP builds. */
+int fe_host_write_binary(const char *path, int tstep) {
+  char name[1100], fn[64];
+  size_t n = fe_host_field_elems();
+  const float *rho = hydroFlds;
+  float *tmp;
+  FILE *f;
+  int rc = 0, q;
+  static const char *hydroNames[5] = {"rho", "u", "v", "w", "theta"};
+  static const char *tauNames[9] = {"Tau11", "Tau21", "Tau31", "Tau32", "Tau22", "Tau33", "TauTH1", "TauTH2", "TauTH3"};
+  static const char *moistNames[2] = {"qv", "ql"};
+  if (!hydroFlds) {
+    snprintf(g_msg, sizeof(g_msg), "fe_host_write_binary: no host state (call fe_host_init first)");
+    return -1;
+  }
+  if (!path || !path[0]) {
+    snprintf(name, sizeof(name), "%s%s_rank_%d.%d", g_outPath, g_outFileBase, 0, tstep);
+    path = name;
+  }
+  f = fopen(path, "wb");
+  if (!f) {
+    snprintf(g_msg, sizeof(g_msg), "fe_host_write_binary: cannot open %s", path);
+    return -1;
+  }
+  tmp = (float *)malloc(n * sizeof(float));
+  if (!tmp) {
+    fclose(f);
+    return -1;
+  }
+#define PUT(nm, nd, v) rc |= put_record(f, (nm), (nd), (v), rho, tmp)
+  PUT("xPos", 3, xPos); PUT("yPos", 3, yPos); PUT("zPos", 3, zPos); PUT("topoPos", 2, topoPos);
+  for (q = 0; q < 5; q++) PUT(hydroNames[q], 3, hydroFlds + q * n);
+  PUT("pressure", 3, hydroPres);
+  if (hydroForcingWrite == 1)
+    for (q = 0; q < 5; q++) {
+      snprintf(fn, sizeof(fn), "F_%s", hydroNames[q]);
+      PUT(fn, 3, hydroFldsFrhs + q * n);
+    }
+  if (TKESelector > 0) {
+    for (q = 0; q < TKESelector; q++) {
+      snprintf(fn, sizeof(fn), "TKE_%d", q);
+      PUT(fn, 3, sgstkeScalars + q * n);
+    }
+    if (hydroForcingWrite == 1)
+      for (q = 0; q < TKESelector; q++) {
+        snprintf(fn, sizeof(fn), "F_TKE%d", q);
+        PUT(fn, 3, sgstkeScalarsFrhs + q * n);
+      }
+  }
+  if (hydroSubGridWrite == 1 && turbulenceSelector > 0)
+    for (q = 0; q < 9; q++) PUT(tauNames[q], 3, hydroTauFlds + q * n);
+  if (surflayerSelector > 0) {
+    PUT("tskin", 2, tskin); PUT("fricVel", 2, fricVel); PUT("htFlux", 2, htFlux); PUT("invOblen", 2, invOblen);
+    if (moistureSelector > 0) { PUT("qskin", 2, qskin); PUT("qFlux", 2, qFlux); }
+    PUT("z0m", 2, z0m); PUT("z0t", 2, z0t);
+  }
+  if (moistureSelector > 0) {
+    for (q = 0; q < moistureNvars && q < 2; q++) PUT(moistNames[q], 3, moistScalars + q * n);
+    if (hydroForcingWrite == 1)
+      for (q = 0; q < moistureNvars && q < 2; q++) {
+        snprintf(fn, sizeof(fn), "F_%s", moistNames[q]);
+        PUT(fn, 3, moistScalarsFrhs + q * n);
+      }
+    if (hydroSubGridWrite == 1 && moistureSGSturb > 0)
+      for (q = 0; q < moistureNvars && q < 2; q++) {
+        int d;
+        for (d = 0; d < 3; d++) {
+          snprintf(fn, sizeof(fn), "TauQ%c%d", q == 0 ? 'v' : 'l', d + 1);
+          PUT(fn, 3, moistTauFlds + (size_t)(q * 3 + d) * n);
+        }
+      }
+  }
+#undef PUT
+  free(tmp);
+  if (fclose(f) != 0) rc = -1;
+  if (rc) snprintf(g_msg, sizeof(g_msg), "fe_host_write_binary: write to %s failed", path);
+  return rc;
+}

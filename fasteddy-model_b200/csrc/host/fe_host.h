@@ -26,6 +26,10 @@ void fe_host_cleanup(void);
 size_t fe_host_field_elems(void);
 size_t fe_host_plane_elems(void);
 const char *fe_host_last_message(void);
+/* Write the host state in the reference's raw binary output format (io_binary.c:19-132):
+ * every variable the reference registers for output, in its order. path NULL or "":
+ * <outPath><outFileBase>_rank_0.<tstep> from the parameter file. Returns 0 or -1. */
+int fe_host_write_binary(const char *path, int tstep);
 const char *fe_host_topofile(void);
 
 #ifdef __cplusplus

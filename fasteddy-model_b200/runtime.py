@@ -115,6 +115,7 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_host_field_elems", ctypes.c_size_t, []),
         ("fe_host_plane_elems", ctypes.c_size_t, []),
         ("fe_host_last_message", ctypes.c_char_p, []),
+        ("fe_host_write_binary", ip, [ctypes.c_char_p, ip]),
     ]:
         _declare(host, name, res, args)
     for name, res, args in [
@@ -237,6 +238,12 @@ class Host:
     def set_topography(self, topo: np.ndarray) -> None:
         t = np.ascontiguousarray(topo, dtype=np.float32)
         if self.h.fe_host_set_topography(_fptr(t), t.shape[0], t.shape[1]) != 0:
+            raise FeError(self.h.fe_host_last_message().decode())
+
+    def write_binary(self, path: str | None = None, tstep: int = 0) -> None:
+        """Write the host state in FastEddy's raw binary output format (one file per output
+        step, io_binary.c:19-132); path None: <outPath><outFileBase>_rank_0.<tstep>."""
+        if self.h.fe_host_write_binary(path.encode() if path else None, tstep) != 0:
             raise FeError(self.h.fe_host_last_message().decode())
 
     def write_topofile(self, path: str) -> None:
@@ -568,3 +575,23 @@ class Mlp:
         ms = ctypes.c_float()
         _check(self.e.fe_mlp_time(self.h, 1 if train else 0, batch, reps, ctypes.byref(ms)), "fe_mlp_time")
         return float(ms.value)
+
+
+def read_binary(path: str) -> dict[str, np.ndarray]:
+    """Records of a FastEddy raw binary output file (io_binary.c:59-126), in file order: name ->
+    float32 array of the halo-inclusive extents (nx, ny, nz) or (nx, ny)."""
+    out: dict[str, np.ndarray] = {}
+    with open(path, "rb") as f:
+        data = f.read()
+    pos = 0
+    while pos < len(data):
+        (nlen,) = np.frombuffer(data, np.int32, 1, pos)
+        name = data[pos + 4:pos + 4 + int(nlen)].decode()
+        pos += 4 + int(nlen)
+        (nd,) = np.frombuffer(data, np.int32, 1, pos)
+        ext = tuple(int(e) for e in np.frombuffer(data, np.int32, int(nd), pos + 4))
+        pos += 4 + 4 * int(nd)
+        cnt = int(np.prod(ext))
+        out[name] = np.frombuffer(data, np.float32, cnt, pos).reshape(ext).copy()
+        pos += 4 * cnt
+    return out

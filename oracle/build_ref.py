@@ -6,6 +6,9 @@ stub in oracle/refshim, and oracle/ref_harness.c. The reference sources are comp
 for sm_100a with their own flags (-std=c++11, relocatable device code, device link),
 replacing only -arch=sm_70. The result runs only on a GPU box; building needs no GPU.
 
+Also builds oracle/_ref/fe_ref_io from the reference's host modules and its binary output
+writer (IO/io_binary.c, compiled as part of IO/io.c) with oracle/ref_io.c: no CUDA, it runs on any machine.
+
 usage: python oracle/build_ref.py [REFERENCE_SRC_DIR]
 """
 from __future__ import annotations
@@ -83,6 +86,30 @@ def build(src: str = DEFAULT_SRC, verbose: bool = False) -> str:
     dl = os.path.join(OUT, "obj", "devlink.o")
     _run([NVCC, *ARCH, "-dlink", *cu_objs, "-o", dl])
     _run([NVCC, *ARCH, "-o", exe, *objs, *cu_objs, "-lm", "-lstdc++"])
+    build_io(src, inc)
+    return exe
+
+
+# host modules the binary-output checker needs (no CUDA wrappers, no FECUDA)
+IO_SOURCES = [
+    "PARAMETERS/parameters.c", "PARAMETERS/hashTable.c", "FEMPI/fempi.c", "MEM_UTILS/mem_utils.c", "IO/io.c",
+    "IO/ioVarsList.c", "GRID/grid.c", "HYDRO_CORE/hydro_core.c", "TIME_INTEGRATION/time_integration.c",
+]  # IO/io.c includes io_binary.c (io.c:202)
+
+
+def build_io(src: str, inc: list[str]) -> str:
+    exe = os.path.join(OUT, "fe_ref_io")
+    objs = []
+    for rel in IO_SOURCES:
+        o = _obj(rel)
+        if not os.path.exists(o):
+            _run(["gcc", "-O2", "-m64", "-w", *DEFINES, *inc, "-c", os.path.join(src, rel), "-o", o])
+        objs.append(o)
+    for name in ("mpi_stub.c", "netcdf_stub.c"):
+        objs.append(os.path.join(OUT, "obj", name[:-2] + ".o"))
+    io = os.path.join(OUT, "obj", "ref_io.o")
+    _run(["gcc", "-O2", "-m64", *inc, "-c", os.path.join(HERE, "ref_io.c"), "-o", io])
+    _run(["gcc", "-o", exe, *objs, io, "-lm"])
     return exe
 
 

@@ -1,0 +1,73 @@
+"""FastEddy's raw binary output (io_binary.c:19-132) written by the host layer, checked byte for
+byte against the reference's own writer (oracle/_ref/fe_ref_io, built by oracle/build_ref.py
+from the reference's host modules; it needs no GPU) on identical host arrays."""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+REF_IO = os.path.join(ROOT, "oracle", "_ref", "fe_ref_io")
+
+# every registered array of the host layer: (file name for the reference program, host symbol,
+# fields, 2-D)
+ARRAYS = [("xPos", "xPos", 1, False), ("yPos", "yPos", 1, False), ("zPos", "zPos", 1, False),
+          ("topoPos", "topoPos", 1, True), ("hydroFlds", "hydroFlds", 5, False), ("hydroPres", "hydroPres", 1, False),
+          ("hydroFldsFrhs", "hydroFldsFrhs", 5, False), ("sgstke", "sgstkeScalars", 1, False),
+          ("sgstkeFrhs", "sgstkeScalarsFrhs", 1, False), ("taus", "hydroTauFlds", 9, False),
+          ("tskin", "tskin", 1, True), ("fricVel", "fricVel", 1, True), ("htFlux", "htFlux", 1, True),
+          ("invOblen", "invOblen", 1, True), ("z0m", "z0m", 1, True), ("z0t", "z0t", 1, True),
+          ("qskin", "qskin", 1, True), ("qFlux", "qFlux", 1, True)]
+
+
+def _host(fe, case, params, outdir):
+    host = fe.Host()
+    text = fe.cases.param_text(case, 8, 6, 6, params=params).replace("outPath = ./output/", f"outPath = {outdir}/")
+    host.load_params_text(text)
+    host.init(5)
+    return host, text
+
+
+@pytest.mark.parametrize("case,params", [
+    ("cbl_moist_hill", dict(hydroForcingWrite=1, hydroSubGridWrite=1)),  # every optional record
+    ("cbl_dry", {}),  # the default record list
+])
+def test_binary_output_matches_the_reference_writer(fe, tmp_path, case, params):
+    if not os.path.exists(REF_IO):
+        pytest.skip("reference IO program not built (python oracle/build_ref.py)")
+    ours, ref, ind = tmp_path / "ours", tmp_path / "ref", tmp_path / "in"
+    for d in (ours, ref, ind):
+        d.mkdir()
+    host, text = _host(fe, case, params, ours)
+    ntke, nm = host.nfields()
+    rng = np.random.default_rng(11)
+    arrays = list(ARRAYS)
+    if nm:
+        arrays += [("moist", "moistScalars", nm, False), ("moistFrhs", "moistScalarsFrhs", nm, False),
+                   ("moistTaus", "moistTauFlds", 3 * nm, False)]
+    for fname, sym, nf, two_d in arrays:
+        if sym.startswith("sgstke") and not ntke:
+            continue
+        a = host.array(sym, nf, two_d)
+        if sym in ("hydroPres", "hydroFldsFrhs", "sgstkeScalarsFrhs", "hydroTauFlds", "invOblen", "moistScalarsFrhs",
+                   "moistTauFlds"):
+            a[...] = rng.standard_normal(a.shape).astype(np.float32)  # fields the initial state leaves at 0
+        a.tofile(str(ind / f"{fname}.bin"))
+    host.write_binary(None, 7)
+    (tmp_path / "ref.in").write_text(text.replace(f"outPath = {ours}/", f"outPath = {ref}/"))
+    res = subprocess.run([REF_IO, str(tmp_path / "ref.in"), str(ind), "7"], capture_output=True, text=True, timeout=120)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+    name = "FE_B200_rank_0.7"
+    mine, theirs = (ours / name).read_bytes(), (ref / name).read_bytes()
+    assert len(mine) == len(theirs)
+    assert mine == theirs
+    recs = fe.read_binary(str(ours / name))
+    state = host.array("hydroFlds", 5)
+    np.testing.assert_array_equal(recs["rho"], state[0])
+    np.testing.assert_array_equal(recs["u"], state[1] / state[0])
+    assert ("Tau11" in recs) == bool(params) and ("F_theta" in recs) == bool(params)
+    host.cleanup()

@@ -919,3 +919,173 @@ int fe_host_write_binary(const char *path, int tstep) {
   if (rc) snprintf(g_msg, sizeof(g_msg), "fe_host_write_binary: write to %s failed", path);
   return rc;
 }
+
+
+/* ------------------------------------------------------------------ netCDF output */
+/* The reference writes its output as netCDF (io_netcdf.c:392-717): dimensions time (unlimited,
+ * one record), zIndex, yIndex, xIndex (interior extents); int coordinate variables zIndex,
+ * yIndex, xIndex holding 0..N-1; then every variable registered for output, in registration
+ * order, as float (time, zIndex, yIndex, xIndex) or (time, yIndex, xIndex) with the interior cells
+ * only, x fastest, u, v, w, theta, TKE and moisture divided by rho (its NORHO build,
+ * io_netcdf.c:340). The reference asks the netCDF library for its NETCDF4 (HDF5) container; this
+ * writer has no library to call and writes the same dimensions, variables and values in the
+ * classic 64-bit-offset container (CDF-2), which the netCDF library and its Python readers open
+ * the same way. No attributes are written (the reference writes none). */
+typedef struct {
+  const char *name;
+  int nd;           /* 3: (time, z, y, x), 2: (time, y, x) */
+  const float *v;   /* halo-inclusive host array */
+} nc_rec;
+
+static void be32(unsigned char *p, uint32_t x) { p[0] = x >> 24; p[1] = x >> 16; p[2] = x >> 8; p[3] = x; }
+static int put_be32(FILE *f, uint32_t x) { unsigned char b[4]; be32(b, x); return fwrite(b, 1, 4, f) == 4 ? 0 : -1; }
+static int put_be64(FILE *f, uint64_t x) {
+  int rc = put_be32(f, (uint32_t)(x >> 32));
+  rc |= put_be32(f, (uint32_t)x);
+  return rc;
+}
+static int put_name(FILE *f, const char *s) {
+  static const unsigned char zero[4] = {0, 0, 0, 0};
+  size_t n = strlen(s);
+  int rc = put_be32(f, (uint32_t)n);
+  if (fwrite(s, 1, n, f) != n) return -1;
+  /* (name bytes follow their length, zero-padded to 4 bytes) */
+  if (n % 4) rc |= fwrite(zero, 1, 4 - n % 4, f) == 4 - n % 4 ? 0 : -1;
+  return rc;
+}
+static size_t name_bytes(const char *s) { size_t n = strlen(s); return 4 + (n + 3) / 4 * 4; }
+
+/* The same registration order and conditions as fe_host_write_binary. Returns the count. */
+static int output_registry(nc_rec *r, char names[][16]) {
+  size_t n = fe_host_field_elems();
+  int c = 0, q, d;
+  static const char *hydroNames[5] = {"rho", "u", "v", "w", "theta"};
+  static const char *tauNames[9] = {"Tau11", "Tau21", "Tau31", "Tau32", "Tau22", "Tau33", "TauTH1", "TauTH2", "TauTH3"};
+  static const char *moistNames[2] = {"qv", "ql"};
+#define REG(nm, dims, arr) do { snprintf(names[c], 16, "%s", (nm)); r[c].name = names[c]; r[c].nd = (dims); r[c].v = (arr); c++; } while (0)
+  REG("xPos", 3, xPos); REG("yPos", 3, yPos); REG("zPos", 3, zPos); REG("topoPos", 2, topoPos);
+  for (q = 0; q < 5; q++) REG(hydroNames[q], 3, hydroFlds + q * n);
+  REG("pressure", 3, hydroPres);
+  if (hydroForcingWrite == 1)
+    for (q = 0; q < 5; q++) { char t[16]; snprintf(t, sizeof(t), "F_%s", hydroNames[q]); REG(t, 3, hydroFldsFrhs + q * n); }
+  if (TKESelector > 0) {
+    for (q = 0; q < TKESelector; q++) { char t[16]; snprintf(t, sizeof(t), "TKE_%d", q); REG(t, 3, sgstkeScalars + q * n); }
+    if (hydroForcingWrite == 1)
+      for (q = 0; q < TKESelector; q++) { char t[16]; snprintf(t, sizeof(t), "F_TKE%d", q); REG(t, 3, sgstkeScalarsFrhs + q * n); }
+  }
+  if (hydroSubGridWrite == 1 && turbulenceSelector > 0)
+    for (q = 0; q < 9; q++) REG(tauNames[q], 3, hydroTauFlds + q * n);
+  if (surflayerSelector > 0) {
+    REG("tskin", 2, tskin); REG("fricVel", 2, fricVel); REG("htFlux", 2, htFlux); REG("invOblen", 2, invOblen);
+    if (moistureSelector > 0) { REG("qskin", 2, qskin); REG("qFlux", 2, qFlux); }
+    REG("z0m", 2, z0m); REG("z0t", 2, z0t);
+  }
+  if (moistureSelector > 0) {
+    for (q = 0; q < moistureNvars && q < 2; q++) REG(moistNames[q], 3, moistScalars + q * n);
+    if (hydroForcingWrite == 1)
+      for (q = 0; q < moistureNvars && q < 2; q++) { char t[16]; snprintf(t, sizeof(t), "F_%s", moistNames[q]); REG(t, 3, moistScalarsFrhs + q * n); }
+    if (hydroSubGridWrite == 1 && moistureSGSturb > 0)
+      for (q = 0; q < moistureNvars && q < 2; q++)
+        for (d = 0; d < 3; d++) { char t[16]; snprintf(t, sizeof(t), "TauQ%c%d", q == 0 ? 'v' : 'l', d + 1); REG(t, 3, moistTauFlds + (size_t)(q * 3 + d) * n); }
+  }
+#undef REG
+  return c;
+}
+
+int fe_host_write_netcdf(const char *path, int tstep) {
+  static const char *dimNames[4] = {"time", "zIndex", "yIndex", "xIndex"};
+  static const char *divided[] = {"u", "v", "w", "theta", "TKE_0", "TKE_1", "qv", "ql", "qr", NULL};
+  nc_rec reg[64];
+  char names[64][16], fname[1100];
+  const int Nx = Nxp, Ny = Nyp, Nz = Nzp, Nyh = Nyp + 2 * Nh, Nzh = Nzp + 2 * Nh;
+  const uint32_t dimLen[4] = {0, (uint32_t)Nz, (uint32_t)Ny, (uint32_t)Nx};
+  int nreg, v, rc = 0, i, j, k, a;
+  uint64_t hdr, off;
+  size_t n3 = (size_t)Nx * Ny * Nz;
+  float *buf;
+  unsigned char *out;
+  FILE *f;
+  if (!hydroFlds) {
+    snprintf(g_msg, sizeof(g_msg), "fe_host_write_netcdf: no host state (call fe_host_init first)");
+    return -1;
+  }
+  nreg = output_registry(reg, names);
+  if (!path || !path[0]) {
+    snprintf(fname, sizeof(fname), "%s%s.%d", g_outPath, g_outFileBase, tstep);
+    path = fname;
+  }
+  /* header size: magic, numrecs, dim list, empty attribute list, variable list */
+  hdr = 4 + 4 + 8;
+  for (a = 0; a < 4; a++) hdr += name_bytes(dimNames[a]) + 4;
+  hdr += 8 + 8;
+  for (a = 1; a < 4; a++) hdr += name_bytes(dimNames[a]) + 4 + 4 + 8 + 4 + 4 + 8;
+  for (v = 0; v < nreg; v++) hdr += name_bytes(reg[v].name) + 4 + 4 * (reg[v].nd == 3 ? 4 : 3) + 8 + 4 + 4 + 8;
+  f = fopen(path, "wb");
+  if (!f) {
+    snprintf(g_msg, sizeof(g_msg), "fe_host_write_netcdf: cannot open %s", path);
+    return -1;
+  }
+  /* every write below is its own statement: the file order is the statement order */
+#define W(x) rc |= (x)
+  W(fwrite("CDF\x02", 1, 4, f) == 4 ? 0 : -1);
+  W(put_be32(f, 1));                         /* numrecs */
+  W(put_be32(f, 0x0A)); W(put_be32(f, 4));   /* NC_DIMENSION, 4 dimensions */
+  for (a = 0; a < 4; a++) { W(put_name(f, dimNames[a])); W(put_be32(f, dimLen[a])); }
+  W(put_be32(f, 0)); W(put_be32(f, 0));      /* no global attributes */
+  W(put_be32(f, 0x0B)); W(put_be32(f, (uint32_t)(3 + nreg)));  /* NC_VARIABLE */
+  off = hdr;
+  for (a = 1; a < 4; a++) {  /* coordinate variables zIndex, yIndex, xIndex: NC_INT, non-record */
+    W(put_name(f, dimNames[a])); W(put_be32(f, 1)); W(put_be32(f, (uint32_t)a));
+    W(put_be32(f, 0)); W(put_be32(f, 0));    /* no attributes */
+    W(put_be32(f, 4)); W(put_be32(f, 4 * dimLen[a])); W(put_be64(f, off));
+    off += 4 * (uint64_t)dimLen[a];
+  }
+  for (v = 0; v < nreg; v++) {  /* record variables, NC_FLOAT, in one record */
+    uint64_t vsize = 4 * (uint64_t)Nx * Ny * (reg[v].nd == 3 ? (uint64_t)Nz : 1);
+    W(put_name(f, reg[v].name)); W(put_be32(f, reg[v].nd == 3 ? 4 : 3)); W(put_be32(f, 0));
+    if (reg[v].nd == 3) W(put_be32(f, 1));
+    W(put_be32(f, 2)); W(put_be32(f, 3));
+    W(put_be32(f, 0)); W(put_be32(f, 0));    /* no attributes */
+    W(put_be32(f, 5)); W(put_be32(f, (uint32_t)vsize)); W(put_be64(f, off));
+    off += vsize;
+  }
+#undef W
+  buf = (float *)malloc(n3 * sizeof(float));
+  out = (unsigned char *)malloc(n3 * 4);
+  if (!buf || !out) {
+    free(buf); free(out); fclose(f);
+    return -1;
+  }
+  for (a = 1; a < 4; a++) {
+    for (i = 0; i < (int)dimLen[a]; i++) be32(out + 4 * i, (uint32_t)i);
+    rc |= fwrite(out, 1, 4 * dimLen[a], f) == 4 * dimLen[a] ? 0 : -1;
+  }
+  for (v = 0; v < nreg; v++) {
+    const float *src = reg[v].v;
+    size_t m = 0;
+    int div = 0;
+    for (a = 0; reg[v].nd == 3 && divided[a]; a++) div |= !strcmp(reg[v].name, divided[a]);
+    if (reg[v].nd == 3) {
+      for (k = 0; k < Nz; k++)
+        for (j = 0; j < Ny; j++)
+          for (i = 0; i < Nx; i++) {
+            size_t c = ((size_t)(i + Nh) * Nyh + (j + Nh)) * Nzh + (k + Nh);
+            buf[m++] = div ? src[c] / hydroFlds[c] : src[c];
+          }
+    } else {
+      for (j = 0; j < Ny; j++)
+        for (i = 0; i < Nx; i++) buf[m++] = src[(size_t)(i + Nh) * Nyh + (j + Nh)];
+    }
+    for (i = 0; i < (int)m; i++) {
+      uint32_t u;
+      memcpy(&u, buf + i, 4);
+      be32(out + 4 * (size_t)i, u);
+    }
+    rc |= fwrite(out, 1, 4 * m, f) == 4 * m ? 0 : -1;
+  }
+  free(buf);
+  free(out);
+  if (fclose(f) != 0) rc = -1;
+  if (rc) snprintf(g_msg, sizeof(g_msg), "fe_host_write_netcdf: write to %s failed", path);
+  return rc;
+}

@@ -30,6 +30,10 @@ const char *fe_host_last_message(void);
  * every variable the reference registers for output, in its order. path NULL or "":
  * <outPath><outFileBase>_rank_0.<tstep> from the parameter file. Returns 0 or -1. */
 int fe_host_write_binary(const char *path, int tstep);
+/* Write the host state as the reference's netCDF output (io_netcdf.c:392-717): dimensions time,
+ * zIndex, yIndex, xIndex, the registered variables over the interior cells, in the classic
+ * 64-bit-offset container. path NULL or "": <outPath><outFileBase>.<tstep>. Returns 0 or -1. */
+int fe_host_write_netcdf(const char *path, int tstep);
 const char *fe_host_topofile(void);
 
 #ifdef __cplusplus

@@ -116,6 +116,7 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_host_plane_elems", ctypes.c_size_t, []),
         ("fe_host_last_message", ctypes.c_char_p, []),
         ("fe_host_write_binary", ip, [ctypes.c_char_p, ip]),
+        ("fe_host_write_netcdf", ip, [ctypes.c_char_p, ip]),
     ]:
         _declare(host, name, res, args)
     for name, res, args in [
@@ -244,6 +245,13 @@ class Host:
         """Write the host state in FastEddy's raw binary output format (one file per output
         step, io_binary.c:19-132); path None: <outPath><outFileBase>_rank_0.<tstep>."""
         if self.h.fe_host_write_binary(path.encode() if path else None, tstep) != 0:
+            raise FeError(self.h.fe_host_last_message().decode())
+
+    def write_netcdf(self, path: str | None = None, tstep: int = 0) -> None:
+        """Write the host state as FastEddy's netCDF output (interior cells, dimensions time,
+        zIndex, yIndex, xIndex; io_netcdf.c:392-717) in the classic 64-bit-offset container;
+        path None: <outPath><outFileBase>.<tstep>."""
+        if self.h.fe_host_write_netcdf(path.encode() if path else None, tstep) != 0:
             raise FeError(self.h.fe_host_last_message().decode())
 
     def write_topofile(self, path: str) -> None:

@@ -71,3 +71,43 @@ def test_binary_output_matches_the_reference_writer(fe, tmp_path, case, params):
     np.testing.assert_array_equal(recs["u"], state[1] / state[0])
     assert ("Tau11" in recs) == bool(params) and ("F_theta" in recs) == bool(params)
     host.cleanup()
+
+
+@pytest.mark.parametrize("case,params", [("cbl_moist_hill", dict(hydroForcingWrite=1, hydroSubGridWrite=1)), ("cbl_dry", {})])
+def test_netcdf_output_has_the_reference_data_model(fe, tmp_path, case, params):
+    """The netCDF output (io_netcdf.c:392-717) read back by an independent reader (scipy's
+    classic-format netcdf_file): dimensions time (one record), zIndex, yIndex, xIndex; int
+    coordinate variables 0..N-1; the registered variables in the binary file's order, float over
+    (time, z, y, x) or (time, y, x), holding the binary record's interior cells transposed."""
+    from scipy.io import netcdf_file
+
+    host, _ = _host(fe, case, params, tmp_path)
+    rng = np.random.default_rng(3)
+    for sym, nf in (("hydroPres", 1), ("hydroFldsFrhs", 5), ("hydroTauFlds", 9)):
+        a = host.array(sym, nf)
+        a[...] = rng.standard_normal(a.shape).astype(np.float32)
+    host.write_binary(str(tmp_path / "out.bin"))
+    host.write_netcdf(None, 3)
+    recs = fe.read_binary(str(tmp_path / "out.bin"))
+    nx, ny, nz = (e - 6 for e in host.shape)
+    with netcdf_file(str(tmp_path / "FE_B200.3"), "r", mmap=False) as nc:
+        assert nc.version_byte == 2
+        assert nc.dimensions == {"time": None, "zIndex": nz, "yIndex": ny, "xIndex": nx}
+        assert "time" not in nc.variables  # a dimension only, as in the reference
+        names = [k for k in nc.variables if k not in ("zIndex", "yIndex", "xIndex")]
+        assert names == list(recs)
+        for d, n in (("zIndex", nz), ("yIndex", ny), ("xIndex", nx)):
+            np.testing.assert_array_equal(nc.variables[d][:], np.arange(n))
+            assert nc.variables[d].typecode() == "i"
+        for name, rec in recs.items():
+            var = nc.variables[name]
+            assert var.typecode() == "f"
+            got = np.asarray(var[:])
+            assert got.shape[0] == 1
+            if rec.ndim == 3:
+                assert var.dimensions == ("time", "zIndex", "yIndex", "xIndex")
+                np.testing.assert_array_equal(got[0], rec[3:-3, 3:-3, 3:-3].transpose(2, 1, 0))
+            else:
+                assert var.dimensions == ("time", "yIndex", "xIndex")
+                np.testing.assert_array_equal(got[0], rec[3:-3, 3:-3].T)
+    host.cleanup()

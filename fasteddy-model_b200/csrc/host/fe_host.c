@@ -96,6 +96,7 @@ static float thetaHeight, thetaAmplitude;
 static float nu_0;
 static char g_topoFile[1024];
 static char g_inFile[1024];
+static char g_inPath[1024];
 static int ioOutputMode, frqOutput;
 static char g_msg[512];
 static char g_outPath[1024], g_outFileBase[256];
@@ -117,7 +118,9 @@ static int query_all(void) {
   /* IO (io.c:65-77): accepted, output is not part of the hot path */
   ioOutputMode = 0;
   Q(rc, fe_params_query_int("ioOutputMode", &ioOutputMode, 0, 1, FE_PARAM_OPTIONAL));
+  g_inPath[0] = 0;
   Q(rc, fe_params_query_string("inPath", &s, FE_PARAM_OPTIONAL));
+  if (s) snprintf(g_inPath, sizeof(g_inPath), "%s", s);
   g_inFile[0] = 0;
   Q(rc, fe_params_query_string("inFile", &s, FE_PARAM_OPTIONAL));
   if (s) snprintf(g_inFile, sizeof(g_inFile), "%s", s);
@@ -744,8 +747,12 @@ static void build_surface(void) {
   }
 }
 
+static int restart_topography(const char *path);
+static int restart_state(const char *path);
+
 int fe_host_init(unsigned long long seed) {
   size_t n, n2;
+  char inName[2100];
   if (fe_params_error_count() != 0) {
     snprintf(g_msg, sizeof(g_msg), "parameter errors present: %s", fe_params_last_message());
     return -1;
@@ -783,15 +790,27 @@ int fe_host_init(unsigned long long seed) {
   if (g_topoFile[0] && !g_topoGlobal) {
     if (read_topofile(g_topoFile) != 0) return -1;
   }
+  snprintf(inName, sizeof(inName), "%s%s", g_inPath, g_inFile);  /* io_netcdf.c:112 */
+  if (g_inFile[0] && !g_topoFile[0] && restart_topography(inName) != 0) return -1;
   build_grid();
   build_metrics();
   build_base_state_and_ics(seed);
   if (surflayerSelector > 0) build_surface();
-  /* time (time_integration.c:69-118): no restart files in this build */
+  /* time (time_integration.c:95-105): a restart continues at the step after the first '.' of inFile */
   simTime = 0.0f;
   simTime_it = 0;
   simTime_itRestart = 0;
   numRKstages = 2;
+  if (g_inFile[0]) {
+    const char *dot = strchr(g_inFile, '.');
+    if (!dot || sscanf(dot + 1, "%d", &simTime_itRestart) != 1) {
+      snprintf(g_msg, sizeof(g_msg), "inFile %s has no .<step> suffix", g_inFile);
+      return -1;
+    }
+    simTime_it = simTime_itRestart;
+    simTime = dt * (float)simTime_it;
+    if (restart_state(inName) != 0) return -1;
+  }
   return 0;
 }
 
@@ -1088,4 +1107,262 @@ int fe_host_write_netcdf(const char *path, int tstep) {
   if (fclose(f) != 0) rc = -1;
   if (rc) snprintf(g_msg, sizeof(g_msg), "fe_host_write_netcdf: write to %s failed", path);
   return rc;
+}
+
+
+/* ------------------------------------------------------------------ restart input */
+/* Reading an initial-condition / restart file (inFile; FastEddy.c:202-243, io_netcdf.c:106-390):
+ * every variable registered for output that the file holds is read from its first time record
+ * into the interior cells; u, v, w, theta, TKE and moisture are multiplied back by rho (its NORHO
+ * build), the Tau fields are skipped, and the surface planes get their periodic halos
+ * (hydro_core.c:982-1014). The file must use the classic netCDF container (CDF-1 or CDF-2, as
+ * fe_host_write_netcdf writes): this build links no netCDF/HDF5 library. The grid is rebuilt from
+ * the file's topoPos (unless a topoFile is given) by the same grid code as a fresh start. */
+typedef struct {
+  char name[64];
+  int ndims, dimids[8], type, isrec;
+  uint64_t vsize, begin;
+} cdf_var;
+typedef struct {
+  FILE *f;
+  int version, ndims, nvars;
+  uint32_t numrecs, dimlen[16];
+  char dimname[16][64];
+  cdf_var var[256];
+  uint64_t recsize;
+} cdf_file;
+
+static int get_be32(FILE *f, uint32_t *x) {
+  unsigned char b[4];
+  if (fread(b, 1, 4, f) != 4) return -1;
+  *x = ((uint32_t)b[0] << 24) | ((uint32_t)b[1] << 16) | ((uint32_t)b[2] << 8) | b[3];
+  return 0;
+}
+static int get_name(FILE *f, char *out, size_t cap) {
+  uint32_t n;
+  char pad[4];
+  if (get_be32(f, &n) || n >= cap || fread(out, 1, n, f) != n) return -1;
+  out[n] = 0;
+  if (n % 4 && fread(pad, 1, 4 - n % 4, f) != 4 - n % 4) return -1;
+  return 0;
+}
+static int skip_atts(FILE *f) {
+  uint32_t tag, n, a, type, cnt;
+  char name[256];
+  static const int tsize[7] = {0, 1, 1, 2, 4, 4, 8};
+  if (get_be32(f, &tag) || get_be32(f, &n)) return -1;
+  if (tag == 0) return n == 0 ? 0 : -1;
+  if (tag != 0x0C) return -1;
+  for (a = 0; a < n; a++) {
+    uint64_t bytes;
+    if (get_name(f, name, sizeof(name)) || get_be32(f, &type) || get_be32(f, &cnt) || type < 1 || type > 6) return -1;
+    bytes = ((uint64_t)cnt * tsize[type] + 3) / 4 * 4;
+    if (fseek(f, (long)bytes, SEEK_CUR) != 0) return -1;
+  }
+  return 0;
+}
+static int cdf_open(cdf_file *c, const char *path) {
+  char magic[4];
+  uint32_t tag, n, k, x, hi, lo;
+  memset(c, 0, sizeof(*c));
+  c->f = fopen(path, "rb");
+  if (!c->f) return -1;
+  if (fread(magic, 1, 4, c->f) != 4 || memcmp(magic, "CDF", 3) != 0 || (magic[3] != 1 && magic[3] != 2)) return -2;
+  c->version = magic[3];
+  if (get_be32(c->f, &c->numrecs) || get_be32(c->f, &tag) || get_be32(c->f, &n)) return -2;
+  if (tag == 0x0A) {
+    if (n > 16) return -2;
+    for (k = 0; k < n; k++)
+      if (get_name(c->f, c->dimname[k], 64) || get_be32(c->f, &c->dimlen[k])) return -2;
+    c->ndims = (int)n;
+  } else if (tag != 0 || n != 0) {
+    return -2;
+  }
+  if (skip_atts(c->f)) return -2;
+  if (get_be32(c->f, &tag) || get_be32(c->f, &n)) return -2;
+  if (tag == 0x0B) {
+    if (n > 256) return -2;
+    for (k = 0; k < n; k++) {
+      cdf_var *v = &c->var[k];
+      uint32_t nd, d, type, vs;
+      if (get_name(c->f, v->name, sizeof(v->name)) || get_be32(c->f, &nd) || nd > 8) return -2;
+      v->ndims = (int)nd;
+      for (d = 0; d < nd; d++) {
+        if (get_be32(c->f, &x) || x >= (uint32_t)c->ndims) return -2;
+        v->dimids[d] = (int)x;
+      }
+      if (skip_atts(c->f) || get_be32(c->f, &type) || get_be32(c->f, &vs)) return -2;
+      v->type = (int)type;
+      v->vsize = vs;
+      if (c->version == 2) {
+        if (get_be32(c->f, &hi) || get_be32(c->f, &lo)) return -2;
+        v->begin = ((uint64_t)hi << 32) | lo;
+      } else {
+        if (get_be32(c->f, &lo)) return -2;
+        v->begin = lo;
+      }
+      v->isrec = nd > 0 && c->dimlen[v->dimids[0]] == 0;
+      if (v->isrec) c->recsize += v->vsize;
+    }
+    c->nvars = (int)n;
+  } else if (tag != 0 || n != 0) {
+    return -2;
+  }
+  return 0;
+}
+static const cdf_var *cdf_find(const cdf_file *c, const char *name) {
+  int k;
+  for (k = 0; k < c->nvars; k++)
+    if (!strcmp(c->var[k].name, name)) return &c->var[k];
+  return NULL;
+}
+static int cdf_dim(const cdf_file *c, const char *name) {
+  int k;
+  for (k = 0; k < c->ndims; k++)
+    if (!strcmp(c->dimname[k], name)) return k;
+  return -1;
+}
+/* First record of a float variable over (time, zIndex, yIndex, xIndex) or (time, yIndex, xIndex)
+ * into the interior of a halo-inclusive host array; nd = 3 or 2. Returns 0, 1 (absent), -1. */
+static int cdf_read_interior(cdf_file *c, const char *name, int nd, float *dst) {
+  const cdf_var *v = cdf_find(c, name);
+  const int Nyh = Nyp + 2 * Nh, Nzh = Nzp + 2 * Nh, nk = nd == 3 ? Nzp : 1;
+  size_t cnt = (size_t)Nxp * Nyp * nk, m;
+  unsigned char *raw;
+  int i, j, k;
+  if (!v) return 1;
+  if (v->type != 5 || v->ndims != nd + 1 || !v->isrec || c->numrecs < 1) return -1;
+  raw = (unsigned char *)malloc(cnt * 4);
+  if (!raw) return -1;
+  if (fseek(c->f, (long)v->begin, SEEK_SET) != 0 || fread(raw, 4, cnt, c->f) != cnt) {
+    free(raw);
+    return -1;
+  }
+  m = 0;
+  for (k = 0; k < nk; k++)
+    for (j = 0; j < Nyp; j++)
+      for (i = 0; i < Nxp; i++, m++) {
+        uint32_t u = ((uint32_t)raw[4 * m] << 24) | ((uint32_t)raw[4 * m + 1] << 16) | ((uint32_t)raw[4 * m + 2] << 8) |
+                     raw[4 * m + 3];
+        float val;
+        memcpy(&val, &u, 4);
+        if (nd == 3) dst[((size_t)(i + Nh) * Nyh + (j + Nh)) * Nzh + (k + Nh)] = val;
+        else dst[(size_t)(i + Nh) * Nyh + (j + Nh)] = val;
+      }
+  free(raw);
+  return 0;
+}
+static int cdf_check_dims(cdf_file *c, const char *path) {
+  int z = cdf_dim(c, "zIndex"), y = cdf_dim(c, "yIndex"), x = cdf_dim(c, "xIndex");
+  if (cdf_dim(c, "time") < 0 || z < 0 || y < 0 || x < 0) {
+    snprintf(g_msg, sizeof(g_msg), "inFile %s lacks the time/zIndex/yIndex/xIndex dimensions", path);
+    return -1;
+  }
+  if ((int)c->dimlen[z] != Nzp || (int)c->dimlen[y] != Nyp || (int)c->dimlen[x] != Nxp) {
+    snprintf(g_msg, sizeof(g_msg), "inFile %s is %ux%ux%u, the parameters ask for %dx%dx%d", path, c->dimlen[x],
+             c->dimlen[y], c->dimlen[z], Nxp, Nyp, Nzp);
+    return -1;
+  }
+  return 0;
+}
+static int cdf_open_checked(cdf_file *c, const char *path) {
+  int rc = cdf_open(c, path);
+  if (rc) {
+    snprintf(g_msg, sizeof(g_msg), rc == -1 ? "cannot open inFile %s" : "inFile %s is not a classic netCDF file", path);
+    if (c->f) fclose(c->f);
+    return -1;
+  }
+  if (cdf_check_dims(c, path)) {
+    fclose(c->f);
+    return -1;
+  }
+  return 0;
+}
+
+static int restart_topography(const char *path) {
+  cdf_file *c = (cdf_file *)calloc(1, sizeof(cdf_file));
+  float *t = alloc_f(fe_host_plane_elems());
+  int rc = -1, i, j;
+  if (!c || !t) goto done;
+  if (cdf_open_checked(c, path)) goto done;
+  rc = cdf_read_interior(c, "topoPos", 2, t);
+  fclose(c->f);
+  if (rc == 1) {  /* no topography in the file: flat, or the parameters' */
+    rc = 0;
+    goto done;
+  }
+  if (rc == 0) {
+    free(g_topoGlobal);
+    g_topoGlobal = (double *)malloc(sizeof(double) * (size_t)Nx * (size_t)Ny);
+    if (!g_topoGlobal) { rc = -1; goto done; }
+    for (i = 0; i < Nx; i++)
+      for (j = 0; j < Ny; j++) g_topoGlobal[(size_t)i * Ny + j] = t[(size_t)(i + Nh) * (Ny + 2 * Nh) + (j + Nh)];
+  } else {
+    snprintf(g_msg, sizeof(g_msg), "inFile %s: cannot read topoPos", path);
+  }
+done:
+  free(t);
+  free(c);
+  return rc;
+}
+
+/* periodic halo of a 2-D host plane (single rank) */
+static void plane_halo(float *a) {
+  const int Nxh = Nxp + 2 * Nh, Nyh = Nyp + 2 * Nh;
+  int i, j;
+  for (i = Nh; i < Nxp + Nh; i++)
+    for (j = 0; j < Nh; j++) {
+      a[(size_t)i * Nyh + j] = a[(size_t)i * Nyh + j + Nyp];
+      a[(size_t)i * Nyh + Nyp + Nh + j] = a[(size_t)i * Nyh + Nh + j];
+    }
+  for (i = 0; i < Nh; i++)
+    for (j = 0; j < Nyh; j++) {
+      a[(size_t)i * Nyh + j] = a[(size_t)(i + Nxp) * Nyh + j];
+      a[(size_t)(Nxp + Nh + i) * Nyh + j] = a[(size_t)(Nh + i) * Nyh + j];
+    }
+  (void)Nxh;
+}
+
+static int restart_state(const char *path) {
+  static const char *hydroNames[5] = {"rho", "u", "v", "w", "theta"};
+  static const char *moistNames[2] = {"qv", "ql"};
+  cdf_file *c = (cdf_file *)calloc(1, sizeof(cdf_file));
+  size_t n = fe_host_field_elems();
+  const int Nyh = Nyp + 2 * Nh, Nzh = Nzp + 2 * Nh;
+  int rc = 0, q, i, j, k;
+  if (!c) return -1;
+  if (cdf_open_checked(c, path)) { free(c); return -1; }
+#define RD(nm, nd, dst) do { int r_ = cdf_read_interior(c, (nm), (nd), (dst)); if (r_ < 0) { snprintf(g_msg, sizeof(g_msg), "inFile %s: cannot read %s", path, (nm)); rc = -1; } } while (0)
+  for (q = 0; q < 5; q++) RD(hydroNames[q], 3, hydroFlds + q * n);
+  RD("pressure", 3, hydroPres);
+  for (q = 0; q < TKESelector; q++) { char t[16]; snprintf(t, sizeof(t), "TKE_%d", q); RD(t, 3, sgstkeScalars + q * n); }
+  if (surflayerSelector > 0) {
+    RD("tskin", 2, tskin); RD("fricVel", 2, fricVel); RD("htFlux", 2, htFlux); RD("invOblen", 2, invOblen);
+    if (moistureSelector > 0) { RD("qskin", 2, qskin); RD("qFlux", 2, qFlux); }
+    RD("z0m", 2, z0m); RD("z0t", 2, z0t);
+  }
+  for (q = 0; moistureSelector > 0 && q < moistureNvars && q < 2; q++) RD(moistNames[q], 3, moistScalars + q * n);
+#undef RD
+  fclose(c->f);
+  free(c);
+  if (rc) return rc;
+  /* back to flux form (io_netcdf.c:340-375): interior cells times the file's rho */
+  {
+    float *flux[2 + 2 + 3] = {hydroFlds + n, hydroFlds + 2 * n, hydroFlds + 3 * n, hydroFlds + 4 * n, NULL, NULL, NULL};
+    int nf = 4;
+    for (q = 0; q < TKESelector && q < 1; q++) flux[nf++] = sgstkeScalars + q * n;
+    for (q = 0; moistureSelector > 0 && q < moistureNvars && q < 2; q++) flux[nf++] = moistScalars + q * n;
+    for (q = 0; q < nf; q++)
+      for (i = Nh; i < Nxp + Nh; i++)
+        for (j = Nh; j < Nyp + Nh; j++)
+          for (k = Nh; k < Nzp + Nh; k++) {
+            size_t cc = ((size_t)i * Nyh + j) * Nzh + k;
+            flux[q][cc] = flux[q][cc] * hydroFlds[cc];
+          }
+  }
+  if (surflayerSelector > 0) {
+    plane_halo(z0m); plane_halo(z0t); plane_halo(htFlux); plane_halo(fricVel); plane_halo(tskin);
+    if (moistureSelector > 0) { plane_halo(qFlux); plane_halo(qskin); }
+  }
+  return 0;
 }

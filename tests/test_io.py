@@ -111,3 +111,55 @@ def test_netcdf_output_has_the_reference_data_model(fe, tmp_path, case, params):
                 assert var.dimensions == ("time", "yIndex", "xIndex")
                 np.testing.assert_array_equal(got[0], rec[3:-3, 3:-3].T)
     host.cleanup()
+
+
+def test_restart_from_netcdf_output(fe, tmp_path):
+    """An inFile restart (FastEddy.c:202-243, io_netcdf.c:106-390, time_integration.c:95-105) from
+    the netCDF output of a perturbed state: the step comes from the name's suffix, the grid from
+    the file's topography, rho and the surface planes come back exactly, the flux-form fields
+    ((phi/rho) * rho) to one rounding, and the surface planes get their periodic halos."""
+    a, text = _host(fe, "cbl_moist_hill", {}, tmp_path)
+    a.gaussian_hill(12.0, 50.0)
+    a.init(5)
+    rng = np.random.default_rng(9)
+    H = a.array("hydroFlds", 5)
+    H[1:4] += rng.standard_normal(H[1:4].shape).astype(np.float32)
+    M = a.array("moistScalars", 2)
+    M[1] = np.abs(rng.standard_normal(M[1].shape)).astype(np.float32) * 1e-3
+    for nm in ("tskin", "htFlux", "fricVel"):
+        p = a.array(nm, 1, True)
+        p[...] = rng.random(p.shape).astype(np.float32)
+    a.write_netcdf(str(tmp_path / "RUN.40"))
+    ia = {k: (v.copy() if v is not None else None) for k, v in a.inputs().items()}
+    ta = a.array("topoPos", 1, True).copy()
+    a.cleanup()
+
+    b = fe.Host()
+    b.load_params_text(text.replace("inPath =\n", f"inPath = {tmp_path}/\n").replace("inFile =\n", "inFile = RUN.40\n"))
+    b.init(5)
+    ib = b.inputs()
+    assert b.gi("simTime_itRestart") == 40 and b.gi("simTime_it") == 40
+    I = (Ellipsis, slice(3, -3), slice(3, -3), slice(3, -3))
+    np.testing.assert_array_equal(b.array("topoPos", 1, True)[0, 3:-3, 3:-3], ta[0, 3:-3, 3:-3])
+    np.testing.assert_allclose(ib["zPos"], ia["zPos"], rtol=1e-6)
+    np.testing.assert_array_equal(ib["hydroFlds"][0][I], ia["hydroFlds"][0][I])
+    for f in range(1, 5):
+        np.testing.assert_allclose(ib["hydroFlds"][f][I], ia["hydroFlds"][f][I], rtol=2.5e-7, atol=1e-30)
+    for f in range(2):
+        np.testing.assert_allclose(ib["moist"][f][I], ia["moist"][f][I], rtol=2.5e-7, atol=1e-30)
+    np.testing.assert_allclose(ib["sgstke"][0][I], ia["sgstke"][0][I], rtol=2.5e-7, atol=1e-30)
+    for nm in ("tskin", "htFlux", "fricVel", "z0m"):
+        np.testing.assert_array_equal(ib[nm][3:-3, 3:-3], ia[nm][3:-3, 3:-3])
+        np.testing.assert_array_equal(ib[nm], np.pad(ib[nm][3:-3, 3:-3], 3, mode="wrap"))  # periodic halos
+    b.cleanup()
+
+
+def test_restart_rejects_a_mismatched_file(fe, tmp_path):
+    a, text = _host(fe, "cbl_dry", {}, tmp_path)
+    a.write_netcdf(str(tmp_path / "RUN.8"))
+    a.cleanup()
+    b = fe.Host()
+    small = fe.cases.param_text("cbl_dry", 8, 6, 4).replace("outPath = ./output/", f"outPath = {tmp_path}/")
+    b.load_params_text(small.replace("inPath =\n", f"inPath = {tmp_path}/\n").replace("inFile =\n", "inFile = RUN.8\n"))
+    with pytest.raises(fe.FeError, match="parameters ask for"):
+        b.init(5)

@@ -43,6 +43,9 @@ CASES = {
     "moist_hill_256": ("cbl_moist_hill", 256, 256, 128, True, 8,
                        "moist CBL over a Gaussian hill, 256x256x128, dx=dy=20 m, dz=10 m"),
     "dry_cbl_128": ("cbl_dry", 128, 128, 64, False, 6, "dry CBL, flat, 128x128x64, dx=dy=20 m, dz=10 m"),
+    "bomex_512": ("bomex", 512, 512, 128, False, 8,
+                  "moist CBL with the BOMEX tutorial's selectors (HYB34 for q_v, explicit filter, large-scale "
+                  "forcing with slab-mean subsidence), flat, 512x512x128, dx=dy=20 m, dz=10 m"),
     "dry_hill_1024": ("cbl_hill_dry", 1024, 1024, 256, True, 6,
                       "dry CBL over a Gaussian hill, 1024x1024x256, dx=dy=20 m, dz=10 m"),
 }

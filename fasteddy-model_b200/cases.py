@@ -8,6 +8,9 @@ input. Sizes can be shrunk for tests; the physics settings stay those of the cas
   cbl_moist_hill moist CBL over a Gaussian hill with Rayleigh damping (the 512x512x128 case)
   abl_neutral    neutral ABL member of the batched ensemble
   cbl_hill_dry   large dry CBL over the hill (the 1024x1024x256 case)
+  bomex          moist CBL, flat, with the selectors of FastEddy's BOMEX tutorial (HYB34 for q_v,
+                 explicit filter, large-scale forcing with slab-mean subsidence, mixing-ratio
+                 condensation on the base pressure)
 """
 from __future__ import annotations
 
@@ -124,6 +127,14 @@ physics_oneRKonly = 1
 """
 
 
+# Selectors of the BOMEX tutorial (tutorials/examples/Example04_BOMEX.in) applied to the moist case.
+BOMEX = dict(moistureAdvSelectorQv=2, moistureCond=3, moistureCondBasePres=1, filterSelector=1, filter_6th_coeff=0.03,
+             lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=1.0, lsf_w_surf=0.0, lsf_w_lev1=-23.4, lsf_w_lev2=0.0,
+             lsf_w_zlev1=1500.0, lsf_w_zlev2=2100.0, lsf_th_surf=-0.0833333, lsf_th_lev1=-0.0833333, lsf_th_lev2=0.0,
+             lsf_th_zlev1=1500.0, lsf_th_zlev2=3000.0, lsf_qv_surf=-0.0432, lsf_qv_lev1=-0.0432, lsf_qv_lev2=0.0,
+             lsf_qv_zlev1=300.0, lsf_qv_zlev2=500.0, surflayer_wq=0.052)
+
+
 # Time step. The cases ask for dx = dy = 20 m, dz = 10 m and dt = 0.05 s, but the
 # explicit acoustic step of this model is unstable there: c*dt*sqrt(dx^-2+dy^-2+dz^-2)
 # = 347*0.05*0.1225 = 2.1 exceeds the RK3 limit sqrt(3), and the reference build, the FP64
@@ -173,6 +184,10 @@ def param_text(case: str, nx: int, ny: int, nz: int, *, dx: float = 20.0, dz: fl
     elif case == "cbl_hill_dry":
         kw = dict(desc="dry CBL over a Gaussian hill", moist=0, damp=1, dampdepth=round(0.2 * nz * dz, 3),
                   wth=0.35, zsb=600.0, pert=1)
+    elif case == "bomex":
+        kw = dict(desc="BOMEX-configured moist CBL, flat terrain", moist=1, damp=1, dampdepth=round(0.2 * nz * dz, 3),
+                  wth=0.008, zsb=600.0, pert=1)
+        params = dict(BOMEX, **(params or {}))
     elif case == "abl_neutral":
         kw = dict(desc="neutral ABL ensemble member", moist=0, damp=0, dampdepth=100.0, wth=0.0,
                   zsb=round(0.8 * ztop, 3), pert=1)
@@ -207,6 +222,6 @@ def setup_host(case: str, nx: int, ny: int, nz: int, seed: int = 12345, hill_hal
     if case in ("cbl_moist_hill", "cbl_hill_dry"):
         host.gaussian_hill(hill_height, HILL_HALFWIDTH if hill_halfwidth is None else hill_halfwidth)
     host.init(seed)
-    if case == "cbl_moist_hill":
+    if case in ("cbl_moist_hill", "bomex"):
         host.set_qv_profile(*(qv if qv is not None else (QV_SFC, QV_TOP, QV_ZTOP)))
     return host

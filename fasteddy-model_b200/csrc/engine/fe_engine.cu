@@ -682,9 +682,12 @@ static cudaError_t march_attrs_one() {
   set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_ANY>, fe::MarchTile<8>::SMEM_BYTES);
   set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_DRY>, fe::MarchTile<8>::SMEM_BYTES);
   set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST>, fe::MarchTile<8>::SMEM_BYTES);
+  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST34>, fe::MarchTile<8>::SMEM_BYTES);
   if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
     set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST, 0>, fe::MarchTile<8>::SMEM_BYTES);
     set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST, 1>, fe::MarchTile<8>::SMEM_BYTES);
+    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST34, 0>, fe::MarchTile<8>::SMEM_BYTES);
+    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST34, 1>, fe::MarchTile<8>::SMEM_BYTES);
   }
   set((const void*)fe::k_march<STAGE, MODE, 4, fe::FL_ANY>, fe::MarchTile<4>::SMEM_BYTES);
   return e;
@@ -704,7 +707,10 @@ static int march_attrs() {
 static int march_flavor(const Phys& P) {
   if (P.pgf && P.tke && P.ntke == 1 && P.advSel == 3 && P.tkeAdvSel == 3 && P.oneRK == 1) {
     if (P.nmoist == 0) return fe::FL_DRY;
-    if (P.nmoist == 2 && P.qvAdvSel == 3 && P.qlSch == fe::ADV_WENO5) return fe::FL_MOIST;
+    if (P.nmoist == 2 && P.qlSch == fe::ADV_WENO5) {
+      if (P.qvAdvSel == 3) return fe::FL_MOIST;
+      if (P.qvAdvSel == 2) return fe::FL_MOIST34;
+    }
   }
   return fe::FL_ANY;
 }
@@ -722,7 +728,21 @@ static void launch_march(const fe_domain* d, cudaStream_t s, const float* cur, c
 // The moist flavour's last stage as a pair (k_march MP = 0 then 1): the kernel that runs in the
 // steps without saturation adjustment carries none of its code.
 static bool split_last_stage(const fe_domain* d) {
-  return d->kind == FE_KERNEL_MARCH && d->mtj == 8 && march_flavor(d->P) == fe::FL_MOIST;
+  if (d->kind != FE_KERNEL_MARCH || d->mtj != 8) return false;
+  const int fl = march_flavor(d->P);
+  return fl == fe::FL_MOIST || fl == fe::FL_MOIST34;
+}
+
+// A moist flavour's stage kernel: the last committing stage as its MP pair.
+template <int STAGE, int MODE, int FL>
+static void launch_moist(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
+                         const float* pcur, float* pnxt, float* frhs) {
+  if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
+    launch_march<STAGE, MODE, 8, FL, 0>(d, s, cur, base, nxt, pcur, pnxt, frhs);
+    launch_march<STAGE, MODE, 8, FL, 1>(d, s, cur, base, nxt, pcur, pnxt, frhs);
+  } else {
+    launch_march<STAGE, MODE, 8, FL>(d, s, cur, base, nxt, pcur, pnxt, frhs);
+  }
 }
 
 // Launch the fused stage kernel of stage STAGE in the domain's chosen form.
@@ -736,14 +756,8 @@ static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, c
     } else {
       switch (march_flavor(P)) {
         case fe::FL_DRY: launch_march<STAGE, MODE, 8, fe::FL_DRY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
-        case fe::FL_MOIST:
-          if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
-            launch_march<STAGE, MODE, 8, fe::FL_MOIST, 0>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-            launch_march<STAGE, MODE, 8, fe::FL_MOIST, 1>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-          } else {
-            launch_march<STAGE, MODE, 8, fe::FL_MOIST>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-          }
-          break;
+        case fe::FL_MOIST: launch_moist<STAGE, MODE, fe::FL_MOIST>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
+        case fe::FL_MOIST34: launch_moist<STAGE, MODE, fe::FL_MOIST34>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
         default: launch_march<STAGE, MODE, 8, fe::FL_ANY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
       }
     }

@@ -116,16 +116,18 @@ __device__ __forceinline__ float slot_b(const Phys& P, int s) {
 constexpr int FL_ANY = 0;
 constexpr int FL_DRY = 1;    // rho, rho u, rho v, rho w, rho theta, rho e
 constexpr int FL_MOIST = 2;  // ... plus rho q_v and rho q_l
+constexpr int FL_MOIST34 = 3;  // the moist set with HYB34 for q_v (the BOMEX tutorial's selectors)
 
 template <int FL>
 __device__ __forceinline__ bool f_on(const Phys& P, int s) {
   if constexpr (FL == FL_DRY) return s <= SL_E || s == SL_P;
-  else if constexpr (FL == FL_MOIST) return true;
+  else if constexpr (FL == FL_MOIST || FL == FL_MOIST34) return true;
   else return slot_on(P, s);
 }
 template <int FL>
 __device__ __forceinline__ int f_sel(const Phys& P, int s) {
-  if constexpr (FL != FL_ANY) return s == SL_QL ? 5 : 3;
+  if constexpr (FL == FL_MOIST34) return s == SL_QL ? 5 : (s == SL_QV ? 2 : 3);
+  else if constexpr (FL != FL_ANY) return s == SL_QL ? 5 : 3;
   else return slot_sel(P, s);
 }
 template <int FL>
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     k_march(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base, float* __restrict__ nxt,
             const float* __restrict__ pcur, float* __restrict__ pnxt, float* __restrict__ frhs, int ni) {
   const int ntke = FL == FL_ANY ? P.ntke : 1;
-  const int nmoist = FL == FL_ANY ? P.nmoist : (FL == FL_MOIST ? 2 : 0);
+  const int nmoist = FL == FL_ANY ? P.nmoist : ((FL == FL_MOIST || FL == FL_MOIST34) ? 2 : 0);
   const bool pgf = FL == FL_ANY ? (P.pgf != 0) : true;
   const bool tke = FL == FL_ANY ? (P.tke != 0) : true;
   // physics stages: every stage without oneRK, else the last; the flavours fix oneRK = 1

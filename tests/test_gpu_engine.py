@@ -362,9 +362,9 @@ def test_unsupported_configuration_is_rejected(fe):
 
 
 # The other advection schemes (upwind, QUICK, HYB34, WENO3, centred 2nd) on every advected field
-# and the explicit 6th-order filter of rho w, by the reference's own parameter keys. The last
-# case keeps the default schemes and adds the filter, so the compile-time moist form of the
-# march kernel carries it.
+# and the explicit 6th-order filter of rho w, by the reference's own parameter keys. The last two
+# cases keep the default schemes (but q_v's, in the last) and add the filter, so the compile-time
+# moist forms of the march kernel carry it.
 SCHEME_CASES = {
     "dry_quick_upwind_filter": ("cbl_dry", dict(advectionSelector=1, TKEAdvSelector=0, filterSelector=1)),
     "dry_hyb34_centred_filter": ("cbl_dry", dict(advectionSelector=2, b_hyb=0.4, TKEAdvSelector=6, filterSelector=1,
@@ -375,6 +375,9 @@ SCHEME_CASES = {
     "moist_upwind_quick": ("moist_hill", dict(advectionSelector=0, TKEAdvSelector=2, TKEAdvSelector_b_hyb=0.5,
                                               moistureAdvSelectorQv=1, moistureAdvSelectorQi=0)),
     "moist_default_filter": ("moist_hill", dict(filterSelector=1, filter_6th_coeff=0.12)),
+    # HYB34 for q_v with the other schemes at their defaults: the compile-time moist form with
+    # q_v's scheme fixed to HYB34 (the BOMEX tutorial's selectors)
+    "moist_hyb34_qv_filter": ("moist_hill", dict(moistureAdvSelectorQv=2, moistureAdvSelectorQv_b=0.2, filterSelector=1)),
 }
 
 

@@ -516,7 +516,10 @@ const char kCkptMagic[8] = {'F', 'E', 'B', '2', '0', '0', 'C', 'K'};
 
 extern "C" size_t fe_checkpoint_bytes(const fe_domain* d) {
   if (!d) return 0;
-  return sizeof(CkptHeader) + sizeof(float) * ((size_t)d->P.nf * (size_t)d->P.n + 11 * (size_t)d->P.n2);
+  // with slab-mean subsidence, also the third state buffer: the next forcing step's slab means read
+  // its halo cells (the previous step's last-stage input)
+  const size_t ns = (size_t)d->P.nf * (size_t)d->P.n;
+  return sizeof(CkptHeader) + sizeof(float) * (ns + 11 * (size_t)d->P.n2 + (d->P.lsfSub ? ns : 0));
 }
 
 extern "C" int fe_checkpoint_save(fe_domain* d, void* buf, size_t bytes) {
@@ -535,6 +538,7 @@ extern "C" int fe_checkpoint_save(fe_domain* d, void* buf, size_t bytes) {
   const size_t ns = (size_t)d->P.nf * (size_t)d->P.n, n2 = 11 * (size_t)d->P.n2;
   CU(cudaMemcpyAsync(f, d->st[0], ns * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
   CU(cudaMemcpyAsync(f + ns, d->surf, n2 * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
+  if (d->P.lsfSub) CU(cudaMemcpyAsync(f + ns + n2, d->st[2], ns * sizeof(float), cudaMemcpyDeviceToHost, d->stream));
   CU(cudaStreamSynchronize(d->stream));
   return FE_OK;
 }
@@ -556,6 +560,10 @@ extern "C" int fe_checkpoint_load(fe_domain* d, const void* buf, size_t bytes) {
   CU(cudaMemcpyAsync(d->surf, f + ns, n2 * sizeof(float), cudaMemcpyHostToDevice, d->stream));
   int rc = finish_state(d);
   if (rc) return rc;
+  if (d->P.lsfSub) {
+    CU(cudaMemcpyAsync(d->st[2], f + ns + n2, ns * sizeof(float), cudaMemcpyHostToDevice, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+  }
   return fe_set_clock(d, h.simTime, h.simIt);
 }
 

@@ -211,7 +211,9 @@ void *fe_ensemble_stream(fe_ensemble *e);
 int fe_ensemble_destroy(fe_ensemble *e);
 
 /* Checkpoint / resume: the prognostic state, the 11 surface planes and the clock in one host
- * buffer of fe_checkpoint_bytes() bytes (a header checks the domain shape on load). Loading
+ * buffer of fe_checkpoint_bytes() bytes (a header checks the domain shape on load); with
+ * large-scale subsidence (lsf_horMnSubTerms = 1) also the previous step's last-stage input,
+ * whose halo values the next slab means read. Loading
  * into a domain with the same grid and base state and advancing repeats the run that wrote it
  * bit for bit (the reference restarts through its netCDF inFile, io_netcdf.c:106-300). */
 size_t fe_checkpoint_bytes(const fe_domain *d);

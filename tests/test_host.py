@@ -102,3 +102,42 @@ def test_moisture_profile(fe):
     np.testing.assert_allclose(qv, expect, rtol=1e-5)
     assert np.all(q[1] == 0.0)
     host.cleanup()
+
+
+
+def test_configuration_checks_of_the_optional_physics(fe):
+    """fe_create validates a configuration before it looks for a device, so on a machine without
+    one an accepted configuration fails only with FE_ERR_NO_DEVICE (7). Every advection selector,
+    the explicit filter and the large-scale forcing are accepted; out-of-range selectors, an
+    interval below half a step and molecular diffusion are refused (FE_ERR_CONFIG, 2) by name."""
+    import ctypes
+
+    eng = fe.load(rebuild=False)["engine"]
+    host = fe.cases.setup_host("cbl_moist_hill", 8, 6, 6)
+    base = host.config()
+    host.cleanup()
+
+    def create(**kw):
+        cfg = type(base).from_buffer_copy(base)
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        h = ctypes.c_void_p()
+        rc = eng.fe_create(ctypes.byref(cfg), 0, ctypes.byref(h))
+        msg = eng.fe_last_error().decode()
+        if rc == 0:
+            eng.fe_destroy(h)
+        return rc, msg
+
+    accepted = [dict(advectionSelector=s) for s in range(7)] + [dict(TKEAdvSelector=s) for s in range(7)]
+    accepted += [dict(moistureAdvSelectorQv=s) for s in range(7)] + [dict(moistureAdvSelectorQi=s) for s in range(3)]
+    accepted += [dict(filterSelector=1, filter_6th_coeff=0.12), dict(lsfSelector=1, lsf_horMnSubTerms=1, lsf_freq=1.0)]
+    for kw in accepted:
+        rc, msg = create(**kw)
+        assert rc in (0, 7), (kw, rc, msg)
+    refused = [(dict(advectionSelector=7), "advectionSelector"), (dict(moistureAdvSelectorQi=3), "moistureAdvSelectorQi"),
+               (dict(filterSelector=2), "filterSelector"), (dict(filterSelector=1, filter_6th_coeff=1.5), "filter_6th_coeff"),
+               (dict(lsfSelector=1, lsf_freq=0.01), "lsf_freq"), (dict(diffusionSelector=1), "diffusion"),
+               (dict(b_hyb=1.5), "b_hyb")]
+    for kw, name in refused:
+        rc, msg = create(**kw)
+        assert rc == 2 and name in msg, (kw, rc, msg)

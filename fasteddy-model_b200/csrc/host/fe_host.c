@@ -1029,6 +1029,12 @@ int fe_host_write_netcdf(const char *path, int tstep) {
     return -1;
   }
   nreg = output_registry(reg, names);
+  /* the classic container records each variable's size in 32 bits */
+  if (4 * (uint64_t)Nx * Ny * Nz > 0xFFFFFFFCull) {
+    snprintf(g_msg, sizeof(g_msg), "fe_host_write_netcdf: a %dx%dx%d field exceeds the classic container's 4 GiB "
+             "variable size; use fe_host_write_binary", Nx, Ny, Nz);
+    return -1;
+  }
   if (!path || !path[0]) {
     snprintf(fname, sizeof(fname), "%s%s.%d", g_outPath, g_outFileBase, tstep);
     path = fname;

@@ -68,6 +68,39 @@ def ensemble_specs(n: int = 64, seed: int = 2024) -> list[tuple[int, int, int, f
     return out
 
 
+def case_text_module():
+    """The parameter-file writer (fasteddy-model_b200/cases.py) loaded on its own: plain Python
+    text generation, so the reference arm maps none of this repository's native libraries and
+    imports nothing of its package."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("fe_case_text", os.path.join(ROOT, "fasteddy-model_b200", "cases.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def hill_topofile_bytes(nx: int, ny: int, dx: float, dy: float, height: float, halfwidth: float) -> bytes:
+    """The Gaussian hill h = height * 2^-(r/halfwidth)^2 (r from cell centres to the domain
+    centre) in the reference's topoFile format (grid.c:313-326): int Nx, int Ny, float[Ny][Nx]."""
+    import numpy as np
+
+    x = (np.arange(nx) + 0.5) * dx - 0.5 * nx * dx
+    y = (np.arange(ny) + 0.5) * dy - 0.5 * ny * dy
+    r = np.sqrt(x[:, None] ** 2 + y[None, :] ** 2) / halfwidth
+    h = (height * np.power(2.0, -r * r)).astype(np.float32)  # [i][j]
+    return np.array([nx, ny], np.int32).tobytes() + np.ascontiguousarray(h.T).tobytes()
+
+
+def case_config(case: str, world: int) -> dict:
+    """The `config` of a bench line: the workload only, identical in both arms."""
+    key, nx, ny, nz, terrain, nprog, desc = CASES[case]
+    text = case_text_module()
+    return {"workload": desc, "cells": nx * ny * nz, "prognostic_fields": nprog, "dt_s": float(text.DT_STABLE),
+            "parallelism": f"replicas{world}",
+            "l2": f"state {4 * nprog * (nx + 6) * (ny + 6) * (nz + 6) / 1e9:.2f} GB per copy >> 126 MB L2, no flush needed"}
+
+
 def graph_warmup(w: int) -> int:
     """Untimed warm-up steps: at least w, rounded up to whole 8-step graph batches, so that the
     engine's CUDA graph is captured and instantiated before the timed region."""
@@ -354,9 +387,8 @@ def run_ours(args, rank: int, world: int, local: int) -> dict | None:
         "metric": "RK3 cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "cells": cells, "prognostic_fields": nprog, "dt_s": float(cfg.dt),
-                   "parallelism": f"replicas{world}", "l2": "state 4*8*N bytes >> 126 MB L2, no flush needed",
-                   "warmup_steps_run": warm, "stage_kernel": shape},
+        "config": case_config(args.case, world),
+        "warmup_steps_run": warm, "stage_kernel": shape,
         "e2e": {"value": whole_job_rate(cells, args.steps, e2e_s, world), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "path": "cuda_timeIntCommence (drop-in C ABI), host buffers, one batch of K steps"},
@@ -472,25 +504,36 @@ def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
 
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, rank: int, world: int) -> dict | None:
+    """The reference's own CUDA build (oracle/_ref/fe_ref_harness, compiled from the reference
+    sources for sm_100a) on the same case through its own cuda_timeIntCommence, from its own
+    initial state: its grid from the case's topoFile, its base state and its theta
+    perturbations; the reference cannot start moisture without a netCDF file, so the harness
+    sets the case's q_v profile in C. Nothing of this repository's package or native libraries
+    is loaded here. Only rank 0 runs it (a single process)."""
     if rank != 0:
         return None
+    if args.case == ENSEMBLE_CASE:
+        return {"impl": "reference", "unavailable": "the reference has no ensemble launcher (one domain per process)"}
     key, nx, ny, nz, terrain, nprog, desc = CASES[args.case]
     base = {"metric": "RK3 cell-updates/s", "unit": "cell-updates/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "cells": nx * ny * nz, "parallelism": "single process"}}
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": case_config(args.case, 1)}
     try:
         from oracle import refrun
         if not refrun.available():
             from oracle import build_ref
             build_ref.build()
-        fe = importlib.import_module("fasteddy-model_b200")
-        host = fe.cases.setup_host(key, nx, ny, nz)
-        inp = host.inputs()
-        text = fe.cases.param_text(key, nx, ny, nz)
+        text_mod = case_text_module()
+        files, topo = {}, ""
+        if terrain:
+            files["hill.topo"] = hill_topofile_bytes(nx, ny, 20.0, 20.0, text_mod.HILL_HEIGHT, text_mod.HILL_HALFWIDTH)
+            topo = "./hill.topo"
+        text = text_mod.param_text(key, nx, ny, nz, topo=topo)
+        qv = None
+        if key in ("cbl_moist_hill", "bomex"):
+            qv = "qv:%g,%g,%g" % (text_mod.QV_SFC, text_mod.QV_TOP, text_mod.QV_ZTOP)
         with ClockSampler(0) as clk:
-            t = refrun.time_steps(text, inp, args.steps)
-        host.cleanup()
+            t = refrun.time_steps(text, None, args.steps, qv=qv, files=files)
     except Exception as exc:  # the reference cannot run here: report why
         return {"impl": "reference", "unavailable": f"{type(exc).__name__}: {str(exc).splitlines()[0][:200]}"}
     ms = t["ms_per_step"]
@@ -500,8 +543,9 @@ def run_reference(args, rank: int, world: int) -> dict | None:
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 0, "kind": "reference",
                          "sample": f"reference CUDA build (oracle/_ref, sm_100a) on the B200 through its own "
-                                   f"cuda_timeIntCommence: ({2 * args.steps}-step batch - {args.steps}-step batch)/"
-                                   f"{args.steps}; the reference has no CPU implementation of this path"},
+                                   f"cuda_timeIntCommence, its own initial state: ({2 * args.steps}-step batch - "
+                                   f"{args.steps}-step batch)/{args.steps}; the reference has no CPU implementation "
+                                   f"of this path"},
         "clocks": clk.summary(),
         "reference_timing": t,
     })

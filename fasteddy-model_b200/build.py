@@ -54,11 +54,30 @@ def build(verbose: bool = False) -> dict[str, str]:
         "host": os.path.join(OUT, "libfe_host.so"),
     }
     hdr = [os.path.join(INC, "fasteddy_b200.h")]
-    eng_src = [os.path.join(ENGINE_DIR, f) for f in ("fe_engine.cu", "fe_noalloc.cu", "fe_learn.cu")]
+    eng_src = _sources(ENGINE_DIR, (".cu",))
     eng_deps = eng_src + _sources(ENGINE_DIR, (".cuh", ".h")) + hdr
     if _stale(libs["engine"], eng_deps):
-        cmd = [_nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-               "-I" + INC, "-I" + ENGINE_DIR, "-o", libs["engine"], *eng_src, "-lcudart"]
+        # one object per translation unit, compiled concurrently (the stage kernel's instantiations
+        # are split by RK stage over fe_march_s*.cu), then one shared library
+        objdir = os.path.join(OUT, "obj")
+        os.makedirs(objdir, exist_ok=True)
+        procs, objs = [], []
+        for src in eng_src:
+            obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+            objs.append(obj)
+            cmd = [_nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC,
+                   "-I" + ENGINE_DIR, "-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+        errors = []
+        for cmd, pr in procs:
+            out, _ = pr.communicate()
+            if pr.returncode != 0:
+                errors.append(" ".join(cmd) + "\n" + out)
+        if errors:
+            raise RuntimeError("build step failed:\n" + "\n".join(errors))
+        cmd = [_nvcc(), *NVCC_ARCH, "-shared", "-o", libs["engine"], *objs, "-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         _run(cmd)

@@ -143,24 +143,13 @@ BOMEX = dict(moistureAdvSelectorQv=2, moistureCond=3, moistureCondBasePres=1, fi
 DT_STABLE = 0.025
 
 
-def exact_tiling(n_halo: int) -> int:
-    """Largest divisor of a halo-inclusive extent that fits a thread block dimension."""
-    for t in range(min(n_halo, 128), 0, -1):
-        if n_halo % t == 0:
-            return t
-    return 1
-
-
 def exact_tb(ny: int, nz: int, max_threads: int = 256) -> tuple[int, int]:
-    """(tBy, tBz) dividing the halo-inclusive extents exactly; at most `max_threads`
-    threads so the reference's register-heavy kernels can launch."""
-    tbz = exact_tiling(nz + 6)
-    while tbz > max_threads:
-        tbz = exact_tiling(tbz - 1) if (nz + 6) % (tbz - 1) == 0 else tbz - 1
-    tby = 1
-    for t in range(1, ny + 7):
-        if (ny + 6) % t == 0 and t * tbz <= max_threads:
-            tby = t
+    """(tBy, tBz) dividing the halo-inclusive extents exactly: tBz the largest divisor of Nz+6
+    within CUDA's 64-thread limit on a block's z extent, tBy the largest divisor of Ny+6 that
+    keeps the block at most `max_threads` threads (the reference's register-heavy kernels)."""
+    nzh, nyh = nz + 6, ny + 6
+    tbz = max(t for t in range(1, min(nzh, 64) + 1) if nzh % t == 0)
+    tby = max(t for t in range(1, nyh + 1) if nyh % t == 0 and t * tbz <= max_threads)
     return tby, tbz
 
 

@@ -26,8 +26,10 @@
 #include "fasteddy_b200.h"
 #include "fe_kernels.cuh"
 #include "fe_march.cuh"
+#include "fe_march_launch.cuh"
 #include "fe_learn.h"
 #include "fe_sgs.cuh"
+#include "fe_config_phys.cuh"
 
 using fe::Phys;
 using fe::Ptrs;
@@ -80,6 +82,7 @@ struct fe_domain {
   int graphSteps = 0;
   long long launches = 0;
   size_t bytes = 0;
+  bool captureFrhs = false;          // keep the last-stage tendencies of the last step of an advance
 };
 
 struct fe_ensemble {
@@ -158,7 +161,8 @@ extern "C" void fe_config_derive(fe_config* c, float lat) {
   }
 }
 
-static int check_config(const fe_config* c) {
+extern "C" int fe_check_config(const fe_config* c) {
+  if (!c) return set_err(FE_ERR_ARG, "NULL configuration");
   if (c->Nh != 3) return set_err(FE_ERR_CONFIG, "Nh must be 3");
   if (c->Nx < 3 || c->Ny < 3 || c->Nz < 2) return set_err(FE_ERR_CONFIG, "need Nx,Ny >= 3 and Nz >= 2");
   if (c->hydroBCs != 2) return set_err(FE_ERR_CONFIG, "only hydroBCs = 2 (periodic horizontal, ABL vertical)");
@@ -197,74 +201,7 @@ static int check_config(const fe_config* c) {
   return FE_OK;
 }
 
-static void make_phys(fe_domain* d) {
-  const fe_config& c = d->cfg;
-  Phys& P = d->P;
-  std::memset(&P, 0, sizeof(P));
-  P.Nx = c.Nx; P.Ny = c.Ny; P.Nz = c.Nz;
-  P.nxh = c.Nx + 6; P.nyh = c.Ny + 6; P.nzh = c.Nz + 6;
-  P.sj = P.nzh;
-  P.si = P.nyh * P.nzh;
-  P.n = (long long)P.nxh * P.nyh * P.nzh;
-  P.n2 = (long long)P.nxh * P.nyh;
-  P.iMin = 3; P.iMax = c.Nx + 3; P.jMin = 3; P.jMax = c.Ny + 3; P.kMin = 3; P.kMax = c.Nz + 3;
-  P.dX = c.dX; P.dY = c.dY; P.dZ = c.dZ;
-  P.dXi = 1.0f / c.dX; P.dYi = 1.0f / c.dY; P.dZi = 1.0f / c.dZ;
-  P.dt = c.dt;
-  P.itRestart = c.simTime_itRestart;
-  P.turb = c.turbulenceSelector > 0;
-  P.tke = P.turb && c.TKESelector > 0;
-  P.ntke = P.tke ? 1 : 0;
-  P.moist = c.moistureSelector > 0;
-  P.nmoist = P.moist ? c.moistureNvars : 0;
-  P.nf = 5 + P.ntke + P.nmoist;
-  P.pgf = c.pgfSelector > 0;
-  P.buoy = c.buoyancySelector > 0;
-  P.cor = c.coriolisSelector > 0;
-  P.advSel = c.advectionSelector;
-  P.tkeAdvSel = c.TKEAdvSelector;
-  P.qvAdvSel = c.moistureAdvSelectorQv;
-  P.qiAdvSel = c.moistureAdvSelectorQi;
-  P.qlSch = fe::ql_scheme(c.moistureAdvSelectorQi);
-  P.bHyb = c.b_hyb; P.tkeBHyb = c.TKEAdvSelector_b_hyb; P.qvB = c.moistureAdvSelectorQv_b;
-  P.filt = c.filterSelector > 0;
-  P.filtCoef = fe::filter_coef(c.filter_6th_coeff, c.dt);
-  P.lsf = c.lsfSelector > 0;
-  P.lsfSub = P.lsf && c.lsf_horMnSubTerms == 1;
-  P.lsfN = P.lsf ? (int)roundf(c.lsf_freq / c.dt) : 1;  // as the reference rounds it (cuda_hydroCoreDevice.cu:402-404)
-  P.lsfFac = (float)P.lsfN;
-  {
-    const float w[5] = {c.lsf_w_surf, c.lsf_w_lev1, c.lsf_w_lev2, c.lsf_w_zlev1, c.lsf_w_zlev2};
-    const float th[5] = {c.lsf_th_surf, c.lsf_th_lev1, c.lsf_th_lev2, c.lsf_th_zlev1, c.lsf_th_zlev2};
-    const float qv[5] = {c.lsf_qv_surf, c.lsf_qv_lev1, c.lsf_qv_lev2, c.lsf_qv_zlev1, c.lsf_qv_zlev2};
-    for (int m = 0; m < 5; m++) { P.lsfW[m] = w[m]; P.lsfTh[m] = th[m]; P.lsfQv[m] = qv[m]; }
-  }
-  P.c_s = c.c_s; P.c_k = c.c_k;
-  P.surf = c.surflayerSelector;
-  P.surfStab = c.surflayer_stab;
-  P.idealSine = c.surflayer_idealsine;
-  P.qskinInput = c.surflayer_qskin_input;
-  P.z0 = c.surflayer_z0; P.z0t = c.surflayer_z0t; P.wth = c.surflayer_wth; P.tr = c.surflayer_tr;
-  P.wq = c.surflayer_wq; P.qr = c.surflayer_qr;
-  P.idealTs = c.surflayer_ideal_ts; P.idealTe = c.surflayer_ideal_te; P.idealAmp = c.surflayer_ideal_amp;
-  P.idealQts = c.surflayer_ideal_qts; P.idealQte = c.surflayer_ideal_qte; P.idealQamp = c.surflayer_ideal_qamp;
-  P.moistSGS = c.moistureSGSturb;
-  P.moistCond = c.moistureCond;
-  P.condBasePres = c.moistureCondBasePres;
-  P.condTscale = c.moistureCondTscale;
-  // cadences as the reference computes them (cuda_hydroCoreDevice.cu:382, cuda_surfaceLayerDevice.cu:128)
-  P.mpFreq = std::max(1, (int)roundf(fmaxf(c.moistureMPcallTscale, c.dt) / c.dt));
-  P.tempFreq = std::max(1, (int)roundf((float)(10.0 / c.dt)));
-  P.damp = c.dampingLayerSelector > 0;
-  P.dampDepth = c.dampingLayerDepth;
-  P.U_g = c.U_g; P.V_g = c.V_g; P.z_Ug = c.z_Ug; P.z_Vg = c.z_Vg; P.Ug_grad = c.Ug_grad; P.Vg_grad = c.Vg_grad;
-  P.fHorz = c.corioConstHorz; P.fVert = c.corioConstVert; P.fLS = c.corioLS_fact;
-  P.oneRK = c.physics_oneRKonly;
-  P.tempGrnd = c.temp_grnd; P.presGrnd = c.pres_grnd;
-  P.R_gas = c.R_gas; P.R_vapor = c.R_vapor; P.Rv_Rg = c.Rv_Rg; P.cp_gas = c.cp_gas; P.cv_gas = c.cv_gas;
-  P.g = c.accel_g; P.R_cp = c.R_cp; P.cp_R = c.cp_R; P.cp_cv = c.cp_cv; P.p0 = c.refPressure; P.kappa = c.kappa;
-  P.L_v = c.L_v;
-}
+static void make_phys(fe_domain* d) { fe::phys_from_config(d->cfg, d->P); }
 
 static int dev_alloc(fe_domain* d, float** p, size_t nfloats) {
   cudaError_t e = cudaMalloc((void**)p, nfloats * sizeof(float));
@@ -305,7 +242,7 @@ static int march_attrs();
 extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   if (!cfg || !out) return set_err(FE_ERR_ARG, "NULL argument");
   *out = nullptr;
-  int rc = check_config(cfg);
+  int rc = fe_check_config(cfg);
   if (rc) return rc;
   int ndev = fe_device_count();
   if (ndev <= 0) return set_err(FE_ERR_NO_DEVICE, "no CUDA device visible");
@@ -681,76 +618,21 @@ static bool stage_has_physics(const fe_domain* d, int stage) { return d->P.oneRK
 
 // Dynamic shared memory limits of the march kernels (three plane buffers exceed the 48 KB
 // default at 8 rows); set on the current device before any launch or capture.
-template <int STAGE, int MODE>
-static cudaError_t march_attrs_one() {
-  cudaError_t e = cudaSuccess;
-  auto set = [&](const void* f, int bytes) {
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  };
-  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_ANY>, fe::MarchTile<8>::SMEM_BYTES);
-  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_DRY>, fe::MarchTile<8>::SMEM_BYTES);
-  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST>, fe::MarchTile<8>::SMEM_BYTES);
-  set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST34>, fe::MarchTile<8>::SMEM_BYTES);
-  if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
-    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST, 0>, fe::MarchTile<8>::SMEM_BYTES);
-    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST, 1>, fe::MarchTile<8>::SMEM_BYTES);
-    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST34, 0>, fe::MarchTile<8>::SMEM_BYTES);
-    set((const void*)fe::k_march<STAGE, MODE, 8, fe::FL_MOIST34, 1>, fe::MarchTile<8>::SMEM_BYTES);
-  }
-  set((const void*)fe::k_march<STAGE, MODE, 4, fe::FL_ANY>, fe::MarchTile<4>::SMEM_BYTES);
-  return e;
-}
 static int march_attrs() {
-  cudaError_t e = march_attrs_one<0, fe::MODE_COMMIT>();
-  if (e == cudaSuccess) e = march_attrs_one<1, fe::MODE_COMMIT>();
-  if (e == cudaSuccess) e = march_attrs_one<2, fe::MODE_COMMIT>();
-  if (e == cudaSuccess) e = march_attrs_one<0, fe::MODE_FRHS>();
-  if (e == cudaSuccess) e = march_attrs_one<1, fe::MODE_FRHS>();
-  if (e == cudaSuccess) e = march_attrs_one<2, fe::MODE_FRHS>();
+  cudaError_t e = fe::march_set_attrs<0, fe::MODE_COMMIT>();
+  if (e == cudaSuccess) e = fe::march_set_attrs<1, fe::MODE_COMMIT>();
+  if (e == cudaSuccess) e = fe::march_set_attrs<2, fe::MODE_COMMIT>();
+  if (e == cudaSuccess) e = fe::march_set_attrs<0, fe::MODE_FRHS>();
+  if (e == cudaSuccess) e = fe::march_set_attrs<1, fe::MODE_FRHS>();
+  if (e == cudaSuccess) e = fe::march_set_attrs<2, fe::MODE_FRHS>();
   if (e != cudaSuccess) return set_err(FE_ERR_CUDA, std::string("march kernel attributes: ") + cudaGetErrorString(e));
   return FE_OK;
-}
-
-// Flavour of the march kernel that matches the configuration (fe_march.cuh).
-static int march_flavor(const Phys& P) {
-  if (P.pgf && P.tke && P.ntke == 1 && P.advSel == 3 && P.tkeAdvSel == 3 && P.oneRK == 1) {
-    if (P.nmoist == 0) return fe::FL_DRY;
-    if (P.nmoist == 2 && P.qlSch == fe::ADV_WENO5) {
-      if (P.qvAdvSel == 3) return fe::FL_MOIST;
-      if (P.qvAdvSel == 2) return fe::FL_MOIST34;
-    }
-  }
-  return fe::FL_ANY;
-}
-
-template <int STAGE, int MODE, int TJ, int FL, int MP = -1>
-static void launch_march(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
-                         const float* pcur, float* pnxt, float* frhs) {
-  const Phys& P = d->P;
-  const int ni = d->mni;
-  dim3 g((P.Nz + fe::MK - 1) / fe::MK, (P.Ny + TJ - 1) / TJ, (P.Nx + ni - 1) / ni);
-  fe::k_march<STAGE, MODE, TJ, FL, MP><<<g, dim3(fe::MK, TJ), fe::MarchTile<TJ>::SMEM_BYTES, s>>>(
-      P, d->Q, cur, base, nxt, pcur, pnxt, frhs, ni);
 }
 
 // The moist flavour's last stage as a pair (k_march MP = 0 then 1): the kernel that runs in the
 // steps without saturation adjustment carries none of its code.
 static bool split_last_stage(const fe_domain* d) {
-  if (d->kind != FE_KERNEL_MARCH || d->mtj != 8) return false;
-  const int fl = march_flavor(d->P);
-  return fl == fe::FL_MOIST || fl == fe::FL_MOIST34;
-}
-
-// A moist flavour's stage kernel: the last committing stage as its MP pair.
-template <int STAGE, int MODE, int FL>
-static void launch_moist(const fe_domain* d, cudaStream_t s, const float* cur, const float* base, float* nxt,
-                         const float* pcur, float* pnxt, float* frhs) {
-  if (STAGE == 2 && MODE == fe::MODE_COMMIT) {
-    launch_march<STAGE, MODE, 8, FL, 0>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-    launch_march<STAGE, MODE, 8, FL, 1>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-  } else {
-    launch_march<STAGE, MODE, 8, FL>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-  }
+  return d->kind == FE_KERNEL_MARCH && fe::march_split_last_stage(d->P, d->mtj);
 }
 
 // Launch the fused stage kernel of stage STAGE in the domain's chosen form.
@@ -759,16 +641,7 @@ static void launch_stage(const fe_domain* d, cudaStream_t s, const float* cur, c
                          const float* pcur, float* pnxt, float* frhs) {
   const Phys& P = d->P;
   if (d->kind == FE_KERNEL_MARCH) {
-    if (d->mtj == 4) {
-      launch_march<STAGE, MODE, 4, fe::FL_ANY>(d, s, cur, base, nxt, pcur, pnxt, frhs);
-    } else {
-      switch (march_flavor(P)) {
-        case fe::FL_DRY: launch_march<STAGE, MODE, 8, fe::FL_DRY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
-        case fe::FL_MOIST: launch_moist<STAGE, MODE, fe::FL_MOIST>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
-        case fe::FL_MOIST34: launch_moist<STAGE, MODE, fe::FL_MOIST34>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
-        default: launch_march<STAGE, MODE, 8, fe::FL_ANY>(d, s, cur, base, nxt, pcur, pnxt, frhs); break;
-      }
-    }
+    fe::march_launch<STAGE, MODE>(P, d->Q, d->mtj, d->mni, s, cur, base, nxt, pcur, pnxt, frhs);
   } else {
     fe::k_stage<STAGE, MODE><<<stage_grid(d), dim3(d->tk, d->tj, d->ti), 0, s>>>(P, d->Q, cur, base, nxt, pcur, pnxt, frhs);
   }
@@ -783,8 +656,9 @@ static int launch_slab_means(const fe_domain* d, cudaStream_t s, const float* cu
   return 2;
 }
 
-// Enqueue one RK3 step on stream s (no host synchronisation; graph-capturable).
-static void enqueue_step(fe_domain* d, cudaStream_t s) {
+// Enqueue one RK3 step on stream s (no host synchronisation; graph-capturable). With `frhs`,
+// the last stage also stores its tendencies there (the reference's Frhs after a step).
+static void enqueue_step(fe_domain* d, cudaStream_t s, float* frhs = nullptr) {
   const Phys& P = d->P;
   const Ptrs& Q = d->Q;
   float *A = d->st[0], *B = d->st[1], *C = d->st[2];
@@ -797,7 +671,7 @@ static void enqueue_step(fe_domain* d, cudaStream_t s) {
   if (physPrep && stage_has_physics(d, 1)) d->launches += launch_physics(d, s, B, 1);
   launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
   if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2);
-  launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], nullptr);
+  launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], frhs);
   fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
   d->launches += 4 + (split_last_stage(d) ? 1 : 0);
 }
@@ -837,7 +711,13 @@ extern "C" int fe_advance(fe_domain* d, int nsteps) {
   if (!d || nsteps < 0) return set_err(FE_ERR_ARG, "bad argument");
   if (!d->haveState) return set_err(FE_ERR_STATE, "state not set");
   CU(cudaSetDevice(d->device));
-  int left = nsteps;
+  const bool capture = d->captureFrhs && nsteps > 0;
+  if (capture && !d->frhs) {
+    int rc = dev_alloc(d, &d->frhs, (size_t)d->P.n * d->P.nf);
+    if (rc) return rc;
+  }
+  // with tendency capture the last step runs on its own, its last stage storing the tendencies
+  int left = capture ? nsteps - 1 : nsteps;
   if (left >= kGraphSteps) {
     if (!d->graph) {
       int rc = build_graph(d);
@@ -850,6 +730,7 @@ extern "C" int fe_advance(fe_domain* d, int nsteps) {
     }
   }
   for (; left > 0; left--) enqueue_step(d, d->stream);
+  if (capture) enqueue_step(d, d->stream, d->frhs);
   CU(cudaGetLastError());
   for (int s = 0; s < nsteps; s++) {
     d->simTime = d->simTime + d->P.dt;
@@ -943,6 +824,27 @@ extern "C" int fe_get_frhs(fe_domain* d, float* hydroFrhs, float* sgstkeFrhs, fl
   if (!rc && P.ntke) rc = d2h(d, sgstkeFrhs, d->frhs + 5 * n, n);
   if (!rc && P.nmoist) rc = d2h(d, moistFrhs, d->frhs + (5 + P.ntke) * n, n * P.nmoist);
   if (!rc) rc = d2h(d, taus, d->Q.tau, 9 * n);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(d->stream));
+  return FE_OK;
+}
+
+extern "C" int fe_set_forcing_capture(fe_domain* d, int on) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  d->captureFrhs = on != 0;
+  return FE_OK;
+}
+
+extern "C" int fe_get_sgs_fluxes(fe_domain* d, float* taus, float* moistTaus) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  const Phys& P = d->P;
+  const size_t n = (size_t)P.n;
+  if (taus && !P.turb) return set_err(FE_ERR_STATE, "no SGS stresses without turbulenceSelector");
+  if (moistTaus && !(P.turb && P.nmoist > 0 && P.moistSGS > 0))
+    return set_err(FE_ERR_STATE, "no moisture SGS fluxes in this configuration");
+  int rc = d2h(d, taus, d->Q.tau, 9 * n);
+  if (!rc) rc = d2h(d, moistTaus, d->Q.mtau, 3 * n * (size_t)P.nmoist);
   if (rc) return rc;
   CU(cudaStreamSynchronize(d->stream));
   return FE_OK;

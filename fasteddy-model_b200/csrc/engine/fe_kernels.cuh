@@ -21,17 +21,17 @@ namespace fe {
 constexpr int MODE_COMMIT = 0;
 constexpr int MODE_FRHS = 1;
 
-__global__ void k_consts(float R_gas, float p0, float R_cp, float presGrnd, float* out) {
+static __global__ void k_consts(float R_gas, float p0, float R_cp, float presGrnd, float* out) {
   out[0] = R_gas / powf(p0, R_cp);
   out[1] = powf((p0 / presGrnd), R_cp);
 }
 
-__global__ void k_delta(Phys P, long long n, const float* __restrict__ D, float* __restrict__ delta) {
+static __global__ void k_delta(Phys P, long long n, const float* __restrict__ D, float* __restrict__ delta) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) delta[t] = grid_scale_of(P, D[t]);
 }
 
-__global__ void k_pbs(long long n, const float* __restrict__ thBS, float c1, float cp_cv, float* __restrict__ pBS) {
+static __global__ void k_pbs(long long n, const float* __restrict__ thBS, float c1, float cp_cv, float* __restrict__ pBS) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) pBS[t] = powf(thBS[t] * c1, cp_cv);
 }
@@ -42,7 +42,7 @@ __device__ __forceinline__ int wrap_j(const Phys& P, int j) { return j < P.jMin 
 // Boundary value of field f at halo cell (i,j,k): the vertical boundary rule applied on
 // the periodic source column, i.e. the reference's Commence BCs (cuda_hydroCoreDevice.cu:
 // 469-550) with every read of the current stage.
-__global__ void k_fill(Phys P, Ptrs Q, float* st) {
+static __global__ void k_fill(Phys P, Ptrs Q, float* st) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= P.n) return;
   const int k = (int)(t % P.nzh);
@@ -73,7 +73,7 @@ __global__ void k_fill(Phys P, Ptrs Q, float* st) {
 
 // Perturbation pressure over the halo-inclusive block (cuda_pressureDevice.cu:53-113):
 // levels 1..kMin-1 use the kMin cell, levels >= kMax use kMax-1, level 0 its own cell.
-__global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, float* __restrict__ pres) {
+static __global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, float* __restrict__ pres) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= P.n) return;
   const int k = (int)(t % P.nzh);
@@ -109,7 +109,7 @@ __device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, cons
 // ------------------------------------------------------------------ surface layer
 // Land-surface update and Monin-Obukhov iteration of one column (cuda_surfaceLayerDevice.cu:
 // 112-521). Writes tau31, tau32, tauTH3 (and the q_v flux) at kMin.
-__device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int stage) {
+static __device__ void surface_column(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int i, int j, int stage) {
   const long long c = (long long)i * P.si + (long long)j * P.sj + P.kMin;
   const long long ij = (long long)i * P.nyh + j;
   const bool moist = P.moist > 0 && P.nmoist > 0;
@@ -380,7 +380,7 @@ __device__ __forceinline__ void turb_cell(const Phys& P, const Ptrs& Q, const fl
 // One thread per cell of the ring i in [iMin-1,iMax], j in [jMin-1,jMax], k in [kMin-1,kMax]
 // (the reference's ring minus the i=iMax+1/j=jMax+1 cells, which nothing reads). The length
 // scale of the level below is recomputed by the same thread (no race on it).
-__global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+static __global__ void __launch_bounds__(256) k_turb(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
   const int k = P.kMin - 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = P.jMin - 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int i = P.iMin - 1 + blockIdx.z * blockDim.z + threadIdx.z;
@@ -423,7 +423,7 @@ struct TilePrims {
   __device__ __forceinline__ float qm(int m, int di, int dj, int dk) const { return at(6 + m, di, dj, dk); }
 };
 
-__global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+static __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
   __shared__ float tile[TP_F * TP_N];
   __shared__ float lsT[TT_I][TT_J][TT_K + 1];  // length scale, levels k0-1..k0+31
   __shared__ float seT[TT_I][TT_J][TT_K + 1];  // sqrt(e/rho), same levels
@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(256) k_turb_t(Phys P, Ptrs Q, const float* __r
 // eddy viscosity is zero by construction, so of its outputs only the vertical TKE flux is ever
 // read (by the transport term of the first level) and it is zero, which the zero-initialised
 // scratch already holds; its moisture gradients and length scale have no reader.
-__global__ void __launch_bounds__(256) k_turb_ring(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+static __global__ void __launch_bounds__(256) k_turb_ring(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nj = P.Ny + 2;
   if (t >= (long long)nj * (P.Nx + 2)) return;
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(256) k_turb_ring(Phys P, Ptrs Q, const float* 
 // Monin-Obukhov iteration would run on one lane of every warp holding the first level while the
 // other 31 lanes wait; here every lane works. It overwrites the same first-level components
 // (tau31, tau32, tauTH3, the q_v flux) the per-cell form's in-kernel call does.
-__global__ void __launch_bounds__(128) k_surface(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
+static __global__ void __launch_bounds__(128) k_surface(Phys P, Ptrs Q, const float* __restrict__ st, int stage) {
   const int j = P.jMin + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = P.iMin + blockIdx.y;
   if (j > P.jMax || i > P.iMax) return;
@@ -551,7 +551,7 @@ __device__ __forceinline__ void store_images(const Phys& P, float* __restrict__ 
 
 // ------------------------------------------------------------------ fused stage
 template <int STAGE, int MODE>
-__global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base,
+static __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base,
                                                float* __restrict__ nxt, const float* __restrict__ pcur,
                                                float* __restrict__ pnxt, float* __restrict__ frhs) {
   const int k = P.kMin + blockIdx.x * blockDim.x + threadIdx.x;
@@ -816,7 +816,8 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
   if (P.filt)
     F3 = __fadd_rn(F3, filter6_tend(mw[c - 3], mw[c - 2], mw[c - 1], mw[c], mw[c + 1], mw[c + 2], mw[c + 3], P.filtCoef));
 
-  if (MODE == MODE_FRHS) {
+  if (MODE == MODE_FRHS || (STAGE == 2 && frhs)) {
+    // tendencies only, or the last stage's tendencies kept beside its commit
     frhs[c] = F0;
     frhs[n + c] = F1;
     frhs[2 * n + c] = F2;
@@ -825,7 +826,7 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
     if (P.ntke) frhs[5 * n + c] = Fe;
     if (P.nmoist > 0) frhs[(5 + P.ntke) * n + c] = Fq0;
     if (P.nmoist > 1) frhs[(6 + P.ntke) * n + c] = Fq1;
-    return;
+    if (MODE == MODE_FRHS) return;
   }
 
   // WS2002 RK3 commit (cuda_RKschemes.cu:113-157) with the reference's rounding:
@@ -872,12 +873,12 @@ __global__ void __launch_bounds__(256) k_stage(Phys P, Ptrs Q, const float* __re
   if (atBot) store_images(P, pnxt, i, j, 0, level0_pressure(P, Q, c - k, P.nmoist, nq0), 0, false);
 }
 
-__global__ void k_clock(Ptrs Q, float dt) {
+static __global__ void k_clock(Ptrs Q, float dt) {
   *Q.clockIt = *Q.clockIt + 1;
   *Q.clockTime = *Q.clockTime + dt;
 }
 
-__global__ void k_nonfinite(Phys P, const float* __restrict__ st, unsigned long long* out) {
+static __global__ void k_nonfinite(Phys P, const float* __restrict__ st, unsigned long long* out) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned int cnt = 0;
   if (t < P.n) {
@@ -899,7 +900,7 @@ __global__ void k_nonfinite(Phys P, const float* __restrict__ st, unsigned long 
 // cells are read from `cur` (phi^n) and halo cells from `halo` (the buffer holding phi** with its
 // boundary images). Sums are FP64: each block accumulates its columns (thread = level) into
 // lsfPart[block][field][level]; k_slab_final adds the blocks in a fixed order.
-__global__ void k_slab_partial(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ halo,
+static __global__ void k_slab_partial(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ halo,
                                int force) {
   if (!force && !lsf_means_step(P, *Q.clockIt)) return;
   const long long cols = (long long)P.nxh * P.nyh;
@@ -924,7 +925,7 @@ __global__ void k_slab_partial(Phys P, Ptrs Q, const float* __restrict__ cur, co
   }
 }
 
-__global__ void k_slab_final(Phys P, Ptrs Q, int nblocks, int force) {
+static __global__ void k_slab_final(Phys P, Ptrs Q, int nblocks, int force) {
   if (!force && !lsf_means_step(P, *Q.clockIt)) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 5 * P.nzh) return;
@@ -934,7 +935,7 @@ __global__ void k_slab_final(Phys P, Ptrs Q, int nblocks, int force) {
 }
 
 // FP64 sums of the interior fields: warp shuffle, then one atomic per warp and field.
-__global__ void k_means(Phys P, const float* __restrict__ st, double* out) {
+static __global__ void k_means(Phys P, const float* __restrict__ st, double* out) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool in = false;
   if (t < P.n) {

@@ -25,6 +25,7 @@
 // same order, evaluated on the register/shared copies.
 #pragma once
 #include "fe_kernels.cuh"
+#include "fe_march_launch.cuh"
 
 namespace fe {
 
@@ -108,16 +109,7 @@ __device__ __forceinline__ float slot_b(const Phys& P, int s) {
   return 0.0f;
 }
 
-// Compile-time configurations ("flavours") of the march kernel. FL_ANY reads every selector at
-// run time; the others fix the field set and the advection schemes of the common cases (PGF on,
-// prognostic TKE, HYB56 for the hydro fields, TKE and q_v, WENO5 for q_l, SGS physics in the last
-// RK stage only), so the field loop has no run-time branches and the first two stages carry no
-// physics code. The host picks the flavour that matches the configuration.
-constexpr int FL_ANY = 0;
-constexpr int FL_DRY = 1;    // rho, rho u, rho v, rho w, rho theta, rho e
-constexpr int FL_MOIST = 2;  // ... plus rho q_v and rho q_l
-constexpr int FL_MOIST34 = 3;  // the moist set with HYB34 for q_v (the BOMEX tutorial's selectors)
-
+// Compile-time configurations ("flavours") of the march kernel: fe_march_launch.cuh.
 template <int FL>
 __device__ __forceinline__ bool f_on(const Phys& P, int s) {
   if constexpr (FL == FL_DRY) return s <= SL_E || s == SL_P;
@@ -678,6 +670,17 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
         if (nmoist > 0) frhs[(5 + ntke) * n + c] = F[SL_QV];
         if (nmoist > 1) frhs[(6 + ntke) * n + c] = F[SL_QL];
       } else {
+        if (STAGE == 2 && frhs) {
+          // the last stage's tendencies, kept when asked (the reference's Frhs after a step)
+          frhs[c] = F[0];
+          frhs[n + c] = F[1];
+          frhs[2 * n + c] = F[2];
+          frhs[3 * n + c] = F[3];
+          frhs[4 * n + c] = F[4];
+          if (ntke) frhs[5 * n + c] = F[SL_E];
+          if (nmoist > 0) frhs[(5 + ntke) * n + c] = F[SL_QV];
+          if (nmoist > 1) frhs[(6 + ntke) * n + c] = F[SL_QL];
+        }
         // WS2002 RK3 commit (cuda_RKschemes.cu:113-157), rounding as in the cell kernel
         auto rk = [&](float phi0, float Fv) -> float {
           if (STAGE == 0) return (float)fma((1.0 / 3.0) * (double)P.dt, (double)Fv, (double)phi0);

@@ -9,13 +9,15 @@
 // perturbation pressure, the last-stage SGS stresses, TKE fluxes, length scale, moisture
 // fluxes, the step clock) live in one file-scope __device__ array of FE_NOALLOC_SCRATCH_BYTES,
 // allocated once per GPU when the library is loaded and kept until exit. Its device
-// address is fetched with cudaGetSymbolAddress on the first call on each device (the name
-// of a __device__ array in host code is only a host-side stand-in, never a device address).
+// address is fetched with cudaGetSymbolAddress on every call, on the caller's current device
+// (the name of a __device__ array in host code is only a host-side stand-in, never a device
+// address).
 //
 // The kernels are the engine's own (fe_kernels.cuh), compiled into a private namespace of
 // this translation unit so they do not collide with the engine's copies.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -25,6 +27,7 @@
 
 namespace fe_noalloc_impl {
 #include "fe_kernels.cuh"
+#include "fe_config_phys.cuh"
 }  // namespace fe_noalloc_impl
 
 using fe_noalloc_impl::fe::Phys;
@@ -40,8 +43,6 @@ static constexpr size_t kScratchFloats = FE_NOALLOC_SCRATCH_BYTES / sizeof(float
 static __device__ __align__(256) float g_noalloc_scratch[kScratchFloats];
 
 namespace {
-constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
 thread_local std::string g_na_err;
 
 int na_err(int code, const std::string& m) {
@@ -54,92 +55,35 @@ __global__ void k_na_clock(int* it, float* t, int simIt, float simTime) {
   *t = simTime;
 }
 
-// Phys from a configuration: the same derivation as the engine's domain creation.
-void make_phys(const fe_config& c, Phys& P) {
-  std::memset(&P, 0, sizeof(P));
-  P.Nx = c.Nx; P.Ny = c.Ny; P.Nz = c.Nz;
-  P.nxh = c.Nx + 6; P.nyh = c.Ny + 6; P.nzh = c.Nz + 6;
-  P.sj = P.nzh;
-  P.si = P.nyh * P.nzh;
-  P.n = (long long)P.nxh * P.nyh * P.nzh;
-  P.n2 = (long long)P.nxh * P.nyh;
-  P.iMin = 3; P.iMax = c.Nx + 3; P.jMin = 3; P.jMax = c.Ny + 3; P.kMin = 3; P.kMax = c.Nz + 3;
-  P.dX = c.dX; P.dY = c.dY; P.dZ = c.dZ;
-  P.dXi = 1.0f / c.dX; P.dYi = 1.0f / c.dY; P.dZi = 1.0f / c.dZ;
-  P.dt = c.dt;
-  P.itRestart = c.simTime_itRestart;
-  P.turb = c.turbulenceSelector > 0;
-  P.tke = P.turb && c.TKESelector > 0;
-  P.ntke = P.tke ? 1 : 0;
-  P.moist = c.moistureSelector > 0;
-  P.nmoist = P.moist ? c.moistureNvars : 0;
-  P.nf = 5 + P.ntke + P.nmoist;
-  P.pgf = c.pgfSelector > 0;
-  P.buoy = c.buoyancySelector > 0;
-  P.cor = c.coriolisSelector > 0;
-  P.advSel = c.advectionSelector;
-  P.tkeAdvSel = c.TKEAdvSelector;
-  P.qvAdvSel = c.moistureAdvSelectorQv;
-  P.qiAdvSel = c.moistureAdvSelectorQi;
-  P.qlSch = K::ql_scheme(c.moistureAdvSelectorQi);
-  P.bHyb = c.b_hyb; P.tkeBHyb = c.TKEAdvSelector_b_hyb; P.qvB = c.moistureAdvSelectorQv_b;
-  P.c_s = c.c_s; P.c_k = c.c_k;
-  P.surf = c.surflayerSelector;
-  P.surfStab = c.surflayer_stab;
-  P.idealSine = c.surflayer_idealsine;
-  P.qskinInput = c.surflayer_qskin_input;
-  P.z0 = c.surflayer_z0; P.z0t = c.surflayer_z0t; P.wth = c.surflayer_wth; P.tr = c.surflayer_tr;
-  P.wq = c.surflayer_wq; P.qr = c.surflayer_qr;
-  P.idealTs = c.surflayer_ideal_ts; P.idealTe = c.surflayer_ideal_te; P.idealAmp = c.surflayer_ideal_amp;
-  P.idealQts = c.surflayer_ideal_qts; P.idealQte = c.surflayer_ideal_qte; P.idealQamp = c.surflayer_ideal_qamp;
-  P.moistSGS = c.moistureSGSturb;
-  P.moistCond = c.moistureCond;
-  P.condBasePres = c.moistureCondBasePres;
-  P.condTscale = c.moistureCondTscale;
-  const int mp = (int)roundf(fmaxf(c.moistureMPcallTscale, c.dt) / c.dt);
-  P.mpFreq = mp < 1 ? 1 : mp;
-  const int tf = (int)roundf((float)(10.0 / c.dt));
-  P.tempFreq = tf < 1 ? 1 : tf;
-  P.damp = c.dampingLayerSelector > 0;
-  P.dampDepth = c.dampingLayerDepth;
-  P.U_g = c.U_g; P.V_g = c.V_g; P.z_Ug = c.z_Ug; P.z_Vg = c.z_Vg; P.Ug_grad = c.Ug_grad; P.Vg_grad = c.Vg_grad;
-  P.fHorz = c.corioConstHorz; P.fVert = c.corioConstVert; P.fLS = c.corioLS_fact;
-  P.oneRK = c.physics_oneRKonly;
-  P.tempGrnd = c.temp_grnd; P.presGrnd = c.pres_grnd;
-  P.R_gas = c.R_gas; P.R_vapor = c.R_vapor; P.Rv_Rg = c.Rv_Rg; P.cp_gas = c.cp_gas; P.cv_gas = c.cv_gas;
-  P.g = c.accel_g; P.R_cp = c.R_cp; P.cp_R = c.cp_R; P.cp_cv = c.cp_cv; P.p0 = c.refPressure; P.kappa = c.kappa;
-  P.L_v = c.L_v;
-}
-
+// The engine's own validation (the checks fe_create applies), then this path's narrower set:
+// the per-cell stage kernel here has no explicit filter and no large-scale forcing, and its
+// advection is HYB56 (3) or WENO5 (5) for the hydro fields, TKE and q_v, WENO5 for q_l.
 int check(const fe_config& c) {
-  if (c.Nh != 3 || c.Nx < 3 || c.Ny < 3 || c.Nz < 2 || c.hydroBCs != 2 || !(c.dt > 0.0f))
-    return na_err(FE_ERR_CONFIG, "need Nh = 3, Nx,Ny >= 3, Nz >= 2, hydroBCs = 2, dt > 0");
+  int rc = fe_check_config(&c);
+  if (rc) return na_err(rc, fe_last_error());
   if (c.advectionSelector != 3 && c.advectionSelector != 5)
     return na_err(FE_ERR_CONFIG, "advectionSelector must be 3 or 5");
   if (c.turbulenceSelector > 0 && c.TKESelector > 0 && c.TKEAdvSelector != 3 && c.TKEAdvSelector != 5)
     return na_err(FE_ERR_CONFIG, "TKEAdvSelector must be 3 or 5");
-  if (c.diffusionSelector || c.filterSelector || c.lsfSelector)
-    return na_err(FE_ERR_CONFIG, "diffusion, filter and large-scale forcing are not on this path");
-  if (c.moistureSelector > 0 && (c.moistureNvars < 1 || c.moistureNvars > 2 ||
-                                 (c.moistureAdvSelectorQv != 3 && c.moistureAdvSelectorQv != 5) ||
+  if (c.filterSelector || c.lsfSelector)
+    return na_err(FE_ERR_CONFIG, "the explicit filter and large-scale forcing are not on this path");
+  if (c.moistureSelector > 0 && ((c.moistureAdvSelectorQv != 3 && c.moistureAdvSelectorQv != 5) ||
                                  (c.moistureNvars > 1 && c.moistureAdvSelectorQi != 2)))
     return na_err(FE_ERR_CONFIG, "unsupported moisture selectors");
   return FE_OK;
 }
 
-// Once per device, with that device current: the device address of the scratch array.
-int scratch_address(int dev, float** out) {
-  if (dev < 0 || dev >= kMaxDevices) return na_err(FE_ERR_ARG, "device ordinal out of range");
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return na_err(FE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    }
-    g_scratch_addr[dev] = p;
+// The device address of the scratch array on the current device, looked up on every call: a
+// cached address would outlive a cudaDeviceReset or a re-created primary context (the module is
+// loaded again there), and a per-call lookup is cheap next to the synchronising call it serves.
+int scratch_address(float** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return na_err(FE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   }
-  *out = (float*)g_scratch_addr[dev];
+  *out = (float*)p;
   return FE_OK;
 }
 }  // namespace
@@ -159,7 +103,7 @@ extern "C" int fe_frhs_noalloc(const fe_config* cfg, int stage, float simTime, i
   int rc = check(*cfg);
   if (rc) return rc;
   Phys P;
-  make_phys(*cfg, P);
+  K::phys_from_config(*cfg, P);
   if (P.n > fe_noalloc_max_cells())
     return na_err(FE_ERR_ARG, "domain of " + std::to_string(P.n) + " halo-inclusive cells exceeds the " +
                                   std::to_string(fe_noalloc_max_cells()) + "-cell scratch of fe_frhs_noalloc");
@@ -169,7 +113,7 @@ extern "C" int fe_frhs_noalloc(const fe_config* cfg, int stage, float simTime, i
     return na_err(FE_ERR_NO_DEVICE, "no current CUDA device");
   }
   float* S = nullptr;
-  rc = scratch_address(dev, &S);
+  rc = scratch_address(&S);
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   const size_t n = (size_t)P.n, n2 = (size_t)P.n2;

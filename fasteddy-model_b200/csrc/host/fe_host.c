@@ -510,94 +510,99 @@ static void build_grid(void) {
       if (jg > Ny - 1) jg = Ny - 1;
       topoPos[IJ(i, j)] = g_topoGlobal ? (float)g_topoGlobal[(size_t)ig * Ny + jg] : 0.0f;
     }
-  /* interior cell centres, terrain-following compression (grid.c:386-410) */
-  for (i = iMin; i < iMax; i++)
-    for (j = jMin; j < jMax; j++) {
-      double h = topoPos[IJ(i, j)];
-      for (k = kMin; k < kMax; k++) {
-        double z = (double)(k - Nh) * dZ + 0.5 * dZ;
-        if (verticalDeformSwitch == 1) z = z_deform(z, 0.0, ztop);
-        xPos[IJK(i, j, k)] = (float)((double)(i - Nh) * dX + 0.5 * dX);
-        yPos[IJK(i, j, k)] = (float)((double)(j - Nh) * dY + 0.5 * dY);
-        zPos[IJK(i, j, k)] = (float)(z * ((ztop - h) / ztop) + h);
+  /* interior cell centres, terrain-following compression (grid.c:386-410), in the reference's
+   * float arithmetic (float products, the 0.5*d literals promoting the sum to double, the
+   * compression in float) so the coordinates equal the reference's bit for bit */
+  {
+    const float ztopf = (float)((double)((float)Nz * dZ) - 0.5 * (double)dZ);
+    for (i = iMin; i < iMax; i++)
+      for (j = jMin; j < jMax; j++) {
+        const float h = topoPos[IJ(i, j)];
+        for (k = kMin; k < kMax; k++) {
+          float z = (float)((double)(((float)k - (float)Nh) * dZ) + 0.5 * (double)dZ);
+          if (verticalDeformSwitch == 1) z = (float)z_deform(z, 0.0, ztop);
+          xPos[IJK(i, j, k)] = (float)((double)((float)(i - Nh) * dX) + 0.5 * (double)dX);
+          yPos[IJK(i, j, k)] = (float)((double)((float)(j - Nh) * dY) + 0.5 * (double)dY);
+          zPos[IJK(i, j, k)] = z * ((ztopf - h) / ztopf) + h;
+        }
       }
-    }
+  }
   /* horizontal coordinate halos: x/y continue linearly, z copies the edge column
    * (single-rank result of grid.c:459-541 after the boundary-rank overrides) */
   for (i = iMin - Nh; i < iMin; i++)
     for (j = jMin; j < jMax; j++)
       for (k = kMin; k < kMax; k++) {
-        xPos[IJK(i, j, k)] = (float)(xPos[IJK(iMin, j, k)] - (double)(Nh - i) * dX);
+        xPos[IJK(i, j, k)] = xPos[IJK(iMin, j, k)] - (float)(Nh - i) * dX;
         yPos[IJK(i, j, k)] = yPos[IJK(iMin, j, k)];
         zPos[IJK(i, j, k)] = zPos[IJK(iMin, j, k)];
       }
   for (i = iMax; i < iMax + Nh; i++)
     for (j = jMin; j < jMax; j++)
       for (k = kMin; k < kMax; k++) {
-        xPos[IJK(i, j, k)] = (float)(xPos[IJK(iMax - 1, j, k)] + (double)(i - iMax + 1) * dX);
+        xPos[IJK(i, j, k)] = xPos[IJK(iMax - 1, j, k)] + (float)(i - iMax + 1) * dX;
         yPos[IJK(i, j, k)] = yPos[IJK(iMax - 1, j, k)];
         zPos[IJK(i, j, k)] = zPos[IJK(iMax - 1, j, k)];
       }
   for (i = iMin - Nh; i < iMax + Nh; i++)
     for (k = kMin; k < kMax; k++) {
       for (j = jMin - Nh; j < jMin; j++) {
-        yPos[IJK(i, j, k)] = (float)(yPos[IJK(i, jMin, k)] - (double)(Nh - j) * dY);
+        yPos[IJK(i, j, k)] = yPos[IJK(i, jMin, k)] - (float)(Nh - j) * dY;
         xPos[IJK(i, j, k)] = xPos[IJK(i, jMin, k)];
         zPos[IJK(i, j, k)] = zPos[IJK(i, jMin, k)];
       }
       for (j = jMax; j < jMax + Nh; j++) {
-        yPos[IJK(i, j, k)] = (float)(yPos[IJK(i, jMax - 1, k)] + (double)(j - jMax + 1) * dY);
+        yPos[IJK(i, j, k)] = yPos[IJK(i, jMax - 1, k)] + (float)(j - jMax + 1) * dY;
         xPos[IJK(i, j, k)] = xPos[IJK(i, jMax - 1, k)];
         zPos[IJK(i, j, k)] = zPos[IJK(i, jMax - 1, k)];
       }
     }
-  /* vertical halos: linear continuation of the first/last interior spacing (grid.c:547-573) */
+  /* vertical halos: linear continuation of the first/last interior spacing in float (grid.c:547-573) */
   for (i = iMin - Nh; i < iMax + Nh; i++)
     for (j = jMin - Nh; j < jMax + Nh; j++) {
-      double dzb = (double)zPos[IJK(i, j, kMin + 1)] - zPos[IJK(i, j, kMin)];
-      double dzt = (double)zPos[IJK(i, j, kMax - 1)] - zPos[IJK(i, j, kMax - 2 >= kMin ? kMax - 2 : kMin)];
+      const float dzb = zPos[IJK(i, j, kMin + 1)] - zPos[IJK(i, j, kMin)];
+      const float dzt = zPos[IJK(i, j, kMax - 1)] - zPos[IJK(i, j, kMax - 2 >= kMin ? kMax - 2 : kMin)];
       for (k = kMin - Nh; k < kMin; k++) {
-        zPos[IJK(i, j, k)] = (float)(zPos[IJK(i, j, kMin)] - (double)(Nh - k) * dzb);
+        zPos[IJK(i, j, k)] = zPos[IJK(i, j, kMin)] - (float)(Nh - k) * dzb;
         xPos[IJK(i, j, k)] = xPos[IJK(i, j, kMin)];
         yPos[IJK(i, j, k)] = yPos[IJK(i, j, kMin)];
       }
       for (k = kMax; k < kMax + Nh; k++) {
-        zPos[IJK(i, j, k)] = (float)(zPos[IJK(i, j, kMax - 1)] + (double)(k - kMax + 1) * dzt);
+        zPos[IJK(i, j, k)] = zPos[IJK(i, j, kMax - 1)] + (float)(k - kMax + 1) * dzt;
         xPos[IJK(i, j, k)] = xPos[IJK(i, j, kMax - 1)];
         yPos[IJK(i, j, k)] = yPos[IJK(i, j, kMax - 1)];
       }
     }
 }
 
-/* Metric terms by centred differences of the coordinates (grid.c:584-655), in double.
- * The inverse-metric entries use the reference's cofactor choice, so J31/J32 come out
- * exactly as the reference computes them for a given coordinate set. Halos copy the
- * nearest interior value (grid.c:663-742). */
+/* Metric terms by centred differences of the coordinates (grid.c:584-655), in the reference's
+ * float arithmetic (float metric tensor and determinant, the inverse determinant divided in
+ * double), so the metrics equal the reference's bit for bit. The inverse-metric entries use the
+ * reference's cofactor choice. Halos copy the nearest interior value (grid.c:663-742). */
 static void build_metrics(void) {
   int i, j, k, b;
-  double i2x = 1.0 / (2.0 * dX), i2y = 1.0 / (2.0 * dY), i2z = 1.0 / (2.0 * dZ);
+  const float i2x = (float)(1.0 / (2.0 * (double)dX)), i2y = (float)(1.0 / (2.0 * (double)dY));
+  const float i2z = (float)(1.0 / (2.0 * (double)dZ));
   for (i = iMin; i < iMax; i++)
     for (j = jMin; j < jMax; j++)
       for (k = kMin; k < kMax; k++) {
-        double T00 = ((double)xPos[IJK(i + 1, j, k)] - xPos[IJK(i - 1, j, k)]) * i2x;
-        double T01 = ((double)yPos[IJK(i + 1, j, k)] - yPos[IJK(i - 1, j, k)]) * i2x;
-        double T02 = ((double)zPos[IJK(i + 1, j, k)] - zPos[IJK(i - 1, j, k)]) * i2x;
-        double T10 = ((double)xPos[IJK(i, j + 1, k)] - xPos[IJK(i, j - 1, k)]) * i2y;
-        double T11 = ((double)yPos[IJK(i, j + 1, k)] - yPos[IJK(i, j - 1, k)]) * i2y;
-        double T12 = ((double)zPos[IJK(i, j + 1, k)] - zPos[IJK(i, j - 1, k)]) * i2y;
-        double T20 = ((double)xPos[IJK(i, j, k + 1)] - xPos[IJK(i, j, k - 1)]) * i2z;
-        double T21 = ((double)yPos[IJK(i, j, k + 1)] - yPos[IJK(i, j, k - 1)]) * i2z;
-        double T22 = ((double)zPos[IJK(i, j, k + 1)] - zPos[IJK(i, j, k - 1)]) * i2z;
-        double det = (T11 * T22 - T12 * T21) * T00 - (T01 * T22 - T02 * T21) * T10 + (T01 * T12 - T02 * T11) * T20;
-        float detf, invf;
-        if (fabs(det) < 1e-6) det = 1e-6;
-        detf = (float)det;
-        invf = 1.0f / detf;
+        const float T00 = (xPos[IJK(i + 1, j, k)] - xPos[IJK(i - 1, j, k)]) * i2x;
+        const float T01 = (yPos[IJK(i + 1, j, k)] - yPos[IJK(i - 1, j, k)]) * i2x;
+        const float T02 = (zPos[IJK(i + 1, j, k)] - zPos[IJK(i - 1, j, k)]) * i2x;
+        const float T10 = (xPos[IJK(i, j + 1, k)] - xPos[IJK(i, j - 1, k)]) * i2y;
+        const float T11 = (yPos[IJK(i, j + 1, k)] - yPos[IJK(i, j - 1, k)]) * i2y;
+        const float T12 = (zPos[IJK(i, j + 1, k)] - zPos[IJK(i, j - 1, k)]) * i2y;
+        const float T20 = (xPos[IJK(i, j, k + 1)] - xPos[IJK(i, j, k - 1)]) * i2z;
+        const float T21 = (yPos[IJK(i, j, k + 1)] - yPos[IJK(i, j, k - 1)]) * i2z;
+        const float T22 = (zPos[IJK(i, j, k + 1)] - zPos[IJK(i, j, k - 1)]) * i2z;
+        float detf = (T11 * T22 - T12 * T21) * T00 - (T01 * T22 - T02 * T21) * T10 + (T01 * T12 - T02 * T11) * T20;
+        float invf;
+        if (fabsf(detf) < 1e-6f) detf = 1e-6f;
+        invf = (float)(1.0 / (double)detf);
         D_Jac[IJK(i, j, k)] = detf;
         invD_Jac[IJK(i, j, k)] = invf;
-        J31[IJK(i, j, k)] = (float)((T10 * T21 - T11 * T20) * invf);
-        J32[IJK(i, j, k)] = (float)(-(T00 * T21 - T01 * T20) * invf);
-        J33[IJK(i, j, k)] = (float)((T00 * T11 - T01 * T10) * invf);
+        J31[IJK(i, j, k)] = (T10 * T21 - T11 * T20) * invf;
+        J32[IJK(i, j, k)] = -(T00 * T21 - T01 * T20) * invf;
+        J33[IJK(i, j, k)] = (T00 * T11 - T01 * T10) * invf;
       }
   for (b = 0; b < 6; b++) {
     int ilo = iMin - Nh, ihi = iMax + Nh, jlo = jMin - Nh, jhi = jMax + Nh, klo = kMin - Nh, khi = kMax + Nh;

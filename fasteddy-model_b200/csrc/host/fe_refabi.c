@@ -9,11 +9,13 @@
  *   cuda_hydroCoreInit          -> base-state upload
  *   cuda_timeIntInit            -> prognostic state, surface arrays and clock upload
  *   cuda_timeIntCommence(it)    -> NtBatch RK3 steps, then state/pressure/surface copied back
- *                                  to the host globals (cuda_timeIntDevice.cu:105-157, :198-257)
+ *                                  to the host globals (cuda_timeIntDevice.cu:105-157, :198-257),
+ *                                  with the last stage's tendencies when hydroForcingWrite or
+ *                                  hydroForcingLog is set and the SGS stresses and moisture SGS
+ *                                  fluxes when hydroSubGridWrite is set (:210-251)
  * Differences from the reference: errors are returned (never exit()); hydroPres returned
  * after a batch is the perturbation pressure of the returned state (the reference returns
- * the one of the last stage's input); Frhs arrays are not copied back by Commence (use
- * cuda_hydroCoreDeviceBuildFrhs to evaluate and fetch a tendency).
+ * the one of the last stage's input).
  */
 #include <stdio.h>
 
@@ -90,6 +92,22 @@ static void fill_config(fe_config *c) {
   c->corioConstHorz = corioConstHorz; c->corioConstVert = corioConstVert; c->corioLS_fact = corioLS_fact;
 }
 
+/* The reference's parameter reader, when the program that loads this library links it (the
+ * FastEddy driver does); absent in programs built on the repository's own host layer. */
+extern int queryIntegerParameter(char *name, int *var, int min, int max, int reqStatus) __attribute__((weak));
+
+int fecuda_GetParams(void) {
+  /* tBx, tBy, tBz stay mandatory keys of the parameter file (fecuda.c:38-47); the engine picks
+   * its own launch shapes, so the values are only read (2 = the reference's PARAM_MANDATORY) */
+  static int tbx, tby, tbz;
+  int rc = 0;
+  if (!queryIntegerParameter) return FE_OK;
+  rc |= queryIntegerParameter("tBx", &tbx, 1, 2147483647, 2);
+  rc |= queryIntegerParameter("tBy", &tby, 1, 2147483647, 2);
+  rc |= queryIntegerParameter("tBz", &tbz, 1, 2147483647, 2);
+  return rc ? FE_ERR_CONFIG : FE_OK;
+}
+
 int fecuda_Init(void) {
   int n = fe_device_count();
   if (n <= 0) return FE_ERR_NO_DEVICE;
@@ -120,6 +138,9 @@ int cuda_gridInit(void) {
   }
   fill_config(&c);
   rc = fe_create(&c, g_device, &g_dom);
+  if (rc) return rc;
+  /* the batch copy-back of the tendencies needs the last stage's tendencies kept */
+  rc = fe_set_forcing_capture(g_dom, hydroForcingWrite == 1 || hydroForcingLog == 1);
   if (rc) return rc;
   return fe_set_grid(g_dom, zPos, J31, J32, J33, D_Jac, invD_Jac);
 }
@@ -159,10 +180,15 @@ int cuda_timeIntHydroSynchFromDevice(void) {
   if (!rc && surflayerSelector > 0)
     rc = fe_get_surface(g_dom, NULL, NULL, fricVel, htFlux, invOblen, tskin, moistureSelector > 0 ? qFlux : NULL,
                         moistureSelector > 0 ? qskin : NULL);
-  if (!rc && hydroSubGridWrite == 1 && turbulenceSelector > 0) {
-    rc = fe_get_frhs(g_dom, NULL, NULL, NULL, hydroTauFlds);
-    if (rc == FE_ERR_STATE) rc = FE_OK; /* no tendency buffer held: nothing to copy */
-  }
+  /* the last stage's tendencies (kept by the engine for the last step of the batch) */
+  if (!rc && (hydroForcingWrite == 1 || hydroForcingLog == 1))
+    rc = fe_get_frhs(g_dom, hydroFldsFrhs, TKESelector > 0 ? sgstkeScalarsFrhs : NULL,
+                     moistureSelector > 0 ? moistScalarsFrhs : NULL, NULL);
+  /* SGS stresses and heat fluxes; moisture SGS fluxes (allocated on the host only in this case,
+   * hydro_core.c:897-898) */
+  if (!rc && hydroSubGridWrite == 1 && turbulenceSelector > 0)
+    rc = fe_get_sgs_fluxes(g_dom, hydroTauFlds,
+                           (moistureSGSturb == 1 && moistureSelector > 0) ? moistTauFlds : NULL);
   return rc;
 }
 

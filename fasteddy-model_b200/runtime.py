@@ -139,6 +139,9 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_get_surface", ip, [vp, fp, fp, fp, fp, fp, fp, fp, fp]),
         ("fe_build_frhs", ip, [vp, ip]),
         ("fe_get_frhs", ip, [vp, fp, fp, fp, fp]),
+        ("fe_set_forcing_capture", ip, [vp, ip]),
+        ("fe_get_sgs_fluxes", ip, [vp, fp, fp]),
+        ("fe_check_config", ip, [ctypes.POINTER(FeConfig)]),
         ("fe_count_nonfinite", ip, [vp, ctypes.POINTER(ctypes.c_longlong)]),
         ("fe_domain_means", ip, [vp, c_double_p]),
         ("fe_set_tiling", ip, [vp, ip, ip, ip]),
@@ -396,15 +399,44 @@ class Domain:
         _check(self.e.fe_get_surface(self.h, *(_fptr(out[k]) for k in names)), "fe_get_surface")
         return out
 
-    def build_frhs(self, stage: int) -> dict[str, np.ndarray]:
+    def build_frhs(self, stage: int, taus: bool = True) -> dict[str, np.ndarray]:
         _check(self.e.fe_build_frhs(self.h, stage), "fe_build_frhs")
         nx, ny, nz = self.shape
         F = np.empty((5, nx, ny, nz), np.float32)
         Fe = np.empty((1, nx, ny, nz), np.float32) if self.ntke else None
         Fm = np.empty((self.nmoist, nx, ny, nz), np.float32) if self.nmoist else None
-        taus = np.empty((9, nx, ny, nz), np.float32)
+        taus = np.empty((9, nx, ny, nz), np.float32) if taus else None
         _check(self.e.fe_get_frhs(self.h, _fptr(F), _fptr(Fe), _fptr(Fm), _fptr(taus)), "fe_get_frhs")
         return {"hydroFrhs": F, "sgstkeFrhs": Fe, "moistFrhs": Fm, "taus": taus}
+
+    def set_forcing_capture(self, on: bool) -> None:
+        """Keep the last RK stage's tendencies of the last step of every later advance."""
+        _check(self.e.fe_set_forcing_capture(self.h, 1 if on else 0), "fe_set_forcing_capture")
+
+    def last_forcing(self) -> dict[str, np.ndarray]:
+        """Tendencies kept by the last advance (set_forcing_capture) and the SGS fluxes of the
+        last physics stage: hydroFrhs, sgstkeFrhs, moistFrhs, taus, moistTaus."""
+        nx, ny, nz = self.shape
+        F = np.empty((5, nx, ny, nz), np.float32)
+        Fe = np.empty((1, nx, ny, nz), np.float32) if self.ntke else None
+        Fm = np.empty((self.nmoist, nx, ny, nz), np.float32) if self.nmoist else None
+        _check(self.e.fe_get_frhs(self.h, _fptr(F), _fptr(Fe), _fptr(Fm), None), "fe_get_frhs")
+        out = {"hydroFrhs": F, "sgstkeFrhs": Fe, "moistFrhs": Fm}
+        out.update(self.sgs_fluxes())
+        return out
+
+    def sgs_fluxes(self) -> dict[str, np.ndarray]:
+        """SGS stresses/heat fluxes (9) and moisture SGS fluxes (3 per species, when the
+        configuration has them) of the last physics stage."""
+        nx, ny, nz = self.shape
+        cfg = self.cfg
+        taus = np.empty((9, nx, ny, nz), np.float32) if cfg.turbulenceSelector > 0 else None
+        mt = None
+        if cfg.turbulenceSelector > 0 and self.nmoist and cfg.moistureSGSturb > 0:
+            mt = np.empty((3 * self.nmoist, nx, ny, nz), np.float32)
+        if taus is not None:
+            _check(self.e.fe_get_sgs_fluxes(self.h, _fptr(taus), _fptr(mt)), "fe_get_sgs_fluxes")
+        return {"taus": taus, "moistTaus": mt}
 
     def nonfinite(self) -> int:
         c = ctypes.c_longlong()

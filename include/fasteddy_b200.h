@@ -41,6 +41,10 @@ extern "C" {
 /* ======================================================= A. reference-named ABI */
 /* Each entry replaces the same-named function of the reference CUDA layer. */
 
+/* replaces SRC/FECUDA/fecuda.c:38 fecuda_GetParams(): reads the tBx/tBy/tBz keys through the
+ * reference's parameter reader when the program links it (they stay mandatory keys); the
+ * engine chooses its own launch shapes. */
+int fecuda_GetParams(void);
 /* replaces SRC/FECUDA/fecuda.h:35 fecuda_Init(): selects device (rank % numDevices). */
 int fecuda_Init(void);
 /* replaces SRC/FECUDA/fecuda.h:45 fecuda_SetBlocksPerGrid(): halo-inclusive extents;
@@ -133,6 +137,9 @@ void fe_config_defaults(fe_config *cfg);
 void fe_config_derive(fe_config *cfg, float coriolisLatitude);
 
 int fe_device_count(void);
+/* Check a configuration as fe_create does (selector ranges as hydro_core.c:221-349 checks
+ * them, and what this path supports); FE_OK or FE_ERR_CONFIG/FE_ERR_ARG with fe_last_error(). */
+int fe_check_config(const fe_config *cfg);
 /* Create a domain on `device`; checks the configuration and allocates device memory. */
 int fe_create(const fe_config *cfg, int device, fe_domain **out);
 int fe_destroy(fe_domain *d);
@@ -170,6 +177,16 @@ int fe_build_frhs(fe_domain *d, int stage);
 /* Copy the tendencies of the last fe_build_frhs (same field blocks as fe_get_state)
  * and, if taus != NULL, the 9 SGS stress/flux fields (order of hydroTauFlds). */
 int fe_get_frhs(fe_domain *d, float *hydroFrhs, float *sgstkeFrhs, float *moistFrhs, float *taus);
+/* With on != 0, every later fe_advance keeps the tendencies of the last RK stage of its last
+ * step in the buffer fe_get_frhs reads: what the reference holds in its Frhs arrays after a
+ * batch and copies back when hydroForcingWrite or hydroForcingLog is set
+ * (cuda_timeIntDevice.cu:210-224). That step then runs outside the step graph. */
+int fe_set_forcing_capture(fe_domain *d, int on);
+/* The SGS stresses and heat fluxes (9 fields, order of hydroTauFlds) and the moisture SGS
+ * fluxes (3 per moisture species, order of moistTauFlds: species-major, x, y, z) of the last
+ * physics stage evaluated, the arrays cuda_timeIntDevice.cu:238-251 copies back. Either
+ * pointer may be NULL. */
+int fe_get_sgs_fluxes(fe_domain *d, float *taus, float *moistTaus);
 
 /* Count NaN/Inf values in the interior prognostic state (device reduction). */
 int fe_count_nonfinite(fe_domain *d, long long *count);
@@ -282,9 +299,11 @@ int fe_coarsen(fe_domain *fine, fe_domain *coarse, float *tau_target);
  * pointers in the reference layout; `state` (5 + TKE + moisture fields) must have its halo
  * cells filled (as fe_get_state returns them); `surface` holds the 11 planes cd, ch, cq,
  * fricVel, htFlux, tskin, invOblen, z0m, z0t, qFlux, qskin and is updated in place on a
- * physics stage; `frhs` receives the interior tendencies. The first call on a device looks
- * up the array's device address; make that first call before any stream capture. Calls
- * share the array, so calls that overlap on the GPU (other streams, other threads) race.
+ * physics stage; `frhs` receives the interior tendencies. Every call looks up the array's
+ * device address on the caller's current device (so a reset device or a re-created context is
+ * followed). Calls share the array, so calls that overlap on the GPU (other streams, other
+ * threads) race. The configuration is checked as fe_check_config does, and further limited to
+ * HYB56/WENO5 advection without the explicit filter or large-scale forcing.
  * Runs on `stream` (a cudaStream_t, NULL = legacy default stream) and synchronises it. */
 #define FE_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 typedef struct fe_noalloc_args {

@@ -113,5 +113,33 @@ def build_io(src: str, inc: list[str]) -> str:
     return exe
 
 
+# The reference's CUDA layer: the four device translation units and the thin C wrappers over them.
+# The drop-in build leaves exactly these out and links the repository's libraries in their place.
+CUDA_WRAPPERS = ["FECUDA/fecuda.c", "GRID/CUDA/cuda_grid.c", "HYDRO_CORE/CUDA/cuda_hydroCore.c",
+                 "TIME_INTEGRATION/CUDA/cuda_timeInt.c"]
+ENGINE_LIBS = os.path.join(os.path.dirname(HERE), "fasteddy-model_b200", "_build")
+
+
+def build_dropin(src: str = DEFAULT_SRC) -> str:
+    """oracle/_ref/fe_dropin_harness: the same driver sequence (ref_harness.c) and the same
+    reference host modules as fe_ref_harness, with the reference's CUDA layer replaced by
+    libfe_refabi.so + libfe_engine.so, linked as a FastEddy user would (-rdynamic exports the
+    driver's globals to the library). Needs fe_ref_harness's objects (build() first) and the
+    repository's libraries."""
+    exe = os.path.join(OUT, "fe_dropin_harness")
+    objs = [_obj(rel) for rel in C_SOURCES if rel not in CUDA_WRAPPERS]
+    objs += [os.path.join(OUT, "obj", n) for n in ("mpi_stub.o", "netcdf_stub.o", "ref_harness.o")]
+    missing = [o for o in objs if not os.path.exists(o)]
+    if missing:
+        if not os.path.isdir(src):
+            raise FileNotFoundError("reference objects not built: " + ", ".join(missing))
+        build(src)
+    rpath = "$ORIGIN/" + os.path.relpath(ENGINE_LIBS, OUT)
+    _run(["gcc", "-o", exe, *objs, "-rdynamic", "-L" + ENGINE_LIBS, "-lfe_refabi", "-lfe_engine",
+          "-Wl,-rpath," + rpath, "-lm"])
+    return exe
+
+
 if __name__ == "__main__":
     print(build(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC, verbose=True))
+    print(build_dropin(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC))

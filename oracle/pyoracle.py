@@ -126,6 +126,11 @@ class Oracle:
 
     def build_frhs(self, stage: int) -> dict:
         self.lib.ora_build_frhs(self.h, stage)
+        return self.last_frhs()
+
+    def last_frhs(self) -> dict:
+        """The tendencies and SGS stresses of the last evaluation (after step(): those of the last
+        RK stage of the last step, what the reference copies back after a batch)."""
         nx, ny, nz = self.shape
         F = np.empty((5, nx, ny, nz))
         Fe = np.empty((1, nx, ny, nz)) if self.ntke else None

@@ -7,6 +7,12 @@
  * with the raw float32 files <INDIR>/<name>.bin and writes <outPath><outFileBase>_rank_0.<TSTEP>.
  *
  * usage: fe_ref_io PARAMFILE INDIR TSTEP
+ *        fe_ref_io PARAMFILE OUTDIR dump
+ *
+ * dump runs the reference's own initial-condition path instead (FastEddy.c:109 seeding,
+ * gridSecondaryPreparations, hydro_coreSetBaseState: FastEddy.c:223-238, grid.c:386-803,
+ * hydro_core.c:1053-1250) and writes the host inputs of the CUDA path as raw float32 files
+ * <OUTDIR>/<name>.bin: coordinates, metrics, base state, initial state and surface arrays.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -41,6 +47,52 @@ static int read_into(const char *dir, const char *name, float *dst, size_t n) {
   return 0;
 }
 
+static int write_from(const char *dir, const char *name, const float *src, size_t n) {
+  char path[2048];
+  FILE *f;
+  size_t put;
+  snprintf(path, sizeof(path), "%s/%s.bin", dir, name);
+  f = fopen(path, "wb");
+  if (!f) return -1;
+  put = fwrite(src, sizeof(float), n, f);
+  fclose(f);
+  return put == n ? 0 : -1;
+}
+
+/* the reference's own initial grid, base state and initial state (FastEddy.c:223-238) */
+static int dump_initial_state(const char *out) {
+  size_t N = (size_t)(Nxp + 2 * Nh) * (Nyp + 2 * Nh) * (Nzp + 2 * Nh);
+  size_t N2 = (size_t)(Nxp + 2 * Nh) * (Nyp + 2 * Nh);
+  int rc = 0;
+  fempi_AllocateBuffers(Nxp, Nyp, Nzp, Nh);
+  if (gridSecondaryPreparations() != 0) return 7;
+  if (hydro_coreSetBaseState() != 0) return 8;
+  rc |= write_from(out, "xPos", xPos, N);
+  rc |= write_from(out, "yPos", yPos, N);
+  rc |= write_from(out, "zPos", zPos, N);
+  rc |= write_from(out, "topoPos", topoPos, N2);
+  rc |= write_from(out, "J31", J31, N);
+  rc |= write_from(out, "J32", J32, N);
+  rc |= write_from(out, "J33", J33, N);
+  rc |= write_from(out, "D_Jac", D_Jac, N);
+  rc |= write_from(out, "invD_Jac", invD_Jac, N);
+  rc |= write_from(out, "baseState", hydroBaseStateFlds, 2 * N);
+  rc |= write_from(out, "hydroFlds", hydroFlds, 5 * N);
+  if (TKESelector > 0) rc |= write_from(out, "sgstke", sgstkeScalars, (size_t)TKESelector * N);
+  if (surflayerSelector > 0) {
+    rc |= write_from(out, "tskin", tskin, N2);
+    rc |= write_from(out, "fricVel", fricVel, N2);
+    rc |= write_from(out, "htFlux", htFlux, N2);
+    rc |= write_from(out, "z0m", z0m, N2);
+    rc |= write_from(out, "z0t", z0t, N2);
+    if (moistureSelector > 0) {
+      rc |= write_from(out, "qskin", qskin, N2);
+      rc |= write_from(out, "qFlux", qFlux, N2);
+    }
+  }
+  return rc ? 9 : 0;
+}
+
 int main(int argc, char **argv) {
   char *desc;
   int rc = 0;
@@ -61,6 +113,7 @@ int main(int argc, char **argv) {
   gridGetParams();
   hydro_coreGetParams();
   timeGetParams();
+  srand(mpi_rank_world + 12345); /* FastEddy.c:109 */
   fempi_Init();
   mem_utilsInit();
   ioInit();
@@ -71,6 +124,7 @@ int main(int argc, char **argv) {
     fprintf(stderr, "ref_io: parameter errors\n");
     return 4;
   }
+  if (strcmp(argv[3], "dump") == 0) return dump_initial_state(in);
   N = (size_t)(Nxp + 2 * Nh) * (Nyp + 2 * Nh) * (Nzp + 2 * Nh);
   N2 = (size_t)(Nxp + 2 * Nh) * (Nyp + 2 * Nh);
   rc |= read_into(in, "xPos", xPos, N);

@@ -2,8 +2,9 @@
 
 Runs the reference's own CUDA build (oracle/_ref, built by oracle/build_ref.py) on small
 seeded cases produced by the host layer and stores its prognostic state after 1 and 10
-RK3 steps, so the FP64 oracle and the engine are checked against the reference's own
-outputs. The reference runs with a thread-block shape that divides the halo-inclusive
+RK3 steps and (cases without large-scale forcing) its tendency of every RK stage on the
+initial state with the SGS stresses of the physics stage, so the FP64 oracle and the engine
+are checked against the reference's own outputs. The reference runs with a thread-block shape that divides the halo-inclusive
 extents (no out-of-range threads), twice, and the run-to-run difference is stored too.
 
 usage: python tests/golden/make_reference_golden.py OUTDIR [CASE ...]
@@ -84,10 +85,26 @@ def main(out: str, names=None) -> None:
         text = fe.cases.param_text(c["case"], c["nx"], c["ny"], c["nz"], tb=fe.cases.exact_tb(c["ny"], c["nz"]),
                                    params=c["kw"].get("params"))
         res = {"input_sha256": np.array(input_digest(inp))}
+        I = (Ellipsis, slice(3, -3), slice(3, -3), slice(3, -3))
+        if not c["kw"].get("params", {}).get("lsfSelector"):
+            # one tendency evaluation of every RK stage on the initial state, with the stresses of
+            # the physics stage (the reference copies them back when these two switches are set)
+            ftext = fe.cases.param_text(c["case"], c["nx"], c["ny"], c["nz"],
+                                        tb=fe.cases.exact_tb(c["ny"], c["nz"]),
+                                        params=dict(c["kw"].get("params") or {}, hydroForcingWrite=1,
+                                                    hydroSubGridWrite=1))
+            for stage in (0, 1, 2):
+                r = refrun.frhs(ftext, inp, stage, host.shape, ntke, nm)
+                res[f"frhs_{stage}"] = r["hydroFrhs"][I]
+                if ntke:
+                    res[f"tkefrhs_{stage}"] = r["sgstkeFrhs"][I]
+                if nm:
+                    res[f"moistfrhs_{stage}"] = r["moistFrhs"][I]
+                if stage == 2:
+                    res["taus_2"] = r["taus"][I]
         for n in (1, 10):
             a = refrun.run(text, inp, n, host.shape, ntke, nm)
             b = refrun.run(text, inp, n, host.shape, ntke, nm)
-            I = (Ellipsis, slice(3, -3), slice(3, -3), slice(3, -3))
             res[f"hydro_{n}"] = a["hydroFlds"][I]
             res[f"self_absdiff_{n}"] = np.abs(a["hydroFlds"][I] - b["hydroFlds"][I]).max(axis=(1, 2, 3))
             if ntke:

@@ -104,3 +104,71 @@ def test_engine_matches_reference_build(fe, name):
     _compare(d.get_state(), gold, 10, gold["self_absdiff_10"])
     d.close()
     host.cleanup()
+
+
+# Tendencies of one evaluation per RK stage on the initial state (cases without large-scale
+# forcing). Engine against reference: both FP32 with the same operator order, momentum
+# tendencies agree to ~1e-6; the advected scalars' (a small divergence of large fluxes) to ~1e-4,
+# because the reference forms its advective face values in double precision. The FP64 oracle
+# against the reference: to the FP32 noise of the perturbation pressure and of the fluxes, 1e-3
+# (2e-3 for the stresses), as the oracle tendency tests use. On flat terrain the mass tendency
+# is zero up to rounding and is bounded in absolute terms.
+FRHS_CASES = [c for c in GOLDEN_CASES if "lsf" not in c]
+
+
+def _compare_frhs(g: dict, gold, stage: int, flat: bool, tight: bool) -> None:
+    tm = 1e-5 if tight else 1e-3  # momentum
+    tt = 1e-5 if tight else 2e-3  # stresses
+    ref = gold[f"frhs_{stage}"]
+    scale = np.abs(ref[4]).max() / 300.0  # the theta tendency's size in mass units
+    for f in range(5):
+        a = interior(g["hydroFrhs"][f]).astype(np.float64)
+        if f == 0 and flat:
+            assert np.abs(a - ref[0]).max() <= 1e-5 * scale + 1e-7, (stage, f)
+        elif np.abs(ref[f]).max() > 0:
+            assert rel_l2(a, ref[f]) < (1e-3 if f in (0, 4) else tm), (stage, f)
+        else:
+            assert np.abs(a).max() < 1e-6, (stage, f)
+    if f"tkefrhs_{stage}" in gold and np.abs(gold[f"tkefrhs_{stage}"]).max() > 0:
+        assert rel_l2(interior(g["sgstkeFrhs"][0]), gold[f"tkefrhs_{stage}"][0]) < 1e-3, (stage, "tke")
+    if f"moistfrhs_{stage}" in gold:
+        for m in range(gold[f"moistfrhs_{stage}"].shape[0]):
+            r = gold[f"moistfrhs_{stage}"][m]
+            if np.abs(r).max() > 0:
+                assert rel_l2(interior(g["moistFrhs"][m]), r) < 1e-3, (stage, "moist", m)
+    if stage == 2 and g.get("taus") is not None:
+        for t in range(9):
+            r = gold["taus_2"][t]
+            if np.abs(r).max() > 0:
+                assert rel_l2(interior(g["taus"][t]), r) < tt, ("tau", t)
+
+
+@pytest.mark.parametrize("name", FRHS_CASES)
+def test_oracle_tendency_matches_reference_build(fe, name):
+    mk, gold = _load(name)
+    if "frhs_0" not in gold:
+        pytest.skip("golden vectors without tendencies")
+    host, inp = mk.make_inputs(name)
+    assert mk.input_digest(inp) == str(gold["input_sha256"])
+    for stage in (0, 1, 2):
+        o = Oracle(host.config())
+        o.set_inputs(inp)
+        _compare_frhs(o.build_frhs(stage), gold, stage, "hill" not in name, tight=False)
+        o.close()
+    host.cleanup()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", FRHS_CASES)
+def test_engine_tendency_matches_reference_build(fe, name):
+    mk, gold = _load(name)
+    if "frhs_0" not in gold:
+        pytest.skip("golden vectors without tendencies")
+    host, inp = mk.make_inputs(name)
+    assert mk.input_digest(inp) == str(gold["input_sha256"])
+    for stage in (0, 1, 2):
+        d = fe.Domain(host.config())
+        d.set_inputs(inp)
+        _compare_frhs(d.build_frhs(stage), gold, stage, "hill" not in name, tight=True)
+        d.close()
+    host.cleanup()

@@ -304,6 +304,72 @@ def test_dropin_entry_points_match_engine(fe):
     host.cleanup()
 
 
+@pytest.mark.parametrize("name", ["moist_hill", "cbl_dry"])
+def test_kept_last_stage_tendencies_match_oracle(fe, name):
+    """With tendency capture on, an advance keeps the last RK stage's tendencies of its last step
+    (what the reference holds in its Frhs arrays after a batch, cuda_timeIntDevice.cu:210-224):
+    after 1 and 3 steps they match the FP64 oracle's last-stage tendencies after the same steps;
+    the state is the same as without capture, bit for bit."""
+    from oracle.pyoracle import Oracle
+
+    host, inp, cfg = _setup(fe, name)
+    d = fe.Domain(cfg)
+    d.set_inputs(inp)
+    d.set_forcing_capture(True)
+    plain = fe.Domain(cfg)
+    plain.set_inputs(inp)
+    o = Oracle(cfg)
+    o.set_inputs(inp)
+    for n in (1, 2):
+        d.advance(n)
+        plain.advance(n)
+        o.step(n)
+        g, r = d.last_forcing(), o.last_frhs()
+        for f in range(5):
+            if f == 0 and name == "cbl_dry":
+                continue  # the mass tendency on flat terrain: zero up to rounding in FP32
+            assert rel_l2(interior(g["hydroFrhs"][f]), interior(r["hydroFrhs"][f])) < 2e-3, (n, f)
+        assert rel_l2(interior(g["sgstkeFrhs"][0]), interior(r["sgstkeFrhs"][0])) < 2e-3
+        if r["moistFrhs"] is not None:
+            assert rel_l2(interior(g["moistFrhs"][0]), interior(r["moistFrhs"][0])) < 2e-3
+        for k in ("hydroFlds", "sgstke", "moist"):
+            if plain.get_state()[k] is not None:
+                np.testing.assert_array_equal(d.get_state()[k], plain.get_state()[k])
+    d.close()
+    plain.close()
+    host.cleanup()
+
+
+def test_dropin_batch_copies_back_tendencies_and_sgs_fluxes(fe):
+    """With hydroForcingWrite and hydroSubGridWrite set, cuda_timeIntCommence copies back the last
+    stage's tendencies (hydroFldsFrhs, sgstkeScalarsFrhs, moistScalarsFrhs) and the SGS stresses and
+    moisture fluxes (hydroTauFlds, moistTauFlds), as cuda_timeIntDevice.cu:210-251 does: they equal
+    the engine's own after the same steps."""
+    host, inp, cfg = _setup(fe, "moist_hill")
+    libs = fe.load()
+    ra = libs["refabi"]
+    host.set_gi("NtBatch", 3)
+    host.set_gi("hydroForcingWrite", 1)
+    host.set_gi("hydroSubGridWrite", 1)
+    for fn in ("fecuda_Init", "cuda_gridInit", "cuda_hydroCoreInit", "cuda_timeIntInit"):
+        assert getattr(ra, fn)() == 0, fn
+    assert ra.cuda_timeIntCommence(0) == 0
+    dom = fe.Domain(cfg)
+    dom.set_inputs(inp)
+    dom.set_forcing_capture(True)
+    dom.advance(3)
+    lf = dom.last_forcing()
+    np.testing.assert_array_equal(interior(host.array("hydroFldsFrhs", 5)), interior(lf["hydroFrhs"]))
+    np.testing.assert_array_equal(interior(host.array("sgstkeScalarsFrhs", 1)), interior(lf["sgstkeFrhs"]))
+    np.testing.assert_array_equal(interior(host.array("moistScalarsFrhs", 2)), interior(lf["moistFrhs"]))
+    np.testing.assert_array_equal(interior(host.array("hydroTauFlds", 9)), interior(lf["taus"]))
+    np.testing.assert_array_equal(interior(host.array("moistTauFlds", 6)), interior(lf["moistTaus"]))
+    assert np.abs(interior(lf["hydroFrhs"][3])).max() > 0 and np.abs(interior(lf["taus"][0])).max() > 0
+    assert ra.cuda_hydroCoreCleanup() == 0
+    dom.close()
+    host.cleanup()
+
+
 def test_nonfinite_state_is_reported(fe):
     host, inp, cfg = _setup(fe, "cbl_dry")
     libs = fe.load()

@@ -278,6 +278,73 @@ __device__ __forceinline__ float adv_face(int sel, float m2, float m1, float z0,
   }
 }
 
+// ---------------------------------------------------------------- two faces at once
+// The same face values for two stencils held lane-wise in float2 (the two y faces or the two
+// z faces of a cell, or the x faces of two fields), on the packed FP32 pipe of sm_100
+// (__ffma2_rn, __fadd2_rn, __fmul2_rn: each lane rounds exactly as the scalar operation). Every
+// lane equals adv_face() of its own stencil bit for bit: the same operations in the same order,
+// x - y written as x + (-y), which IEEE addition gives exactly. The WENO division stays per lane.
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 f2s(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ float2 hyb56_flux2(float2 m2, float2 m1, float2 z0, float2 p1, float2 p2, float2 p3,
+                                              float2 vel, float2 bfac) {
+  const float2 a = add2(p1, z0), b = add2(p2, m1), c = add2(p3, m2);
+  const float2 d = sub2(p3, m2), e = sub2(p2, m1), f = sub2(p1, z0);
+  const float2 cen = add2(fma2(f2s(37.0f), a, mul2(f2s(-8.0f), b)), c);
+  const float2 upw = fma2(f2s(10.0f), f, fma2(f2s(-5.0f), e, d));
+  const float2 msb = f2(-copysignf(bfac.x, vel.x), -copysignf(bfac.y, vel.y));
+  return mul2(f2s(1.0f / 60.0f), fma2(msb, upw, cen));
+}
+
+template <bool FAST = false>
+__device__ __forceinline__ float2 weno5_face2(float2 a, float2 b, float2 c, float2 d, float2 e) {
+  const float g1 = 1.0f / 10.0f, g2 = 3.0f / 5.0f, g3 = 3.0f / 10.0f, tol = 1e-6f;
+  const float k13 = 1.0f / 3.0f, k76 = 7.0f / 6.0f, k116 = 11.0f / 6.0f, k16 = 1.0f / 6.0f, k56 = 5.0f / 6.0f;
+  const float2 f1 = fma2(f2s(k116), c, fma2(f2s(-k76), b, mul2(f2s(k13), a)));
+  const float2 fB = fma2(f2s(k13), d, fma2(f2s(k56), c, mul2(f2s(-k16), b)));
+  const float2 f3 = fma2(f2s(-k16), e, fma2(f2s(k56), d, mul2(f2s(k13), c)));
+  const float2 s1 = add2(fma2(f2s(-2.0f), b, a), c), t1 = fma2(f2s(3.0f), c, fma2(f2s(-4.0f), b, a));
+  const float2 s2 = add2(fma2(f2s(-2.0f), c, b), d), t2 = sub2(b, d);
+  const float2 s3 = add2(fma2(f2s(-2.0f), d, c), e), t3 = add2(fma2(f2s(-4.0f), d, mul2(f2s(3.0f), c)), e);
+  const float k1312 = 13.0f / 12.0f, k14 = 1.0f / 4.0f;
+  const float2 b1 = fma2(f2s(k14), mul2(t1, t1), mul2(f2s(k1312), mul2(s1, s1)));
+  const float2 b2 = fma2(f2s(k14), mul2(t2, t2), mul2(f2s(k1312), mul2(s2, s2)));
+  const float2 b3 = fma2(f2s(k14), mul2(t3, t3), mul2(f2s(k1312), mul2(s3, s3)));
+  const float2 q1 = add2(f2s(tol), b1), q2 = add2(f2s(tol), b2), q3 = add2(f2s(tol), b3);
+  const float2 a1 = mul2(q2, q3), a2 = mul2(q1, q3), a3 = mul2(q1, q2);
+  const float2 u1 = mul2(f2s(g1), mul2(a1, a1));
+  const float2 u2 = mul2(f2s(g2), mul2(a2, a2));
+  const float2 u3 = mul2(f2s(g3), mul2(a3, a3));
+  const float2 num = fma2(u3, f3, fma2(u2, fB, mul2(u1, f1)));
+  const float2 den = add2(add2(u1, u2), u3);
+  return FAST ? f2(__fdividef(num.x, den.x), __fdividef(num.y, den.y)) : f2(__fdiv_rn(num.x, den.x), __fdiv_rn(num.y, den.y));
+}
+
+template <bool FAST = false>
+__device__ __forceinline__ float2 weno5_flux2(float2 m2, float2 m1, float2 z0, float2 p1, float2 p2, float2 p3, float2 vel) {
+  const bool ux = sgnf(vel.x) > 0.0f, uy = sgnf(vel.y) > 0.0f;
+  return weno5_face2<FAST>(f2(ux ? m2.x : p3.x, uy ? m2.y : p3.y), f2(ux ? m1.x : p2.x, uy ? m1.y : p2.y),
+                           f2(ux ? z0.x : p1.x, uy ? z0.y : p1.y), f2(ux ? p1.x : z0.x, uy ? p1.y : z0.y),
+                           f2(ux ? p2.x : m1.x, uy ? p2.y : m1.y));
+}
+
+// adv_face() of two stencils (bfac per lane): HYB56 and WENO5 on the packed pipe, the other
+// schemes lane by lane.
+template <bool FAST = false>
+__device__ __forceinline__ float2 adv_face2(int sel, float2 m2, float2 m1, float2 z0, float2 p1, float2 p2, float2 p3,
+                                            float2 vel, float2 bfac) {
+  if (sel == ADV_HYB56) return hyb56_flux2(m2, m1, z0, p1, p2, p3, vel, bfac);
+  if (sel == ADV_WENO5) return weno5_flux2<FAST>(m2, m1, z0, p1, p2, p3, vel);
+  return f2(adv_face<FAST>(sel, m2.x, m1.x, z0.x, p1.x, p2.x, p3.x, vel.x, bfac.x),
+            adv_face<FAST>(sel, m2.y, m1.y, z0.y, p1.y, p2.y, p3.y, vel.y, bfac.y));
+}
+
 // q_l's selector (moistureAdvSelectorQi) as a scheme id.
 __host__ __device__ constexpr int ql_scheme(int qi) { return qi == 0 ? ADV_UPWIND : (qi == 1 ? ADV_WENO3 : ADV_WENO5); }
 // The filter's factor as the reference forms it (cuda_filtersDevice.cu:86): the literal

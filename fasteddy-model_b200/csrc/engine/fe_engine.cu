@@ -27,6 +27,7 @@
 #include "fe_kernels.cuh"
 #include "fe_march.cuh"
 #include "fe_march_launch.cuh"
+#include "fe_sgs_march.cuh"
 #include "fe_learn.h"
 #include "fe_sgs.cuh"
 #include "fe_config_phys.cuh"
@@ -75,6 +76,8 @@ struct fe_domain {
   int tk = 32, tj = 4, ti = 2;       // cell-kernel tiling
   int kind = FE_KERNEL_MARCH;        // stage-kernel form
   int mtj = 8, mni = 64;             // march kernel: rows per tile, planes per thread block
+  int sgsNi = 32;                    // fused SGS kernel: planes per thread block
+  int sgsRows = 8;                   // fused last-stage physics: rows per tile (8 or 16; 0 = kernel chain)
   int mniDefault = 64;               // planes per block chosen for the domain size at creation
   fe_mlp* mlp = nullptr;             // learned SGS closure (nullptr: TKE closure)
   float* feat = nullptr;             // its inputs per ring cell (allocated with the first network)
@@ -238,6 +241,7 @@ static void free_domain(fe_domain* d) {
 }
 
 static int march_attrs();
+static cudaError_t sgs_march_attrs();
 
 extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   if (!cfg || !out) return set_err(FE_ERR_ARG, "NULL argument");
@@ -276,9 +280,21 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
         break;
       }
     d->mniDefault = d->mni;
+    // fused SGS kernel (tiles of 32 levels x 8 rows, two blocks per SM): the most planes per block
+    // of 64, 32, 16, 8 that still leaves 10 waves
+    d->sgsNi = 8;
+    for (int ni = 64; ni >= 8; ni /= 2)
+      if (cols * ((P.Nx + ni - 1) / ni) >= 20LL * nsm) {
+        d->sgsNi = ni;
+        break;
+      }
     d->lsfBlocks = P.lsfSub ? 2 * nsm : 0;
   }
   rc = march_attrs();
+  if (rc == FE_OK) {
+    cudaError_t ea = sgs_march_attrs();
+    if (ea != cudaSuccess) rc = set_err(FE_ERR_CUDA, std::string("SGS kernel attributes: ") + cudaGetErrorString(ea));
+  }
   for (int b = 0; b < 3 && rc == FE_OK; b++) {
     rc = dev_alloc(d, &d->st[b], n * P.nf);
     if (rc == FE_OK) rc = dev_alloc(d, &d->pr[b], n);
@@ -587,11 +603,73 @@ static int launch_turb(const fe_domain* d, cudaStream_t s, const float* st, int 
   return P.surf > 0 ? 3 : 2;
 }
 
+// The fused SGS kernel (fe_sgs_march.cuh) of the configuration's field set.
+template <bool TKE, int NQ, int TJ>
+static void launch_sgs_march_tj(const fe_domain* d, cudaStream_t s, const float* st, int stage, bool store) {
+  const Phys& P = d->P;
+  const int ni = d->sgsNi;
+  const dim3 g((P.Nz + fe::SG_K - 1) / fe::SG_K, (P.Ny + TJ - 1) / TJ, (P.Nx + ni - 1) / ni);
+  fe::k_sgs_march<TKE, NQ, TJ><<<g, dim3(fe::SG_K, TJ), fe::SgsTile<TJ>::SMEM_BYTES, s>>>(P, d->Q, st, stage, ni,
+                                                                                         store ? 1 : 0);
+}
+template <bool TKE, int NQ>
+static void launch_sgs_march_nq(const fe_domain* d, cudaStream_t s, const float* st, int stage, bool store) {
+  if (d->sgsRows == 16) launch_sgs_march_tj<TKE, NQ, 16>(d, s, st, stage, store);
+  else launch_sgs_march_tj<TKE, NQ, 8>(d, s, st, stage, store);
+}
+static void launch_sgs_march(const fe_domain* d, cudaStream_t s, const float* st, int stage, bool store) {
+  const Phys& P = d->P;
+  const int nq = (P.nmoist > 0 && P.moistSGS > 0) ? std::min(P.nmoist, 2) : 0;
+  if (P.tke) {
+    if (nq == 2) launch_sgs_march_nq<true, 2>(d, s, st, stage, store);
+    else if (nq == 1) launch_sgs_march_nq<true, 1>(d, s, st, stage, store);
+    else launch_sgs_march_nq<true, 0>(d, s, st, stage, store);
+  } else {
+    if (nq == 2) launch_sgs_march_nq<false, 2>(d, s, st, stage, store);
+    else if (nq == 1) launch_sgs_march_nq<false, 1>(d, s, st, stage, store);
+    else launch_sgs_march_nq<false, 0>(d, s, st, stage, store);
+  }
+}
+static cudaError_t sgs_march_attrs() {
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f, int bytes) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  };
+  const int b8 = fe::SgsTile<8>::SMEM_BYTES, b16 = fe::SgsTile<16>::SMEM_BYTES;
+  set((const void*)fe::k_sgs_march<true, 0, 8>, b8);
+  set((const void*)fe::k_sgs_march<true, 1, 8>, b8);
+  set((const void*)fe::k_sgs_march<true, 2, 8>, b8);
+  set((const void*)fe::k_sgs_march<false, 0, 8>, b8);
+  set((const void*)fe::k_sgs_march<false, 1, 8>, b8);
+  set((const void*)fe::k_sgs_march<false, 2, 8>, b8);
+  set((const void*)fe::k_sgs_march<true, 0, 16>, b16);
+  set((const void*)fe::k_sgs_march<true, 1, 16>, b16);
+  set((const void*)fe::k_sgs_march<true, 2, 16>, b16);
+  set((const void*)fe::k_sgs_march<false, 0, 16>, b16);
+  set((const void*)fe::k_sgs_march<false, 1, 16>, b16);
+  set((const void*)fe::k_sgs_march<false, 2, 16>, b16);
+  return e;
+}
+
+// Whether the last-stage physics runs as the fused kernel: the march stage kernel, SGS closure
+// on, no learned closure (whose stresses replace the closure's between the two kernels).
+static bool fused_sgs(const fe_domain* d) {
+  return d->sgsRows > 0 && d->kind == FE_KERNEL_MARCH && d->P.turb && !d->mlp;
+}
+
 // Everything a physics stage needs before its stage kernel, on state st: the SGS kernel and
 // surface layer, the learned closure's stresses (when a network is set) and, for the march
-// kernel, the SGS tendencies it reads. Returns the number of kernels launched.
-static int launch_physics(const fe_domain* d, cudaStream_t s, const float* st, int stage) {
+// kernel, the SGS tendencies it reads. With `store`, the closure's stresses and fluxes are left
+// in the scratch fields too (the fused kernel keeps them on chip otherwise). Returns the number
+// of kernels launched.
+static int launch_physics(const fe_domain* d, cudaStream_t s, const float* st, int stage, bool store = false) {
   const Phys& P = d->P;
+  if (fused_sgs(d)) {
+    // the surface layer first: the fused kernel reads its first-level stresses
+    if (P.surf > 0) fe::k_surface<<<dim3((P.Ny + 1 + 127) / 128, P.Nx + 1), 128, 0, s>>>(P, d->Q, st, stage);
+    launch_sgs_march(d, s, st, stage, store);
+    return P.surf > 0 ? 2 : 1;
+  }
   int l = launch_turb(d, s, st, stage);
   if (d->mlp && P.turb) {
     fe_learn_enqueue_tau(d->mlp, P, d->Q, st, s);
@@ -670,7 +748,7 @@ static void enqueue_step(fe_domain* d, cudaStream_t s, float* frhs = nullptr) {
   launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
   if (physPrep && stage_has_physics(d, 1)) d->launches += launch_physics(d, s, B, 1);
   launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
-  if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2);
+  if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2, frhs != nullptr);
   launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], frhs);
   fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
   d->launches += 4 + (split_last_stage(d) ? 1 : 0);
@@ -701,7 +779,9 @@ static int launches_per_step(const fe_domain* d) {
   const Phys& P = d->P;
   int l = 4 + (split_last_stage(d) ? 1 : 0) + (P.lsfSub ? 2 : 0);
   if (P.turb || P.surf > 0) {
-    const int phys = 2 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) + ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
+    const int phys = fused_sgs(d) ? 1 + (P.surf > 0)
+                                  : 2 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) +
+                                        ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
     l += (P.oneRK ? 1 : 3) * phys;
   }
   return l;
@@ -800,7 +880,7 @@ extern "C" int fe_build_frhs(fe_domain* d, int stage) {
   // the last stage's large-scale forcing on a forcing step uses the slab means of this state
   if (stage == 2 && P.lsfSub) d->launches += launch_slab_means(d, d->stream, A, A, false);
   if ((P.turb || P.surf > 0) && stage_has_physics(d, stage)) {
-    d->launches += launch_physics(d, d->stream, A, stage);
+    d->launches += launch_physics(d, d->stream, A, stage, true);
     CU(cudaGetLastError());
   }
   switch (stage) {
@@ -905,6 +985,14 @@ extern "C" int fe_set_stage_kernel(fe_domain* d, int kind, int tj, int ni) {
     d->mni = ni;
   }
   d->kind = kind;
+  invalidate_graph(d);
+  return FE_OK;
+}
+
+extern "C" int fe_set_sgs_kernel(fe_domain* d, int rows) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (rows != 0 && rows != 8 && rows != 16) return set_err(FE_ERR_ARG, "fused SGS kernel: rows must be 0, 8 or 16");
+  d->sgsRows = rows;
   invalidate_graph(d);
   return FE_OK;
 }

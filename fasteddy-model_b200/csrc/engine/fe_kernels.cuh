@@ -246,83 +246,153 @@ static __device__ void surface_column(const Phys& P, const Ptrs& Q, const float*
 }
 
 // ------------------------------------------------------------------ last-stage SGS physics
-// SGS physics of ring cell (i,j,k), given the length scale of the cell (lsc) and of the level
-// below (lsm) and sqrt(e/rho) of the level below (sem), all 0 without prognostic TKE; the
-// neighbours' primitive variables come from accessor `pr` (state or shared-memory tile).
+// The SGS physics of one ring point: the 9 stresses and heat fluxes (hydroTauFlds order), the
+// TKE transport fluxes (de/dx_j) Km rho, the moisture SGS fluxes (3 per species) and the length
+// scale. Computed at every level by turb_point(); the stresses and the stress-like moisture
+// fluxes are the closure's only at k >= kMin (at lower levels: stresses untouched = 0, moisture
+// fluxes the raw gradients, tke fluxes 0, as the reference's kernels leave them).
+struct TurbOut {
+  float tau[9];
+  float tkeQ[3];
+  float mtau[6];
+  float ls;
+};
+
+// SGS physics of ring point c = (i,j,k), given the length scale of the cell (lsc) and of the level
+// below (lsm) and sqrt(e/rho) of the level below (sem) and of the cell (sec; < 0: computed here),
+// all 0 without prognostic TKE; the neighbours' primitive variables come from accessor `pr` (state
+// or a shared-memory tile).
+template <class A>
+__device__ __forceinline__ void turb_point(const Phys& P, const Ptrs& Q, const A& pr, long long c, int k, float lsc,
+                                           float lsm, float sem, float sec, TurbOut& o) {
+#pragma unroll
+  for (int t = 0; t < 9; t++) o.tau[t] = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 3; t++) o.tkeQ[t] = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 6; t++) o.mtau[t] = 0.0f;
+  o.ls = lsc;
+  float Km = 0.0f;
+  const float delta = grid_scale(P, Q, c);
+  if (k >= P.kMin) {
+    const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
+    const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
+    // c, a = i-1, b = j-1, d = k-1 and their combinations
+    const float uc = pr.u(0, 0, 0), ua = pr.u(-1, 0, 0), ub = pr.u(0, -1, 0), ud = pr.u(0, 0, -1);
+    const float uab = pr.u(-1, -1, 0), uad = pr.u(-1, 0, -1), ubd = pr.u(0, -1, -1), uabd = pr.u(-1, -1, -1);
+    const float vc = pr.v(0, 0, 0), va = pr.v(-1, 0, 0), vb = pr.v(0, -1, 0), vd = pr.v(0, 0, -1);
+    const float vab = pr.v(-1, -1, 0), vad = pr.v(-1, 0, -1), vbd = pr.v(0, -1, -1), vabd = pr.v(-1, -1, -1);
+    const float wc = pr.w(0, 0, 0), wa = pr.w(-1, 0, 0), wb = pr.w(0, -1, 0), wd = pr.w(0, 0, -1);
+    const float wad = pr.w(-1, 0, -1), wbd = pr.w(0, -1, -1);
+    const float thc = pr.th(0, 0, 0), tha = pr.th(-1, 0, 0), thb = pr.th(0, -1, 0), thd = pr.th(0, 0, -1);
+    float S11 = dXi * (uc - ua);
+    float S22 = dYi * (vc - vb);
+    float S33 = J1 * dXi * (wc - wa) + J2 * dYi * (wc - wb) + J3 * dZi * (wc - wd);
+    float S21 = 0.5f * (0.5f * (dXi * (vc - va) + dXi * (vb - vab)) + 0.5f * (dYi * (uc - ub) + dYi * (ua - uab)));
+    float S31 = 0.5f * (0.5f * (dXi * (wc - wa) + dXi * (wd - wad)) + 0.5f * (J1 * dXi * (uc - ua) + J1 * dXi * (ud - uad)) +
+                        0.25f * (J2 * dYi * (uc - ub) + J2 * dYi * (ua - uab) + J2 * dYi * (ud - ubd) + J2 * dYi * (uad - uabd)) +
+                        0.5f * (J3 * dZi * (uc - ud) + J3 * dZi * (ua - uad)));
+    float S32 = 0.5f * (0.5f * (dYi * (wc - wb) + dYi * (wd - wbd)) +
+                        0.25f * (J1 * dXi * (vc - va) + J1 * dXi * (vb - vab) + J1 * dXi * (vd - vad) + J1 * dXi * (vbd - vabd)) +
+                        0.5f * (J2 * dYi * (vc - vb) + J2 * dYi * (vd - vbd)) + 0.5f * (J3 * dZi * (vc - vd) + J3 * dZi * (vb - vbd)));
+    float ST1 = dXi * (thc - tha);
+    float ST2 = dYi * (thc - thb);
+    float ST3 = (J1 * dXi * (thc - tha)) + (J2 * dYi * (thc - thb)) + (J3 * dZi * (thc - thd));
+    const float r = pr.r(0, 0, 0);
+    if (P.tke) {
+      const float e0 = pr.ev(0, 0, 0);
+      const float se0 = sec >= 0.0f ? sec : sqrtf(e0);  // sqrt(e/rho) of this cell (given by the tiled form)
+      Km = (float)((double)P.c_k * 0.5 * (double)(lsc * se0 + lsm * sem));
+      const float invPr = 1.0f + 2.0f * lsc / delta;
+      const float dev = (float)((2.0 / 3.0) * (double)r *
+                                (double)(Km * (dXi * (uc - ua) + dYi * (vc - vb) + J1 * dXi * (wc - wa) +
+                                               J2 * dYi * (wc - wb) + J3 * dZi * (wc - wd)) +
+                                         e0));
+      o.tau[0] = -2.0f * r * Km * S11 + dev;
+      o.tau[1] = -2.0f * r * Km * S21;
+      o.tau[4] = -2.0f * r * Km * S22 + dev;
+      o.tau[5] = -2.0f * r * Km * S33 + dev;
+      o.tau[6] = -r * Km * invPr * ST1;
+      o.tau[7] = -r * Km * invPr * ST2;
+      o.tau[2] = -2.0f * r * Km * S31;
+      o.tau[3] = -2.0f * r * Km * S32;
+      o.tau[8] = -r * Km * invPr * ST3;
+    } else {
+      const float t1 = 0.5f * (S11 * S11 + S22 * S22 + S33 * S33) + S21 * S21 + S31 * S31 + S32 * S32;
+      const float N2 = P.g / thc * ST3;
+      const float t2 = N2 * 3.0f;
+      Km = (P.c_s * delta) * (P.c_s * delta) * sqrtf(fmaxf(0.0f, t1 - fmaxf(0.0f, t2)));
+      const float invPr = 1.0f + 2.0f * delta / delta;
+      o.tau[0] = -2.0f * r * Km * S11;
+      o.tau[1] = -2.0f * r * Km * S21;
+      o.tau[4] = -2.0f * r * Km * S22;
+      o.tau[5] = -2.0f * r * Km * S33;
+      o.tau[6] = -r * Km * invPr * ST1;
+      o.tau[7] = -r * Km * invPr * ST2;
+      o.tau[2] = -2.0f * r * Km * S31;
+      o.tau[3] = -2.0f * r * Km * S32;
+      o.tau[8] = -r * Km * invPr * ST3;
+    }
+  }
+  if (P.tke) {
+    // TKE transport fluxes (de/dx_j)*Km*rho (cuda_sgstkeDevice.cu:309-397), Km = 0 below kMin
+    const float ex = pr.ev(1, 0, 0) - pr.ev(-1, 0, 0);
+    const float ey = pr.ev(0, 1, 0) - pr.ev(0, -1, 0);
+    const float ez = pr.ev(0, 0, 1) - pr.ev(0, 0, -1);
+    const float dedx = 0.5f * (P.dXi * ex);
+    const float dedy = 0.5f * (P.dYi * ey);
+    const float dedz = 0.5f * (Q.J31[c] * P.dXi * ex + Q.J32[c] * P.dYi * ey + Q.J33[c] * P.dZi * ez);
+    const float rc = pr.r(0, 0, 0);
+    o.tkeQ[0] = dedx * Km * rc;
+    o.tkeQ[1] = dedy * Km * rc;
+    o.tkeQ[2] = dedz * Km * rc;
+  }
+  if (P.moist && P.moistSGS > 0) {
+    const float invPr = 1.0f + 2.0f * (P.tke ? lsc : delta) / delta;
+    const float rc = pr.r(0, 0, 0);
+    for (int m = 0; m < P.nmoist && m < 2; m++) {
+      const float qc = pr.qm(m, 0, 0, 0), qa = pr.qm(m, -1, 0, 0);
+      const float qb = pr.qm(m, 0, -1, 0), qd = pr.qm(m, 0, 0, -1);
+      float g1 = P.dXi * (qc - qa);
+      float g2 = P.dYi * (qc - qb);
+      float g3 = Q.J31[c] * P.dXi * (qc - qa) + Q.J32[c] * P.dYi * (qc - qb) + Q.J33[c] * P.dZi * (qc - qd);
+      if (k >= P.kMin) {
+        g1 = -rc * Km * invPr * g1;
+        g2 = -rc * Km * invPr * g2;
+        g3 = -rc * Km * invPr * g3;
+      }
+      o.mtau[3 * m + 0] = g1;
+      o.mtau[3 * m + 1] = g2;
+      o.mtau[3 * m + 2] = g3;
+    }
+  }
+}
+
+// SGS physics of ring cell (i,j,k) stored to the scratch fields (turb_point), plus the learned
+// closure's inputs when a network is set and, with SURF, the surface layer of a first-level cell.
+// Without SURF (the surface layer in its own kernel) the first-level tau31, tau32, tauTH3 and q_v
+// flux of the surface columns are that kernel's: this cell leaves them alone.
 template <class A, bool SURF = true>
 __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const A& pr, const float* __restrict__ st, int i,
                                             int j, int k, float lsc, float lsm, float sem, float sec, int stage) {
   const long long n = P.n;
   const long long c = (long long)i * P.si + (long long)j * P.sj + k;
-  // with the surface layer in its own kernel (not SURF), the first-level tau31, tau32, tauTH3 and
-  // q_v flux of its columns are that kernel's: this cell leaves them alone
   const bool surfCell = !SURF && P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin;
   if (P.turb) {
+    TurbOut o;
+    turb_point(P, Q, pr, c, k, lsc, lsm, sem, sec, o);
     float* T = Q.tau;
-    float Km = 0.0f;
-    const float delta = grid_scale(P, Q, c);
     if (k >= P.kMin) {
-      const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
-      const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
-      // c, a = i-1, b = j-1, d = k-1 and their combinations
-      const float uc = pr.u(0, 0, 0), ua = pr.u(-1, 0, 0), ub = pr.u(0, -1, 0), ud = pr.u(0, 0, -1);
-      const float uab = pr.u(-1, -1, 0), uad = pr.u(-1, 0, -1), ubd = pr.u(0, -1, -1), uabd = pr.u(-1, -1, -1);
-      const float vc = pr.v(0, 0, 0), va = pr.v(-1, 0, 0), vb = pr.v(0, -1, 0), vd = pr.v(0, 0, -1);
-      const float vab = pr.v(-1, -1, 0), vad = pr.v(-1, 0, -1), vbd = pr.v(0, -1, -1), vabd = pr.v(-1, -1, -1);
-      const float wc = pr.w(0, 0, 0), wa = pr.w(-1, 0, 0), wb = pr.w(0, -1, 0), wd = pr.w(0, 0, -1);
-      const float wad = pr.w(-1, 0, -1), wbd = pr.w(0, -1, -1);
-      const float thc = pr.th(0, 0, 0), tha = pr.th(-1, 0, 0), thb = pr.th(0, -1, 0), thd = pr.th(0, 0, -1);
-      float S11 = dXi * (uc - ua);
-      float S22 = dYi * (vc - vb);
-      float S33 = J1 * dXi * (wc - wa) + J2 * dYi * (wc - wb) + J3 * dZi * (wc - wd);
-      float S21 = 0.5f * (0.5f * (dXi * (vc - va) + dXi * (vb - vab)) + 0.5f * (dYi * (uc - ub) + dYi * (ua - uab)));
-      float S31 = 0.5f * (0.5f * (dXi * (wc - wa) + dXi * (wd - wad)) + 0.5f * (J1 * dXi * (uc - ua) + J1 * dXi * (ud - uad)) +
-                          0.25f * (J2 * dYi * (uc - ub) + J2 * dYi * (ua - uab) + J2 * dYi * (ud - ubd) + J2 * dYi * (uad - uabd)) +
-                          0.5f * (J3 * dZi * (uc - ud) + J3 * dZi * (ua - uad)));
-      float S32 = 0.5f * (0.5f * (dYi * (wc - wb) + dYi * (wd - wbd)) +
-                          0.25f * (J1 * dXi * (vc - va) + J1 * dXi * (vb - vab) + J1 * dXi * (vd - vad) + J1 * dXi * (vbd - vabd)) +
-                          0.5f * (J2 * dYi * (vc - vb) + J2 * dYi * (vd - vbd)) + 0.5f * (J3 * dZi * (vc - vd) + J3 * dZi * (vb - vbd)));
-      float ST1 = dXi * (thc - tha);
-      float ST2 = dYi * (thc - thb);
-      float ST3 = (J1 * dXi * (thc - tha)) + (J2 * dYi * (thc - thb)) + (J3 * dZi * (thc - thd));
-      const float r = pr.r(0, 0, 0);
-      if (P.tke) {
-        const float e0 = pr.ev(0, 0, 0);
-        const float se0 = sec >= 0.0f ? sec : sqrtf(e0);  // sqrt(e/rho) of this cell (given by the tiled form)
-        Km = (float)((double)P.c_k * 0.5 * (double)(lsc * se0 + lsm * sem));
-        const float invPr = 1.0f + 2.0f * lsc / delta;
-        const float dev = (float)((2.0 / 3.0) * (double)r *
-                                  (double)(Km * (dXi * (uc - ua) + dYi * (vc - vb) + J1 * dXi * (wc - wa) +
-                                                 J2 * dYi * (wc - wb) + J3 * dZi * (wc - wd)) +
-                                           e0));
-        T[c] = -2.0f * r * Km * S11 + dev;
-        T[n + c] = -2.0f * r * Km * S21;
-        T[4 * n + c] = -2.0f * r * Km * S22 + dev;
-        T[5 * n + c] = -2.0f * r * Km * S33 + dev;
-        T[6 * n + c] = -r * Km * invPr * ST1;
-        T[7 * n + c] = -r * Km * invPr * ST2;
-        if (!surfCell) {
-          T[2 * n + c] = -2.0f * r * Km * S31;
-          T[3 * n + c] = -2.0f * r * Km * S32;
-          T[8 * n + c] = -r * Km * invPr * ST3;
-        }
-      } else {
-        const float t1 = 0.5f * (S11 * S11 + S22 * S22 + S33 * S33) + S21 * S21 + S31 * S31 + S32 * S32;
-        const float N2 = P.g / thc * ST3;
-        const float t2 = N2 * 3.0f;
-        Km = (P.c_s * delta) * (P.c_s * delta) * sqrtf(fmaxf(0.0f, t1 - fmaxf(0.0f, t2)));
-        const float invPr = 1.0f + 2.0f * delta / delta;
-        T[c] = -2.0f * r * Km * S11;
-        T[n + c] = -2.0f * r * Km * S21;
-        T[4 * n + c] = -2.0f * r * Km * S22;
-        T[5 * n + c] = -2.0f * r * Km * S33;
-        T[6 * n + c] = -r * Km * invPr * ST1;
-        T[7 * n + c] = -r * Km * invPr * ST2;
-        if (!surfCell) {
-          T[2 * n + c] = -2.0f * r * Km * S31;
-          T[3 * n + c] = -2.0f * r * Km * S32;
-          T[8 * n + c] = -r * Km * invPr * ST3;
-        }
+      T[c] = o.tau[0];
+      T[n + c] = o.tau[1];
+      T[4 * n + c] = o.tau[4];
+      T[5 * n + c] = o.tau[5];
+      T[6 * n + c] = o.tau[6];
+      T[7 * n + c] = o.tau[7];
+      if (!surfCell) {
+        T[2 * n + c] = o.tau[2];
+        T[3 * n + c] = o.tau[3];
+        T[8 * n + c] = o.tau[8];
       }
     }
     if (Q.feat && k >= P.kMin) {
@@ -334,35 +404,15 @@ __device__ __forceinline__ void turb_cell_a(const Phys& P, const Ptrs& Q, const 
     }
     if (P.tke) {
       Q.ls[c] = lsc;
-      // TKE transport fluxes (de/dx_j)*Km*rho (cuda_sgstkeDevice.cu:309-397), Km = 0 below kMin
-      const float ex = pr.ev(1, 0, 0) - pr.ev(-1, 0, 0);
-      const float ey = pr.ev(0, 1, 0) - pr.ev(0, -1, 0);
-      const float ez = pr.ev(0, 0, 1) - pr.ev(0, 0, -1);
-      const float dedx = 0.5f * (P.dXi * ex);
-      const float dedy = 0.5f * (P.dYi * ey);
-      const float dedz = 0.5f * (Q.J31[c] * P.dXi * ex + Q.J32[c] * P.dYi * ey + Q.J33[c] * P.dZi * ez);
-      const float rc = pr.r(0, 0, 0);
-      Q.tkeQ[c] = dedx * Km * rc;
-      Q.tkeQ[n + c] = dedy * Km * rc;
-      Q.tkeQ[2 * n + c] = dedz * Km * rc;
+      Q.tkeQ[c] = o.tkeQ[0];
+      Q.tkeQ[n + c] = o.tkeQ[1];
+      Q.tkeQ[2 * n + c] = o.tkeQ[2];
     }
     if (P.moist && P.moistSGS > 0) {
-      const float invPr = 1.0f + 2.0f * (P.tke ? lsc : delta) / delta;
-      const float rc = pr.r(0, 0, 0);
-      for (int m = 0; m < P.nmoist; m++) {
-        const float qc = pr.qm(m, 0, 0, 0), qa = pr.qm(m, -1, 0, 0);
-        const float qb = pr.qm(m, 0, -1, 0), qd = pr.qm(m, 0, 0, -1);
-        float g1 = P.dXi * (qc - qa);
-        float g2 = P.dYi * (qc - qb);
-        float g3 = Q.J31[c] * P.dXi * (qc - qa) + Q.J32[c] * P.dYi * (qc - qb) + Q.J33[c] * P.dZi * (qc - qd);
-        if (k >= P.kMin) {
-          g1 = -rc * Km * invPr * g1;
-          g2 = -rc * Km * invPr * g2;
-          g3 = -rc * Km * invPr * g3;
-        }
-        Q.mtau[(3 * m + 0) * n + c] = g1;
-        Q.mtau[(3 * m + 1) * n + c] = g2;
-        if (!(surfCell && m == 0)) Q.mtau[(3 * m + 2) * n + c] = g3;
+      for (int m = 0; m < P.nmoist && m < 2; m++) {
+        Q.mtau[(3 * m + 0) * n + c] = o.mtau[3 * m + 0];
+        Q.mtau[(3 * m + 1) * n + c] = o.mtau[3 * m + 1];
+        if (!(surfCell && m == 0)) Q.mtau[(3 * m + 2) * n + c] = o.mtau[3 * m + 2];
       }
     }
   }

@@ -122,6 +122,20 @@ __device__ __forceinline__ int f_sel(const Phys& P, int s) {
   else if constexpr (FL != FL_ANY) return s == SL_QL ? 5 : 3;
   else return slot_sel(P, s);
 }
+// Fields s and s + 1 (s even) evaluate their x faces as one lane pair: both present and on the
+// same scheme of the packed path, known at compile time. The moist flavours only: in the dry
+// flavour the pairs cost more registers than the 128 the launch shape allows (spills).
+template <int FL>
+__host__ __device__ constexpr bool x_paired(int s) {
+  if constexpr (FL == FL_ANY || FL == FL_DRY) {
+    return false;
+  } else {
+    if (s % 2 != 0 || s + 1 > SL_QL) return false;
+    const int a = FL == FL_MOIST34 ? (s == SL_QL ? 5 : (s == SL_QV ? 2 : 3)) : (s == SL_QL ? 5 : 3);
+    const int b = FL == FL_MOIST34 ? (s + 1 == SL_QL ? 5 : (s + 1 == SL_QV ? 2 : 3)) : (s + 1 == SL_QL ? 5 : 3);
+    return a == b && (a == ADV_HYB56 || a == ADV_WENO5);
+  }
+}
 template <int FL>
 __device__ __forceinline__ const float* f_src(const Phys& P, const float* cur, const float* pcur, int s) {
   if constexpr (FL != FL_ANY) {
@@ -190,8 +204,9 @@ __global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float
     const float ce = (float)(1.9 * (double)P.c_k + (0.93 - 1.9 * (double)P.c_k) * (double)lsc / (double)delta);
     const float ec = mec * ri;
     Se = Se + (-ce * mec * sqrtf(ec) / lsc);
-    // (rho phi)/rho of field f at the neighbour c + o
-    auto G = [&](int f, long long o) -> float { return st[f * n + c + o] * rinv(st[c + o]); };
+    // (rho phi)/rho of field f at the neighbour c + o, rounded on its own (as the fused SGS kernel's
+    // shared-memory primitives are), so the differences below are not contracted into FMAs
+    auto G = [&](int f, long long o) -> float { return __fmul_rn(st[f * n + c + o], rinv(st[c + o])); };
     const float ux = G(1, si) - G(1, -si), uy = G(1, sj) - G(1, -sj), uz = G(1, 1) - G(1, -1);
     const float vx = G(2, si) - G(2, -si), vy = G(2, sj) - G(2, -sj), vz = G(2, 1) - G(2, -1);
     const float wx = G(3, si) - G(3, -si), wy = G(3, sj) - G(3, -sj), wz = G(3, 1) - G(3, -1);
@@ -535,6 +550,7 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     }
 
     // advection of every field (cuda_hydroCoreDevice.cu:631-736; WENO3/WENO5 as x, y, z updates)
+    float fxNext = 0.0f;  // x face of field s + 1 when it was evaluated with field s
 #pragma unroll
     for (int s = 0; s < 8; s++) {
       if (!f_on<FL>(P, s)) continue;
@@ -543,18 +559,52 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
       const float xm2 = ns[s * PLANE + own], xm1 = ps[s * PLANE + own];
       const int sel = f_sel<FL>(P, s);
       const float bf = adv_split(sel) ? 1.0f : 1.0f - slot_b(P, s);
-      const float fxp = adv_face<true>(sel, xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
+      // the x faces of an even and the following odd field as a lane pair when both use the same
+      // packed scheme (compile-time flavours only)
+      float fxp;
+      if (x_paired<FL>(s)) {
+        const int s1 = s + 1;
+        const float bf1 = adv_split(sel) ? 1.0f : 1.0f - slot_b(P, s1);
+        const float2 fx = adv_face2<true>(sel, f2(xm2, ns[s1 * PLANE + own]), f2(xm1, ps[s1 * PLANE + own]),
+                                          f2(z0, w[s1][0]), f2(w[s][1], w[s1][1]), f2(w[s][2], w[s1][2]),
+                                          f2(w[s][3], w[s1][3]), f2s(up), f2(bf, bf1));
+        fxp = fx.x;
+        fxNext = fx.y;
+      } else if (s > 0 && x_paired<FL>(s - 1)) {
+        fxp = fxNext;
+      } else {
+        fxp = adv_face<true>(sel, xm2, xm1, z0, w[s][1], w[s][2], w[s][3], up, bf);
+      }
       const float pxp = __fmul_rn(up, fxp);
       const float Dx = __fsub_rn(pxp, xcs[s * T::NT + tid]);
       xcs[s * T::NT + tid] = pxp;
+      // moist flavours: the two y faces, then the two z faces, as lane pairs (upper face, lower
+      // face) on the packed pipe; the other flavours face by face (their register budget has no
+      // room for the pairs)
       float Dy, Dz;
       {
         const float m3 = pl[-3 * PK], m2 = pl[-2 * PK], m1 = pl[-PK], p1 = pl[PK], p2 = pl[2 * PK], p3 = pl[3 * PK];
-        Dy = vp * adv_face<true>(sel, m2, m1, z0, p1, p2, p3, vp, bf) - vm * adv_face<true>(sel, m3, m2, m1, z0, p1, p2, vm, bf);
+        if constexpr (FL == FL_MOIST || FL == FL_MOIST34) {
+          const float2 v2 = f2(vp, vm);
+          const float2 fy = adv_face2<true>(sel, f2(m2, m3), f2(m1, m2), f2(z0, m1), f2(p1, z0), f2(p2, p1), f2(p3, p2),
+                                            v2, f2s(bf));
+          const float2 py = mul2(v2, fy);
+          Dy = __fsub_rn(py.x, py.y);
+        } else {
+          Dy = vp * adv_face<true>(sel, m2, m1, z0, p1, p2, p3, vp, bf) - vm * adv_face<true>(sel, m3, m2, m1, z0, p1, p2, vm, bf);
+        }
       }
       {
         const float m3 = pl[-3], m2 = pl[-2], m1 = pl[-1], p1 = pl[1], p2 = pl[2], p3 = pl[3];
-        Dz = wp * adv_face<true>(sel, m2, m1, z0, p1, p2, p3, wp, bf) - wm * adv_face<true>(sel, m3, m2, m1, z0, p1, p2, wm, bf);
+        if constexpr (FL == FL_MOIST || FL == FL_MOIST34) {
+          const float2 w2 = f2(wp, wm);
+          const float2 fz = adv_face2<true>(sel, f2(m2, m3), f2(m1, m2), f2(z0, m1), f2(p1, z0), f2(p2, p1), f2(p3, p2),
+                                            w2, f2s(bf));
+          const float2 pz = mul2(w2, fz);
+          Dz = __fsub_rn(pz.x, pz.y);
+        } else {
+          Dz = wp * adv_face<true>(sel, m2, m1, z0, p1, p2, p3, wp, bf) - wm * adv_face<true>(sel, m3, m2, m1, z0, p1, p2, wm, bf);
+        }
         // the explicit filter of rho w reads the same column; it is added after every other term
         if (s == 3 && P.filt) fw = filter6_tend(m3, m2, m1, z0, p1, p2, p3, P.filtCoef);
       }

@@ -146,6 +146,7 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_domain_means", ip, [vp, c_double_p]),
         ("fe_set_tiling", ip, [vp, ip, ip, ip]),
         ("fe_set_stage_kernel", ip, [vp, ip, ip, ip]),
+        ("fe_set_sgs_kernel", ip, [vp, ip]),
         ("fe_get_stage_kernel", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_autotune", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_launch_count", ctypes.c_longlong, [vp]),
@@ -194,6 +195,18 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
     _declare(refabi, "fe_refabi_fill_config", None, [ctypes.POINTER(FeConfig)])
     _LIBS.update(host=host, engine=engine, refabi=refabi)
     return _LIBS
+
+
+def pin(a: Optional[np.ndarray]) -> None:
+    """Page-lock a host array (cudaHostRegister) so copies to and from the device run at full
+    link speed; undo with unpin() before the array is freed."""
+    if a is not None:
+        _check(load()["engine"].fe_host_register(a.ctypes.data_as(ctypes.c_void_p), a.nbytes), "fe_host_register")
+
+
+def unpin(a: Optional[np.ndarray]) -> None:
+    if a is not None:
+        _check(load()["engine"].fe_host_unregister(a.ctypes.data_as(ctypes.c_void_p)), "fe_host_unregister")
 
 
 def _fptr(a: Optional[np.ndarray]):
@@ -383,12 +396,19 @@ class Domain:
     def stream(self) -> int:
         return int(self.e.fe_stream(self.h) or 0)
 
-    def get_state(self) -> dict[str, np.ndarray]:
+    def state_buffers(self) -> dict[str, np.ndarray]:
+        """Empty host arrays of the shapes get_state() returns (to pass as `out`)."""
         nx, ny, nz = self.shape
-        hydro = np.empty((5, nx, ny, nz), np.float32)
-        tke = np.empty((1, nx, ny, nz), np.float32) if self.ntke else None
-        moist = np.empty((self.nmoist, nx, ny, nz), np.float32) if self.nmoist else None
-        pres = np.empty((nx, ny, nz), np.float32)
+        return {"hydroFlds": np.empty((5, nx, ny, nz), np.float32),
+                "sgstke": np.empty((1, nx, ny, nz), np.float32) if self.ntke else None,
+                "moist": np.empty((self.nmoist, nx, ny, nz), np.float32) if self.nmoist else None,
+                "pres": np.empty((nx, ny, nz), np.float32)}
+
+    def get_state(self, out: dict | None = None) -> dict[str, np.ndarray]:
+        """The state (flux form, reference layout) and perturbation pressure; into `out`
+        (from state_buffers(), e.g. page-locked with pin()) when given."""
+        b = out if out is not None else self.state_buffers()
+        hydro, tke, moist, pres = b["hydroFlds"], b["sgstke"], b["moist"], b["pres"]
         _check(self.e.fe_get_state(self.h, _fptr(hydro), _fptr(tke), _fptr(moist), _fptr(pres)), "fe_get_state")
         return {"hydroFlds": hydro, "sgstke": tke, "moist": moist, "pres": pres}
 
@@ -493,6 +513,11 @@ class Domain:
         """kind 'march' (tiles of 32 levels x tj rows marching ni planes) or 'cell'."""
         code = {"cell": KERNEL_CELL, "march": KERNEL_MARCH}[kind]
         _check(self.e.fe_set_stage_kernel(self.h, code, tj, ni), "fe_set_stage_kernel")
+
+    def set_sgs_kernel(self, rows: int) -> None:
+        """Last-stage SGS physics as one fused kernel with tiles of `rows` rows (8 or 16), or
+        (rows = 0) as the separate kernels."""
+        _check(self.e.fe_set_sgs_kernel(self.h, int(rows)), "fe_set_sgs_kernel")
 
     def stage_kernel(self) -> tuple[str, int, int]:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -206,6 +206,12 @@ int fe_set_tiling(fe_domain *d, int tk, int tj, int ti);
 #define FE_KERNEL_MARCH 1
 int fe_set_stage_kernel(fe_domain *d, int kind, int tj, int ni);
 int fe_get_stage_kernel(const fe_domain *d, int *kind, int *tj, int *ni);
+/* Form of the last RK stage's SGS physics with the march stage kernel: rows = 8 or 16 evaluates
+ * the closure's stresses and fluxes and the tendencies they give in one i-marching kernel with
+ * tiles of 32 levels x rows that keeps them on chip; 0 runs them as separate kernels through the
+ * scratch fields (the form the learned closure and the per-cell stage kernel always use). Results
+ * are equal bit for bit. */
+int fe_set_sgs_kernel(fe_domain *d, int rows);
 /* Pick the stage-kernel form and launch shape by timing the candidates (the autotuner);
  * tk/tj/ti receive the cell-kernel tiling, fe_get_stage_kernel the chosen form. */
 int fe_autotune(fe_domain *d, int *tk, int *tj, int *ti);

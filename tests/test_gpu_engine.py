@@ -370,6 +370,41 @@ def test_dropin_batch_copies_back_tendencies_and_sgs_fluxes(fe):
     host.cleanup()
 
 
+@pytest.mark.parametrize("name", list(CASES) + ["bomex"])
+def test_fused_sgs_kernel_equals_kernel_chain(fe, name):
+    """The last stage's SGS physics as one fused kernel (the default with the march stage kernel)
+    and as the kernel chain (closure into scratch fields, then the tendencies): the same state after
+    10 steps bit for bit, and the same tendencies and stresses of a physics stage."""
+    if name == "bomex":
+        host = fe.cases.setup_host("bomex", 24, 20, 16)
+        inp, cfg = host.inputs(), host.config()
+    else:
+        host, inp, cfg = _setup(fe, name, nx=37, ny=13, nz=45)  # ragged tiles
+    a = fe.Domain(cfg)
+    a.set_inputs(inp)
+    b = fe.Domain(cfg)
+    b.set_inputs(inp)
+    b.set_sgs_kernel(0)
+    c = fe.Domain(cfg)
+    c.set_inputs(inp)
+    c.set_sgs_kernel(16)
+    fa, fb, fc = a.build_frhs(2), b.build_frhs(2), c.build_frhs(2)
+    for key in ("hydroFrhs", "sgstkeFrhs", "moistFrhs", "taus"):
+        if fa.get(key) is not None:
+            np.testing.assert_array_equal(interior(fa[key]), interior(fb[key]), err_msg=key)
+            np.testing.assert_array_equal(interior(fc[key]), interior(fb[key]), err_msg=key)
+    for dom in (a, b, c):
+        dom.advance(10)
+    sa, sb, sc = a.get_state(), b.get_state(), c.get_state()
+    for key in ("hydroFlds", "sgstke", "moist"):
+        if sa.get(key) is not None:
+            np.testing.assert_array_equal(sa[key], sb[key], err_msg=key)
+            np.testing.assert_array_equal(sc[key], sb[key], err_msg=key)
+    for dom in (a, b, c):
+        dom.close()
+    host.cleanup()
+
+
 def test_nonfinite_state_is_reported(fe):
     host, inp, cfg = _setup(fe, "cbl_dry")
     libs = fe.load()

@@ -468,7 +468,7 @@ def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
     t0 = time.perf_counter()
     for d, inp in zip(doms, inputs):
         d.set_state(inp["hydroFlds"], inp.get("sgstke"), inp.get("moist"))
-    ens.advance(steps, sync=False)
+    ens.advance(steps)
     for d, o in zip(doms, outs):
         d.get_state(out=o)
     t1 = time.perf_counter()

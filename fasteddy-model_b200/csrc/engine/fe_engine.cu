@@ -454,16 +454,21 @@ static int finish_state(fe_domain* d);
 // ------------------------------------------------------------------ checkpoint / resume
 // A checkpoint holds everything a step reads that a step also changes: the prognostic state A,
 // the 11 surface planes (the surface layer starts from the previous drag, friction velocity,
-// Obukhov length, fluxes and skin values) and the clock. Scratch, the intermediate stage
-// states and the perturbation pressure are rebuilt from these on load, so a resumed run repeats
-// the continuous one bit for bit.
+// Obukhov length, fluxes and skin values), the clock and, with slab-mean subsidence, the third
+// state buffer (the next forcing step's slab means read its halo cells: the previous step's
+// last-stage input). Scratch, the second state buffer and the perturbation pressure are rebuilt
+// on load, so a resumed run repeats the continuous one bit for bit. Version 2 records whether the
+// third buffer is present; a checkpoint loads only into a domain of the same shape, field set and
+// subsidence setting.
 namespace {
 struct CkptHeader {
   char magic[8];
   int version, Nx, Ny, Nz, nf, simIt;
   float simTime;
-  int pad[8];
+  int lsfSub;  // 1: the third state buffer follows the surface planes
+  int pad[7];
 };
+constexpr int kCkptVersion = 2;
 const char kCkptMagic[8] = {'F', 'E', 'B', '2', '0', '0', 'C', 'K'};
 }  // namespace
 
@@ -484,7 +489,8 @@ extern "C" int fe_checkpoint_save(fe_domain* d, void* buf, size_t bytes) {
   CkptHeader h;
   std::memset(&h, 0, sizeof(h));
   std::memcpy(h.magic, kCkptMagic, 8);
-  h.version = 1; h.Nx = d->P.Nx; h.Ny = d->P.Ny; h.Nz = d->P.Nz; h.nf = d->P.nf;
+  h.version = kCkptVersion; h.Nx = d->P.Nx; h.Ny = d->P.Ny; h.Nz = d->P.Nz; h.nf = d->P.nf;
+  h.lsfSub = d->P.lsfSub ? 1 : 0;
   h.simIt = d->simIt; h.simTime = d->simTime;
   std::memcpy(buf, &h, sizeof(h));
   float* f = reinterpret_cast<float*>(static_cast<char*>(buf) + sizeof(h));
@@ -502,9 +508,12 @@ extern "C" int fe_checkpoint_load(fe_domain* d, const void* buf, size_t bytes) {
   if (bytes < sizeof(CkptHeader)) return set_err(FE_ERR_ARG, "checkpoint too short");
   CkptHeader h;
   std::memcpy(&h, buf, sizeof(h));
-  if (std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1) return set_err(FE_ERR_ARG, "not a checkpoint of this engine");
+  if (std::memcmp(h.magic, kCkptMagic, 8) != 0) return set_err(FE_ERR_ARG, "not a checkpoint of this engine");
+  if (h.version != kCkptVersion) return set_err(FE_ERR_ARG, "checkpoint of another format version");
   if (h.Nx != d->P.Nx || h.Ny != d->P.Ny || h.Nz != d->P.Nz || h.nf != d->P.nf)
     return set_err(FE_ERR_ARG, "checkpoint of a different domain shape or field set");
+  if (h.lsfSub != (d->P.lsfSub ? 1 : 0))
+    return set_err(FE_ERR_ARG, "checkpoint of a domain with a different large-scale subsidence setting");
   if (bytes < fe_checkpoint_bytes(d)) return set_err(FE_ERR_ARG, "checkpoint too short");
   CU(cudaSetDevice(d->device));
   const float* f = reinterpret_cast<const float*>(static_cast<const char*>(buf) + sizeof(h));
@@ -1332,6 +1341,14 @@ extern "C" int fe_ensemble_advance(fe_ensemble* e, int nsteps) {
       cudaEventDestroy(done);
     }
     cudaEventDestroy(fork);
+  }
+  // later work on a member's own stream (fe_get_state, fe_advance, ...) waits for the ensemble's
+  {
+    cudaEvent_t done;
+    CU(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    cudaEventRecord(done, e->stream);
+    for (auto* d : e->m) cudaStreamWaitEvent(d->stream, done, 0);
+    cudaEventDestroy(done);
   }
   CU(cudaGetLastError());
   for (auto* d : e->m)

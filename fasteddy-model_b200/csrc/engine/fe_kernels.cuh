@@ -84,13 +84,21 @@ static __global__ void k_pressure(Phys P, Ptrs Q, const float* __restrict__ st, 
 }
 
 // SGS length scale at cell c + dk (cuda_sgstkeDevice.cu:96-151), from primitives.
+// The metric terms and grid scale of one point (the values the SGS helpers below read at c).
+struct PointMetrics {
+  float J1, J2, J3, delta;
+};
+__device__ __forceinline__ PointMetrics point_metrics(const Phys& P, const Ptrs& Q, long long c) {
+  return {Q.J31[c], Q.J32[c], Q.J33[c], grid_scale(P, Q, c)};
+}
+
 template <class A>
-__device__ __forceinline__ float length_scale_a(const Phys& P, const Ptrs& Q, const A& pr, long long c, int dk) {
-  const float dthdz = (float)(0.5 * (double)((Q.J31[c] * P.dXi * (pr.th(1, 0, dk) - pr.th(-1, 0, dk))) +
-                                             (Q.J32[c] * P.dYi * (pr.th(0, 1, dk) - pr.th(0, -1, dk))) +
-                                             (Q.J33[c] * P.dZi * (pr.th(0, 0, dk + 1) - pr.th(0, 0, dk - 1)))));
+__device__ __forceinline__ float length_scale_m(const Phys& P, const A& pr, int dk, const PointMetrics& m) {
+  const float dthdz = (float)(0.5 * (double)((m.J1 * P.dXi * (pr.th(1, 0, dk) - pr.th(-1, 0, dk))) +
+                                             (m.J2 * P.dYi * (pr.th(0, 1, dk) - pr.th(0, -1, dk))) +
+                                             (m.J3 * P.dZi * (pr.th(0, 0, dk + 1) - pr.th(0, 0, dk - 1)))));
   const float N2 = (P.g / pr.th(0, 0, dk)) * dthdz;
-  const float len2 = grid_scale(P, Q, c);
+  const float len2 = m.delta;
   if (N2 > 0.0f) {
     const float tb = 1.0f / sqrtf(N2);  // N2^(-1/2): two correctly rounded operations
     const float ec = pr.ev(0, 0, dk);
@@ -98,6 +106,11 @@ __device__ __forceinline__ float length_scale_a(const Phys& P, const Ptrs& Q, co
     return fmaxf(fminf(len1, len2), 1e-2f);
   }
   return len2;
+}
+
+template <class A>
+__device__ __forceinline__ float length_scale_a(const Phys& P, const Ptrs& Q, const A& pr, long long c, int dk) {
+  return length_scale_m(P, pr, dk, point_metrics(P, Q, c));
 }
 
 __device__ __forceinline__ float length_scale(const Phys& P, const Ptrs& Q, const float* __restrict__ rho,
@@ -263,8 +276,17 @@ struct TurbOut {
 // all 0 without prognostic TKE; the neighbours' primitive variables come from accessor `pr` (state
 // or a shared-memory tile).
 template <class A>
+__device__ __forceinline__ void turb_point_m(const Phys& P, const A& pr, int k, float lsc, float lsm, float sem,
+                                             float sec, const PointMetrics& mt, TurbOut& o);
+template <class A>
 __device__ __forceinline__ void turb_point(const Phys& P, const Ptrs& Q, const A& pr, long long c, int k, float lsc,
                                            float lsm, float sem, float sec, TurbOut& o) {
+  turb_point_m(P, pr, k, lsc, lsm, sem, sec, point_metrics(P, Q, c), o);
+}
+// turb_point() with the point's metric terms and grid scale given.
+template <class A>
+__device__ __forceinline__ void turb_point_m(const Phys& P, const A& pr, int k, float lsc, float lsm, float sem,
+                                             float sec, const PointMetrics& mt, TurbOut& o) {
 #pragma unroll
   for (int t = 0; t < 9; t++) o.tau[t] = 0.0f;
 #pragma unroll
@@ -273,9 +295,9 @@ __device__ __forceinline__ void turb_point(const Phys& P, const Ptrs& Q, const A
   for (int t = 0; t < 6; t++) o.mtau[t] = 0.0f;
   o.ls = lsc;
   float Km = 0.0f;
-  const float delta = grid_scale(P, Q, c);
+  const float delta = mt.delta;
   if (k >= P.kMin) {
-    const float J1 = Q.J31[c], J2 = Q.J32[c], J3 = Q.J33[c];
+    const float J1 = mt.J1, J2 = mt.J2, J3 = mt.J3;
     const float dXi = P.dXi, dYi = P.dYi, dZi = P.dZi;
     // c, a = i-1, b = j-1, d = k-1 and their combinations
     const float uc = pr.u(0, 0, 0), ua = pr.u(-1, 0, 0), ub = pr.u(0, -1, 0), ud = pr.u(0, 0, -1);
@@ -341,7 +363,7 @@ __device__ __forceinline__ void turb_point(const Phys& P, const Ptrs& Q, const A
     const float ez = pr.ev(0, 0, 1) - pr.ev(0, 0, -1);
     const float dedx = 0.5f * (P.dXi * ex);
     const float dedy = 0.5f * (P.dYi * ey);
-    const float dedz = 0.5f * (Q.J31[c] * P.dXi * ex + Q.J32[c] * P.dYi * ey + Q.J33[c] * P.dZi * ez);
+    const float dedz = 0.5f * (mt.J1 * P.dXi * ex + mt.J2 * P.dYi * ey + mt.J3 * P.dZi * ez);
     const float rc = pr.r(0, 0, 0);
     o.tkeQ[0] = dedx * Km * rc;
     o.tkeQ[1] = dedy * Km * rc;
@@ -355,7 +377,7 @@ __device__ __forceinline__ void turb_point(const Phys& P, const Ptrs& Q, const A
       const float qb = pr.qm(m, 0, -1, 0), qd = pr.qm(m, 0, 0, -1);
       float g1 = P.dXi * (qc - qa);
       float g2 = P.dYi * (qc - qb);
-      float g3 = Q.J31[c] * P.dXi * (qc - qa) + Q.J32[c] * P.dYi * (qc - qb) + Q.J33[c] * P.dZi * (qc - qd);
+      float g3 = mt.J1 * P.dXi * (qc - qa) + mt.J2 * P.dYi * (qc - qb) + mt.J3 * P.dZi * (qc - qd);
       if (k >= P.kMin) {
         g1 = -rc * Km * invPr * g1;
         g2 = -rc * Km * invPr * g2;

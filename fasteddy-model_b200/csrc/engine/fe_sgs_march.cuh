@@ -36,7 +36,7 @@ struct SgsTile {
   static constexpr int PHJ = TJ + 2, PHK = SG_K + 2, PHN = PHJ * PHK;  // rows j0-1.., levels k0-1..
   static constexpr int NPH = 19;                                     // tau 0..8, tkeQ 9..11, mtau 12..17, ls 18
   static constexpr int LSK = SG_K + 3, LSN = PHJ * LSK;              // levels k0-2..k0+32
-  static constexpr int FLOATS = 3 * NPF * PRN + 2 * NPH * PHN + 2 * LSN;
+  static constexpr int FLOATS = 3 * NPF * PRN + 2 * NPH * PHN + 2 * LSN + 4 * LSN;  // + J31, J32, J33, delta
   static constexpr int SMEM_BYTES = FLOATS * 4;
 };
 
@@ -121,12 +121,54 @@ __device__ __forceinline__ void sgs_load_plane(const Phys& P, const float* __res
   sgs_put_plane<TJ>(tid, r, dst);
 }
 
+// The metric terms and grid scale of plane i for rows j0-1..j0+TJ, levels k0-2..k0+32 (the points
+// the length scales and the physics of the plane read), fetched into registers ahead of use and
+// then put into a shared-memory table [4][LSN].
+template <int TJ>
+struct MetricRegs {
+  static constexpr int PER = (SgsTile<TJ>::LSN + SgsTile<TJ>::NT - 1) / SgsTile<TJ>::NT;
+  PointMetrics m[PER];
+};
+template <int TJ>
+__device__ __forceinline__ void sgs_fetch_metrics(const Phys& P, const Ptrs& Q, int i, int j0, int k0, int tid,
+                                                  MetricRegs<TJ>& r) {
+  using T = SgsTile<TJ>;
+#pragma unroll
+  for (int e = 0; e < MetricRegs<TJ>::PER; e++) {
+    const int q = tid + e * T::NT;
+    const int row = q / T::LSK, lv = q - row * T::LSK;
+    const int j = j0 - 1 + row, k = k0 - 2 + lv;
+    r.m[e] = PointMetrics{0.0f, 0.0f, 0.0f, 0.0f};
+    if (q < T::LSN && i < P.nxh && j < P.nyh && k < P.nzh)
+      r.m[e] = point_metrics(P, Q, (long long)i * P.si + (long long)j * P.sj + k);
+  }
+}
+template <int TJ>
+__device__ __forceinline__ void sgs_put_metrics(int tid, const MetricRegs<TJ>& r, float* __restrict__ dst) {
+  using T = SgsTile<TJ>;
+#pragma unroll
+  for (int e = 0; e < MetricRegs<TJ>::PER; e++) {
+    const int q = tid + e * T::NT;
+    if (q < T::LSN) {
+      dst[q] = r.m[e].J1;
+      dst[T::LSN + q] = r.m[e].J2;
+      dst[2 * T::LSN + q] = r.m[e].J3;
+      dst[3 * T::LSN + q] = r.m[e].delta;
+    }
+  }
+}
+template <int TJ>
+__device__ __forceinline__ PointMetrics sgs_metrics_at(const float* mt, int q) {
+  constexpr int L = SgsTile<TJ>::LSN;
+  return PointMetrics{mt[q], mt[L + q], mt[2 * L + q], mt[3 * L + q]};
+}
+
 // Length scale and sqrt(e/rho) of plane i (prims planes pm, p0, pp) for rows j0-1..j0+TJ and
 // levels k0-2..k0+32 (0 outside the ring [iMin-1, iMax] x [jMin-1, jMax] x [1, kMax]).
 template <int TJ>
 __device__ __forceinline__ void sgs_length_scales(const Phys& P, const Ptrs& Q, int i, int j0, int k0, int tid,
                                                   const float* pm, const float* p0, const float* pp, float* lsT,
-                                                  float* seT) {
+                                                  float* seT, const float* mt) {
   using T = SgsTile<TJ>;
   for (int q = tid; q < T::LSN; q += T::NT) {
     const int row = q / T::LSK, lv = q - row * T::LSK;
@@ -135,7 +177,8 @@ __device__ __forceinline__ void sgs_length_scales(const Phys& P, const Ptrs& Q, 
     if (i >= P.iMin - 1 && i <= P.iMax && j >= P.jMin - 1 && j <= P.jMax && k >= 1 && k <= P.kMax) {
       const long long c = (long long)i * P.si + (long long)j * P.sj + k;
       const RingPrims<TJ> pr{pm, p0, pp, (row + 1) * T::PRK + (lv + 1)};
-      ls = length_scale_a(P, Q, pr, c, 0);
+      (void)c;
+      ls = length_scale_m(P, pr, 0, sgs_metrics_at<TJ>(mt, q));
       se = sqrtf(pr.ev(0, 0, 0));
     }
     lsT[q] = ls;
@@ -149,7 +192,8 @@ __device__ __forceinline__ void sgs_length_scales(const Phys& P, const Ptrs& Q, 
 template <int TJ>
 __device__ __forceinline__ void sgs_physics_plane(const Phys& P, const Ptrs& Q, int i, int j0, int k0, int tid,
                                                   const float* pm, const float* p0, const float* pp,
-                                                  const float* lsT, const float* seT, float* ph, bool store) {
+                                                  const float* lsT, const float* seT, const float* mt, float* ph,
+                                                  bool store) {
   using T = SgsTile<TJ>;
   const long long n = P.n;
   for (int q = tid; q < T::PHN; q += T::NT) {
@@ -162,8 +206,8 @@ __device__ __forceinline__ void sgs_physics_plane(const Phys& P, const Ptrs& Q, 
       const RingPrims<TJ> pr{pm, p0, pp, (row + 1) * T::PRK + (col + 2)};
       const int l = row * T::LSK + (col + 1);  // this level in the length-scale table; l - 1 below
       const bool tke = P.tke != 0;
-      turb_point(P, Q, pr, c, k, tke ? lsT[l] : 0.0f, tke ? lsT[l - 1] : 0.0f, tke ? seT[l - 1] : 0.0f,
-                 tke ? seT[l] : -1.0f, o);
+      turb_point_m(P, pr, k, tke ? lsT[l] : 0.0f, tke ? lsT[l - 1] : 0.0f, tke ? seT[l - 1] : 0.0f,
+                   tke ? seT[l] : -1.0f, sgs_metrics_at<TJ>(mt, l), o);
       const bool surfCell = P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin;
       if (surfCell) {
         o.tau[2] = Q.tau[2 * n + c];
@@ -217,6 +261,7 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
   float* const phys = prim + 3 * T::NPF * T::PRN;  // [2][NPH][PHN]
   float* const lsT = phys + 2 * T::NPH * T::PHN;   // [PHJ][LSK]
   float* const seT = lsT + T::LSN;
+  float* const mtT = seT + T::LSN;                 // [4][PHJ][LSK] metrics of the physics plane
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SG_K + tx;
   const int k0 = P.kMin + blockIdx.x * SG_K, j0 = P.jMin + blockIdx.y * TJ;
   const int i0 = P.iMin + blockIdx.z * ni;
@@ -253,14 +298,22 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
   }
   __syncthreads();  // plane i0-2 is about to be replaced
   sgs_load_plane<TJ>(P, st, i0 + 1, j0, k0, tid, plane(i0 + 1));
+  {
+    MetricRegs<TJ> m0;
+    sgs_fetch_metrics<TJ>(P, Q, i0, j0, k0, tid, m0);
+    sgs_put_metrics<TJ>(tid, m0, mtT);
+  }
   __syncthreads();
-  sgs_length_scales<TJ>(P, Q, i0, j0, k0, tid, plane(i0 - 1), plane(i0), plane(i0 + 1), lsT, seT);
+  sgs_length_scales<TJ>(P, Q, i0, j0, k0, tid, plane(i0 - 1), plane(i0), plane(i0 + 1), lsT, seT, mtT);
   __syncthreads();
   float* cur = phys;
   float* nxt = phys + T::NPH * T::PHN;
-  PlaneRegs<TJ> ahead;  // the raw state of the plane after next, in flight during the computation
+  PlaneRegs<TJ> ahead;     // the raw state of the plane after next, in flight during the computation
+  MetricRegs<TJ> mahead;   // the metrics of the next physics plane, likewise
   sgs_fetch_plane<TJ>(P, st, i0 + 2, j0, k0, tid, ahead);
-  sgs_physics_plane<TJ>(P, Q, i0, j0, k0, tid, plane(i0 - 1), plane(i0), plane(i0 + 1), lsT, seT, cur, store != 0);
+  sgs_fetch_metrics<TJ>(P, Q, i0 + 1, j0, k0, tid, mahead);
+  sgs_physics_plane<TJ>(P, Q, i0, j0, k0, tid, plane(i0 - 1), plane(i0), plane(i0 + 1), lsT, seT, mtT, cur,
+                        store != 0);
 
   // ---------------------------------------------------------------- march
   for (int i = i0; i < i1; i++) {
@@ -274,11 +327,16 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
     }
     __syncthreads();
     sgs_put_plane<TJ>(tid, ahead, plane(i + 2));
-    if (i + 1 < i1) sgs_fetch_plane<TJ>(P, st, i + 3, j0, k0, tid, ahead);
+    sgs_put_metrics<TJ>(tid, mahead, mtT);
+    if (i + 1 < i1) {
+      sgs_fetch_plane<TJ>(P, st, i + 3, j0, k0, tid, ahead);
+      sgs_fetch_metrics<TJ>(P, Q, i + 2, j0, k0, tid, mahead);
+    }
     __syncthreads();
-    sgs_length_scales<TJ>(P, Q, i + 1, j0, k0, tid, plane(i), plane(i + 1), plane(i + 2), lsT, seT);
+    sgs_length_scales<TJ>(P, Q, i + 1, j0, k0, tid, plane(i), plane(i + 1), plane(i + 2), lsT, seT, mtT);
     __syncthreads();
-    sgs_physics_plane<TJ>(P, Q, i + 1, j0, k0, tid, plane(i), plane(i + 1), plane(i + 2), lsT, seT, nxt, store != 0);
+    sgs_physics_plane<TJ>(P, Q, i + 1, j0, k0, tid, plane(i), plane(i + 1), plane(i + 2), lsT, seT, mtT, nxt,
+                          store != 0);
     __syncthreads();
 
     if (active) {

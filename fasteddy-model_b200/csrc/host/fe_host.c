@@ -1243,6 +1243,19 @@ static int cdf_read_interior(cdf_file *c, const char *name, int nd, float *dst) 
   int i, j, k;
   if (!v) return 1;
   if (v->type != 5 || v->ndims != nd + 1 || !v->isrec || c->numrecs < 1) return -1;
+  /* the dimensions must be (time, zIndex, yIndex, xIndex) or (time, yIndex, xIndex) in this order
+   * (io_netcdf.c:392-717): any other order or any other dimensions would be read transposed */
+  {
+    const char *order[4] = {"time", "zIndex", "yIndex", "xIndex"};
+    int d;
+    for (d = 0; d <= nd; d++) {
+      const char *want = d == 0 ? order[0] : order[nd == 3 ? d : d + 1];
+      if (v->dimids[d] != cdf_dim(c, want)) {
+        snprintf(g_msg, sizeof(g_msg), "variable %s: dimension %d is not %s", name, d, want);
+        return -2;
+      }
+    }
+  }
   raw = (unsigned char *)malloc(cnt * 4);
   if (!raw) return -1;
   if (fseek(c->f, (long)v->begin, SEEK_SET) != 0 || fread(raw, 4, cnt, c->f) != cnt) {
@@ -1308,7 +1321,7 @@ static int restart_topography(const char *path) {
     if (!g_topoGlobal) { rc = -1; goto done; }
     for (i = 0; i < Nx; i++)
       for (j = 0; j < Ny; j++) g_topoGlobal[(size_t)i * Ny + j] = t[(size_t)(i + Nh) * (Ny + 2 * Nh) + (j + Nh)];
-  } else {
+  } else if (rc != -2) {
     snprintf(g_msg, sizeof(g_msg), "inFile %s: cannot read topoPos", path);
   }
 done:
@@ -1343,7 +1356,10 @@ static int restart_state(const char *path) {
   int rc = 0, q, i, j, k;
   if (!c) return -1;
   if (cdf_open_checked(c, path)) { free(c); return -1; }
-#define RD(nm, nd, dst) do { int r_ = cdf_read_interior(c, (nm), (nd), (dst)); if (r_ < 0) { snprintf(g_msg, sizeof(g_msg), "inFile %s: cannot read %s", path, (nm)); rc = -1; } } while (0)
+#define RD(nm, nd, dst) do { int r_ = cdf_read_interior(c, (nm), (nd), (dst)); \
+    if (r_ == -2) { char t_[sizeof(g_msg)]; snprintf(t_, sizeof(t_), "%s", g_msg); \
+      snprintf(g_msg, sizeof(g_msg), "inFile %s: %s", path, t_); rc = -1; } \
+    else if (r_ < 0) { snprintf(g_msg, sizeof(g_msg), "inFile %s: cannot read %s", path, (nm)); rc = -1; } } while (0)
   for (q = 0; q < 5; q++) RD(hydroNames[q], 3, hydroFlds + q * n);
   RD("pressure", 3, hydroPres);
   for (q = 0; q < TKESelector; q++) { char t[16]; snprintf(t, sizeof(t), "TKE_%d", q); RD(t, 3, sgstkeScalars + q * n); }

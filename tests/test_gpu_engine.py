@@ -267,6 +267,14 @@ def test_checkpoint_resume_is_bit_identical(fe, name):
     bad[0:8] = b"XXXXXXXX"
     with pytest.raises(fe.FeError):
         c.restore(bytes(bad))
+    if name == "moist_hill_lsf":
+        # a checkpoint with the subsidence buffer does not load into a domain without subsidence
+        cfg.lsf_horMnSubTerms = 0
+        e = fe.Domain(cfg)
+        e.set_inputs(inp)
+        with pytest.raises(fe.FeError, match="subsidence"):
+            e.restore(blob)
+        e.close()
     a.close()
     c.close()
     host.cleanup()
@@ -451,6 +459,14 @@ def test_ensemble_of_uneven_domains_matches_members(fe):
         solo = fe.Domain(cfg)
         solo.set_inputs(inp)
         solo.advance(11)
+        np.testing.assert_array_equal(interior(d.get_state()["hydroFlds"]), interior(solo.get_state()["hydroFlds"]))
+        solo.close()
+    # without a host synchronisation, a member's own stream (its state copy) waits for the ensemble
+    ens.advance(16, sync=False)
+    for cfg, inp, d in zip(cfgs, inps, members):
+        solo = fe.Domain(cfg)
+        solo.set_inputs(inp)
+        solo.advance(27)
         np.testing.assert_array_equal(interior(d.get_state()["hydroFlds"]), interior(solo.get_state()["hydroFlds"]))
         solo.close()
     ens.close()

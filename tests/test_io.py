@@ -163,3 +163,30 @@ def test_restart_rejects_a_mismatched_file(fe, tmp_path):
     b.load_params_text(small.replace("inPath =\n", f"inPath = {tmp_path}/\n").replace("inFile =\n", "inFile = RUN.8\n"))
     with pytest.raises(fe.FeError, match="parameters ask for"):
         b.init(5)
+
+
+def test_restart_rejects_a_variable_in_another_dimension_order(fe, tmp_path):
+    """A variable whose dimensions are not (time, zIndex, yIndex, xIndex) -- here u written as
+    (time, xIndex, yIndex, zIndex) by scipy's independent writer -- is refused with a message, not
+    read transposed into the state."""
+    from scipy.io import netcdf_file
+
+    a, text = _host(fe, "cbl_dry", {}, tmp_path)
+    a.write_netcdf(str(tmp_path / "GOOD.8"))
+    a.cleanup()
+    with netcdf_file(str(tmp_path / "GOOD.8"), "r", mmap=False) as src, \
+            netcdf_file(str(tmp_path / "BAD.8"), "w", version=2) as dst:
+        for name, size in src.dimensions.items():
+            dst.createDimension(name, size)
+        for name, var in src.variables.items():
+            dims = var.dimensions
+            data = var.data.copy()
+            if name == "u":
+                dims = ("time", "xIndex", "yIndex", "zIndex")
+                data = np.ascontiguousarray(data.transpose(0, 3, 2, 1))
+            out = dst.createVariable(name, var.data.dtype, dims)
+            out[:] = data
+    b = fe.Host()
+    b.load_params_text(text.replace("inPath =\n", f"inPath = {tmp_path}/\n").replace("inFile =\n", "inFile = BAD.8\n"))
+    with pytest.raises(fe.FeError, match="dimension"):
+        b.init(5)

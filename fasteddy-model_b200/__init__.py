@@ -5,7 +5,7 @@ host C layer; libfe_refabi.so: the reference-named drop-in entry points). This p
 only builds and binds them. The directory name has a hyphen, so import it with
 importlib.import_module("fasteddy-model_b200").
 """
-from . import build, cases, runtime  # noqa: F401
+from . import build, cases, halo, runtime  # noqa: F401
 from .runtime import Domain, Ensemble, FeConfig, FeError, Host, Mlp, load, read_binary  # noqa: F401
 
-__all__ = ["build", "cases", "runtime", "Domain", "Ensemble", "FeConfig", "FeError", "Host", "Mlp", "load", "read_binary"]
+__all__ = ["build", "cases", "halo", "runtime", "Domain", "Ensemble", "FeConfig", "FeError", "Host", "Mlp", "load", "read_binary"]

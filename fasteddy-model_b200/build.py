@@ -77,7 +77,7 @@ def build(verbose: bool = False) -> dict[str, str]:
                 errors.append(" ".join(cmd) + "\n" + out)
         if errors:
             raise RuntimeError("build step failed:\n" + "\n".join(errors))
-        cmd = [_nvcc(), *NVCC_ARCH, "-shared", "-o", libs["engine"], *objs, "-lcudart"]
+        cmd = [_nvcc(), *NVCC_ARCH, "-shared", "-o", libs["engine"], *objs, "-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         _run(cmd)

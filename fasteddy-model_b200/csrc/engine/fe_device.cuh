@@ -52,6 +52,11 @@ struct Phys {
   float R_gas, R_vapor, Rv_Rg, cp_gas, cv_gas, g, R_cp, cp_R, cp_cv, p0, kappa, L_v;
   float c1;                  // R/p0^(R/cp), evaluated on the device (as the reference does)
   float presFac;             // powf(p0/pres_grnd, R_cp), evaluated on the device
+  // halo exchange of a decomposed domain: offsets, in floats, from this domain's state arena to
+  // the arena of the domain holding the horizontal neighbour (dx, dy) at [(dx+1)*3 + (dy+1)]
+  // (all 0 for an undecomposed domain), and whether the x / y halos come from neighbours
+  long long nbr[9];
+  int peerX, peerY;
 };
 
 // Device pointers of one domain.

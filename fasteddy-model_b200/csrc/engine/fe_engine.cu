@@ -4,6 +4,8 @@
 // Memory plan of one domain (all fields halo-inclusive, reference layout):
 //   state A, B, C      nf fields each: A = phi^n (and phi^{n+1}), B = phi*, C = phi**
 //   pres pA, pB, pC    perturbation pressure of A, B, C
+//                      (A, B, C, pA, pB, pC are one allocation, the state arena, so that one
+//                      offset per neighbour reaches the same buffer of a neighbouring slab)
 //   grid               zPos, J31, J32, J33, D_Jac, invD_Jac
 //   base               rho_BS, (rho theta)_BS, powf((rho theta)_BS c1, cp/cv)
 //   scratch            9 stresses, 3 TKE fluxes, length scale, 3 per moisture species
@@ -31,6 +33,7 @@
 #include "fe_learn.h"
 #include "fe_sgs.cuh"
 #include "fe_config_phys.cuh"
+#include "fe_comm.h"
 
 using fe::Phys;
 using fe::Ptrs;
@@ -61,6 +64,9 @@ struct fe_domain {
   cudaEvent_t fork = nullptr, join = nullptr;          // ordering between stream and side
   float* st[3] = {nullptr, nullptr, nullptr};
   float* pr[3] = {nullptr, nullptr, nullptr};
+  float* arena = nullptr;                              // the allocation holding st[] and pr[]
+  std::vector<void*> peerMaps;                         // neighbours' arenas opened by IPC handle
+  fe_comm* comm = nullptr;                             // stage barrier of a multi-process decomposition
   float* grid = nullptr;
   float* base = nullptr;
   float* scratch = nullptr;
@@ -93,6 +99,7 @@ struct fe_ensemble {
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graphSteps = 0;
+  bool coupled = false;  // slabs of one decomposed domain: every stage of all waits for the last
 };
 
 extern "C" const char* fe_last_error(void) { return g_err.c_str(); }
@@ -220,10 +227,8 @@ static int dev_alloc(fe_domain* d, float** p, size_t nfloats) {
 static void free_domain(fe_domain* d) {
   if (!d) return;
   if (d->graph) cudaGraphExecDestroy(d->graph);
-  for (int b = 0; b < 3; b++) {
-    cudaFree(d->st[b]);
-    cudaFree(d->pr[b]);
-  }
+  for (void* m : d->peerMaps) cudaIpcCloseMemHandle(m);
+  cudaFree(d->arena);
   cudaFree(d->grid);
   cudaFree(d->base);
   cudaFree(d->scratch);
@@ -295,9 +300,10 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
     cudaError_t ea = sgs_march_attrs();
     if (ea != cudaSuccess) rc = set_err(FE_ERR_CUDA, std::string("SGS kernel attributes: ") + cudaGetErrorString(ea));
   }
+  if (rc == FE_OK) rc = dev_alloc(d, &d->arena, 3 * n * (P.nf + 1));
   for (int b = 0; b < 3 && rc == FE_OK; b++) {
-    rc = dev_alloc(d, &d->st[b], n * P.nf);
-    if (rc == FE_OK) rc = dev_alloc(d, &d->pr[b], n);
+    d->st[b] = d->arena + b * n * P.nf;
+    d->pr[b] = d->arena + 3 * n * P.nf + b * n;
   }
   const size_t nsgs = (size_t)(9 + 3 + 1 + 3 * std::max(P.nmoist, 1));
   const size_t nscr = nsgs + (P.turb ? 7 : 0);  // + the march kernel's SGS tendencies
@@ -743,24 +749,36 @@ static int launch_slab_means(const fe_domain* d, cudaStream_t s, const float* cu
   return 2;
 }
 
-// Enqueue one RK3 step on stream s (no host synchronisation; graph-capturable). With `frhs`,
-// the last stage also stores its tendencies there (the reference's Frhs after a step).
-static void enqueue_step(fe_domain* d, cudaStream_t s, float* frhs = nullptr) {
+// Enqueue RK3 stage `stage` on stream s (no host synchronisation; graph-capturable). With
+// `frhs`, the last stage also stores its tendencies there (the reference's Frhs after a step).
+// A slab of a multi-process decomposition ends each stage on the stage barrier: its commit
+// wrote the neighbours' halos, and their commits wrote its own.
+static void enqueue_stage(fe_domain* d, cudaStream_t s, int stage, float* frhs = nullptr) {
   const Phys& P = d->P;
-  const Ptrs& Q = d->Q;
   float *A = d->st[0], *B = d->st[1], *C = d->st[2];
   const bool physPrep = (P.turb || P.surf > 0);
-  // slab means of the subsidence terms at the start of a forcing step (phi^n in A; C still holds
-  // the previous step's phi** with its boundary images, the reference's halo values at this point)
-  if (P.lsfSub) d->launches += launch_slab_means(d, s, A, C, false);
-  if (physPrep && stage_has_physics(d, 0)) d->launches += launch_physics(d, s, A, 0);
-  launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
-  if (physPrep && stage_has_physics(d, 1)) d->launches += launch_physics(d, s, B, 1);
-  launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
-  if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2, frhs != nullptr);
-  launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], frhs);
-  fe::k_clock<<<1, 1, 0, s>>>(Q, P.dt);
-  d->launches += 4 + (split_last_stage(d) ? 1 : 0);
+  if (stage == 0) {
+    // slab means of the subsidence terms at the start of a forcing step (phi^n in A; C still
+    // holds the previous step's phi** with its boundary images, the reference's halo values)
+    if (P.lsfSub) d->launches += launch_slab_means(d, s, A, C, false);
+    if (physPrep && stage_has_physics(d, 0)) d->launches += launch_physics(d, s, A, 0);
+    launch_stage<0, fe::MODE_COMMIT>(d, s, A, A, B, d->pr[0], d->pr[1], nullptr);
+  } else if (stage == 1) {
+    if (physPrep && stage_has_physics(d, 1)) d->launches += launch_physics(d, s, B, 1);
+    launch_stage<1, fe::MODE_COMMIT>(d, s, B, A, C, d->pr[1], d->pr[2], nullptr);
+  } else {
+    if (physPrep && stage_has_physics(d, 2)) d->launches += launch_physics(d, s, C, 2, frhs != nullptr);
+    launch_stage<2, fe::MODE_COMMIT>(d, s, C, A, A, d->pr[2], d->pr[0], frhs);
+    fe::k_clock<<<1, 1, 0, s>>>(d->Q, P.dt);
+    d->launches += 1 + (split_last_stage(d) ? 1 : 0);
+  }
+  d->launches += 1;
+  if (d->comm) fe_comm_barrier(d->comm, s);
+}
+
+// Enqueue one RK3 step on stream s.
+static void enqueue_step(fe_domain* d, cudaStream_t s, float* frhs = nullptr) {
+  for (int stage = 0; stage < 3; stage++) enqueue_stage(d, s, stage, stage == 2 ? frhs : nullptr);
 }
 
 static const int kGraphSteps = 8;
@@ -1014,6 +1032,19 @@ extern "C" int fe_get_stage_kernel(const fe_domain* d, int* kind, int* tj, int* 
   return FE_OK;
 }
 
+// While alive, the domain's commits write their halo images into its own buffers only: the
+// timing launches below must not write into a neighbouring slab's halos (their own halo cells
+// of C are rewritten by the neighbours' next stage-2 commit before any read).
+struct LocalImages {
+  fe_domain* d;
+  long long nbr[9];
+  explicit LocalImages(fe_domain* dd) : d(dd) {
+    std::memcpy(nbr, d->P.nbr, sizeof(nbr));
+    std::memset(d->P.nbr, 0, sizeof(nbr));
+  }
+  ~LocalImages() { std::memcpy(d->P.nbr, nbr, sizeof(nbr)); }
+};
+
 // Autotuner: times the dynamics stage kernel (writes only the stage-2 buffer C, which
 // every step overwrites) for each candidate form and launch shape and keeps the fastest.
 extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
@@ -1034,7 +1065,9 @@ extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
   float best = 1e30f;
   size_t bi = 0;
   const int reps = 5;
-  const fe_domain saved = *d;
+  LocalImages local(d);
+  const int saved_kind = d->kind, saved_mtj = d->mtj, saved_mni = d->mni, saved_tk = d->tk, saved_tj = d->tj,
+            saved_ti = d->ti;
   for (size_t c = 0; c < cand.size(); c++) {
     d->kind = cand[c].kind;
     if (d->kind == FE_KERNEL_MARCH) { d->mtj = cand[c].a; d->mni = cand[c].b; }
@@ -1053,7 +1086,7 @@ extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CU(cudaGetLastError());
-  d->kind = saved.kind; d->mtj = saved.mtj; d->mni = saved.mni; d->tk = saved.tk; d->tj = saved.tj; d->ti = saved.ti;
+  d->kind = saved_kind; d->mtj = saved_mtj; d->mni = saved_mni; d->tk = saved_tk; d->tj = saved_tj; d->ti = saved_ti;
   const Cand& b = cand[bi];
   d->kind = b.kind;
   if (b.kind == FE_KERNEL_MARCH) { d->mtj = b.a; d->mni = b.b; }
@@ -1243,6 +1276,7 @@ extern "C" int fe_time_stage_kernel(fe_domain* d, int reps, float* ms) {
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
+  LocalImages local(d);
   cudaEventRecord(e0, d->stream);
   for (int r = 0; r < reps; r++)
     launch_stage<1, fe::MODE_COMMIT>(d, d->stream, d->st[1], d->st[0], d->st[2], d->pr[1], d->pr[2], nullptr);
@@ -1288,16 +1322,33 @@ static int ens_build_graph(fe_ensemble* e) {
   CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   for (auto& x : ev) CU(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
   CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-  cudaEventRecord(fork, e->stream);
-  for (size_t i = 0; i < e->m.size(); i++) {
-    fe_domain* d = e->m[i];
-    cudaStreamWaitEvent(d->stream, fork, 0);
-    const long long before = d->launches;
-    for (int s = 0; s < kGraphSteps; s++) enqueue_step(d, d->stream);
-    d->launches = before;
-    cudaEventRecord(ev[i], d->stream);
-    cudaStreamWaitEvent(e->stream, ev[i], 0);
+  std::vector<long long> before;
+  for (auto* d : e->m) before.push_back(d->launches);
+  if (e->coupled) {
+    // slabs of one domain: each stage of every slab, then the next stage (its halos are the
+    // neighbours' commits)
+    for (int s = 0; s < kGraphSteps; s++)
+      for (int stage = 0; stage < 3; stage++) {
+        cudaEventRecord(fork, e->stream);
+        for (size_t i = 0; i < e->m.size(); i++) {
+          fe_domain* d = e->m[i];
+          cudaStreamWaitEvent(d->stream, fork, 0);
+          enqueue_stage(d, d->stream, stage);
+          cudaEventRecord(ev[i], d->stream);
+          cudaStreamWaitEvent(e->stream, ev[i], 0);
+        }
+      }
+  } else {
+    cudaEventRecord(fork, e->stream);
+    for (size_t i = 0; i < e->m.size(); i++) {
+      fe_domain* d = e->m[i];
+      cudaStreamWaitEvent(d->stream, fork, 0);
+      for (int s = 0; s < kGraphSteps; s++) enqueue_step(d, d->stream);
+      cudaEventRecord(ev[i], d->stream);
+      cudaStreamWaitEvent(e->stream, ev[i], 0);
+    }
   }
+  for (size_t i = 0; i < e->m.size(); i++) e->m[i]->launches = before[i];
   cudaError_t err = cudaStreamEndCapture(e->stream, &g);
   cudaEventDestroy(fork);
   for (auto& x : ev) cudaEventDestroy(x);
@@ -1330,15 +1381,21 @@ extern "C" int fe_ensemble_advance(fe_ensemble* e, int nsteps) {
   if (left > 0) {
     cudaEvent_t fork;
     CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-    cudaEventRecord(fork, e->stream);
-    for (auto* d : e->m) {
-      cudaStreamWaitEvent(d->stream, fork, 0);
-      for (int s = 0; s < left; s++) enqueue_step(d, d->stream);
-      cudaEvent_t done;
-      cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
-      cudaEventRecord(done, d->stream);
-      cudaStreamWaitEvent(e->stream, done, 0);
-      cudaEventDestroy(done);
+    // one pass per stage for coupled slabs, one pass over all steps otherwise
+    const int passes = e->coupled ? 3 * left : 1;
+    for (int p = 0; p < passes; p++) {
+      cudaEventRecord(fork, e->stream);
+      for (auto* d : e->m) {
+        cudaStreamWaitEvent(d->stream, fork, 0);
+        if (e->coupled) enqueue_stage(d, d->stream, p % 3);
+        else
+          for (int s = 0; s < left; s++) enqueue_step(d, d->stream);
+        cudaEvent_t done;
+        cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+        cudaEventRecord(done, d->stream);
+        cudaStreamWaitEvent(e->stream, done, 0);
+        cudaEventDestroy(done);
+      }
     }
     cudaEventDestroy(fork);
   }
@@ -1378,3 +1435,114 @@ extern "C" int fe_ensemble_destroy(fe_ensemble* e) {
   delete e;
   return FE_OK;
 }
+
+// ------------------------------------------------------------------ domain decomposition
+// A domain decomposed over px x py slabs (FastEddy's numProcsX x numProcsY ranks, fempi.c:
+// 98-160, with the periodic rank topology of fempi.c:226-245): slab r covers the x range
+// rx*Nxp.. and y range ry*Nyp.. (rx = r % px, ry = r / px) and is created with Nx = Nxp,
+// Ny = Nyp. Each commit writes the slab's own cells and, for its cells within 3 of a slab
+// edge, their images in the neighbouring slabs' halos (the per-stage halo exchange of
+// cuda_hydroCoreDevice.cu:276-314 and fecuda_Utils.cu:205-418, fused into the commit).
+static int check_decomposable(const fe_domain* d, int px, int py) {
+  if (px < 1 || py < 1) return set_err(FE_ERR_ARG, "slab counts must be >= 1");
+  if (d->P.lsfSub) return set_err(FE_ERR_CONFIG, "the large-scale subsidence means span the whole domain; not decomposable");
+  if ((px > 1 && d->P.Nx < 3) || (py > 1 && d->P.Ny < 3))
+    return set_err(FE_ERR_CONFIG, "a decomposed direction needs at least 3 cells per slab (the halo width)");
+  return FE_OK;
+}
+
+static void set_decomposed(fe_domain* d, int px, int py, const long long nbr[9]) {
+  std::memcpy(d->P.nbr, nbr, sizeof(d->P.nbr));
+  d->P.peerX = px > 1;
+  d->P.peerY = py > 1;
+  invalidate_graph(d);
+}
+
+extern "C" int fe_slab_group_create(fe_domain** slabs, int px, int py, fe_ensemble** out) {
+  if (!slabs || !out || px < 1 || py < 1) return set_err(FE_ERR_ARG, "bad argument");
+  const int n = px * py;
+  for (int r = 0; r < n; r++) {
+    if (!slabs[r] || slabs[r]->device != slabs[0]->device) return set_err(FE_ERR_ARG, "slabs must be valid and on one device");
+    const Phys &a = slabs[r]->P, &b = slabs[0]->P;
+    if (a.Nx != b.Nx || a.Ny != b.Ny || a.Nz != b.Nz || a.nf != b.nf)
+      return set_err(FE_ERR_ARG, "slabs must have the same shape and fields");
+    int rc = check_decomposable(slabs[r], px, py);
+    if (rc) return rc;
+  }
+  int rc = fe_ensemble_create(slabs, n, out);
+  if (rc) return rc;
+  (*out)->coupled = true;
+  for (int r = 0; r < n; r++) {
+    const int rx = r % px, ry = r / px;
+    long long nbr[9];
+    for (int dx = -1; dx <= 1; dx++)
+      for (int dy = -1; dy <= 1; dy++) {
+        const int nr = ((ry + dy + py) % py) * px + (rx + dx + px) % px;
+        nbr[(dx + 1) * 3 + (dy + 1)] = (long long)(slabs[nr]->arena - slabs[r]->arena);
+      }
+    set_decomposed(slabs[r], px, py, nbr);
+  }
+  return FE_OK;
+}
+
+extern "C" size_t fe_ipc_handle_bytes(void) { return sizeof(cudaIpcMemHandle_t); }
+
+extern "C" int fe_arena_ipc_handle(fe_domain* d, void* out, size_t bytes) {
+  if (!d || !out || bytes < sizeof(cudaIpcMemHandle_t)) return set_err(FE_ERR_ARG, "bad argument");
+  CU(cudaSetDevice(d->device));
+  cudaIpcMemHandle_t h;
+  CU(cudaIpcGetMemHandle(&h, d->arena));
+  std::memcpy(out, &h, sizeof(h));
+  return FE_OK;
+}
+
+extern "C" int fe_set_halo_peers(fe_domain* d, int px, int py, const void* const* handles) {
+  if (!d || !handles) return set_err(FE_ERR_ARG, "bad argument");
+  int rc = check_decomposable(d, px, py);
+  if (rc) return rc;
+  CU(cudaSetDevice(d->device));
+  long long nbr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<std::pair<std::string, float*>> opened;  // one mapping per distinct peer
+  for (int t = 0; t < 9; t++) {
+    if (!handles[t] || t == 4) continue;
+    const std::string key((const char*)handles[t], sizeof(cudaIpcMemHandle_t));
+    float* base = nullptr;
+    for (auto& o : opened)
+      if (o.first == key) base = o.second;
+    if (!base) {
+      cudaIpcMemHandle_t h;
+      std::memcpy(&h, handles[t], sizeof(h));
+      void* p = nullptr;
+      cudaError_t e = cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(FE_ERR_CUDA, std::string("cudaIpcOpenMemHandle: ") + cudaGetErrorString(e));
+      }
+      d->peerMaps.push_back(p);
+      base = (float*)p;
+      opened.emplace_back(key, base);
+    }
+    nbr[t] = (long long)(base - d->arena);
+  }
+  set_decomposed(d, px, py, nbr);
+  return FE_OK;
+}
+
+extern "C" int fe_clear_halo_peers(fe_domain* d) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  CU(cudaSetDevice(d->device));
+  CU(cudaStreamSynchronize(d->stream));
+  for (void* m : d->peerMaps) cudaIpcCloseMemHandle(m);
+  d->peerMaps.clear();
+  const long long none[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  set_decomposed(d, 1, 1, none);
+  return FE_OK;
+}
+
+extern "C" int fe_set_halo_comm(fe_domain* d, fe_comm* c) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  d->comm = c;
+  invalidate_graph(d);
+  return FE_OK;
+}
+

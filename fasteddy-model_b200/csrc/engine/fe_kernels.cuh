@@ -36,8 +36,14 @@ static __global__ void k_pbs(long long n, const float* __restrict__ thBS, float 
   if (t < n) pBS[t] = powf(thBS[t] * c1, cp_cv);
 }
 
-__device__ __forceinline__ int wrap_i(const Phys& P, int i) { return i < P.iMin ? i + P.Nx : (i >= P.iMax ? i - P.Nx : i); }
-__device__ __forceinline__ int wrap_j(const Phys& P, int j) { return j < P.jMin ? j + P.Ny : (j >= P.jMax ? j - P.Ny : j); }
+// Source column of a halo column: its periodic image, or itself in a direction whose halos the
+// neighbouring slabs provide.
+__device__ __forceinline__ int wrap_i(const Phys& P, int i) {
+  return P.peerX ? i : (i < P.iMin ? i + P.Nx : (i >= P.iMax ? i - P.Nx : i));
+}
+__device__ __forceinline__ int wrap_j(const Phys& P, int j) {
+  return P.peerY ? j : (j < P.jMin ? j + P.Ny : (j >= P.jMax ? j - P.Ny : j));
+}
 
 // Boundary value of field f at halo cell (i,j,k): the vertical boundary rule applied on
 // the periodic source column, i.e. the reference's Commence BCs (cuda_hydroCoreDevice.cu:
@@ -601,23 +607,29 @@ __device__ __forceinline__ void store_column(float* __restrict__ F, long long cb
     for (int h = 1; h <= 3; h++) F[cb + h] = v;
 }
 
+// The image of a cell near the low x edge is a cell of the high x halo of the domain that holds
+// the neighbour at dx = -1 (and so on): P.nbr[(dx+1)*3 + (dy+1)] is the offset, in floats, from
+// this domain's state arena to that domain's. A domain that spans its periodic direction is its
+// own neighbour there (offset 0); a slab of a decomposed domain writes the images straight into
+// its neighbours' halos, on this device or a peer's (the halo exchange of fecuda_Utils.cu:205-418,
+// fused into the commit).
 __device__ __forceinline__ void store_images(const Phys& P, float* __restrict__ F, int i, int j, int k, float v, int nbot,
                                              bool top) {
   const long long c = (long long)i * P.si + (long long)j * P.sj + k;
   const long long dI = (long long)P.Nx * P.si, dJ = (long long)P.Ny * P.sj;
   const bool ilo = i < P.iMin + 3, ihi = i >= P.iMax - 3, jlo = j < P.jMin + 3, jhi = j >= P.jMax - 3;
   store_column(F, c, v, nbot, top);
-  if (jlo) store_column(F, c + dJ, v, nbot, top);
-  if (jhi) store_column(F, c - dJ, v, nbot, top);
+  if (jlo) store_column(F + P.nbr[3], c + dJ, v, nbot, top);
+  if (jhi) store_column(F + P.nbr[5], c - dJ, v, nbot, top);
   if (ilo) {
-    store_column(F, c + dI, v, nbot, top);
-    if (jlo) store_column(F, c + dI + dJ, v, nbot, top);
-    if (jhi) store_column(F, c + dI - dJ, v, nbot, top);
+    store_column(F + P.nbr[1], c + dI, v, nbot, top);
+    if (jlo) store_column(F + P.nbr[0], c + dI + dJ, v, nbot, top);
+    if (jhi) store_column(F + P.nbr[2], c + dI - dJ, v, nbot, top);
   }
   if (ihi) {
-    store_column(F, c - dI, v, nbot, top);
-    if (jlo) store_column(F, c - dI + dJ, v, nbot, top);
-    if (jhi) store_column(F, c - dI - dJ, v, nbot, top);
+    store_column(F + P.nbr[7], c - dI, v, nbot, top);
+    if (jlo) store_column(F + P.nbr[6], c - dI + dJ, v, nbot, top);
+    if (jhi) store_column(F + P.nbr[8], c - dI - dJ, v, nbot, top);
   }
 }
 

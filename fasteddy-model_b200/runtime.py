@@ -158,6 +158,16 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_ensemble_sync", ip, [vp]),
         ("fe_ensemble_stream", vp, [vp]),
         ("fe_ensemble_destroy", ip, [vp]),
+        ("fe_slab_group_create", ip, [ctypes.POINTER(vp), ip, ip, ctypes.POINTER(vp)]),
+        ("fe_ipc_handle_bytes", ctypes.c_size_t, []),
+        ("fe_arena_ipc_handle", ip, [vp, vp, ctypes.c_size_t]),
+        ("fe_set_halo_peers", ip, [vp, ip, ip, ctypes.POINTER(vp)]),
+        ("fe_clear_halo_peers", ip, [vp]),
+        ("fe_comm_unique_id_bytes", ctypes.c_size_t, []),
+        ("fe_comm_unique_id", ip, [vp, ctypes.c_size_t]),
+        ("fe_comm_create", ip, [vp, ip, ip, ip, ctypes.POINTER(vp)]),
+        ("fe_comm_destroy", ip, [vp]),
+        ("fe_set_halo_comm", ip, [vp, vp]),
         ("fe_last_error", ctypes.c_char_p, []),
         ("fe_noalloc_max_cells", ctypes.c_longlong, []),
         ("fe_checkpoint_bytes", ctypes.c_size_t, [vp]),

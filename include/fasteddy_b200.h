@@ -86,6 +86,7 @@ int cuda_timeIntHydroSynchFromDevice(void);
 /* ===================================================================== B. engine */
 typedef struct fe_domain fe_domain;
 typedef struct fe_ensemble fe_ensemble;
+typedef struct fe_comm fe_comm;
 
 /* Physics configuration of one domain. Names and meanings follow the reference's
  * parameter keys (SRC/HYDRO_CORE/hydro_core.c:197-395, SRC/GRID/grid.c:68-88,
@@ -232,6 +233,37 @@ int fe_ensemble_advance(fe_ensemble *e, int nsteps);
 int fe_ensemble_sync(fe_ensemble *e);
 void *fe_ensemble_stream(fe_ensemble *e);
 int fe_ensemble_destroy(fe_ensemble *e);
+
+/* Domain decomposition over px x py slabs, FastEddy's numProcsX x numProcsY ranks
+ * (fempi.c:98-160 rank grid: rx = r % px, ry = r / px; periodic neighbours fempi.c:226-245).
+ * Each slab is a domain created with Nx = Nx_global/px, Ny = Ny_global/py and given the
+ * halo-inclusive slab of the global inputs. Every RK stage's commit writes the slab's cells
+ * and, for cells within 3 of a slab edge, their images in the neighbouring slabs' halos: the
+ * per-stage exchange of cuda_hydroCoreDevice.cu:276-314 (fecuda_SendRecvWestEast/EastWest/
+ * SouthNorth/NorthSouth, fecuda_Utils.cu:205-418) fused into the commit as peer stores.
+ * Set the decomposition before the inputs (the initial boundary fill then keeps the given
+ * slab halos). Not with lsf_horMnSubTerms = 1 (its slab means span the domain).
+ *
+ * All slabs on one device, in this process: slabs[r] for rank r; the group advances with
+ * fe_ensemble_advance (stages of all slabs in lock step) and is released by
+ * fe_ensemble_destroy. */
+int fe_slab_group_create(fe_domain **slabs, int px, int py, fe_ensemble **out);
+/* One slab per process (one GPU each): exchange the slabs' state-arena handles
+ * (fe_arena_ipc_handle, fe_ipc_handle_bytes() bytes) among the ranks, then give each slab
+ * the handles of its 8 neighbours, handles[(dx+1)*3 + (dy+1)] for dx, dy in {-1,0,1}
+ * (NULL where the neighbour is the slab itself), and a stage barrier: a communicator of all
+ * ranks (fe_comm_create from the unique id rank 0 made with fe_comm_unique_id, of
+ * fe_comm_unique_id_bytes() bytes, passed to every rank). All ranks advance the same steps. */
+size_t fe_ipc_handle_bytes(void);
+int fe_arena_ipc_handle(fe_domain *d, void *out, size_t bytes);
+int fe_set_halo_peers(fe_domain *d, int px, int py, const void *const *handles);
+/* Unmap the neighbours' arenas (after every rank's last step); the slab is undecomposed again. */
+int fe_clear_halo_peers(fe_domain *d);
+size_t fe_comm_unique_id_bytes(void);
+int fe_comm_unique_id(void *out, size_t bytes);
+int fe_comm_create(const void *uid, int nranks, int rank, int device, fe_comm **out);
+int fe_comm_destroy(fe_comm *c);
+int fe_set_halo_comm(fe_domain *d, fe_comm *c);
 
 /* Checkpoint / resume: the prognostic state, the 11 surface planes and the clock in one host
  * buffer of fe_checkpoint_bytes() bytes (a header checks the domain shape on load); with

@@ -38,6 +38,8 @@ struct ora_domain {
   /* large-scale forcing: slab means of rho, rho u, rho v, rho theta, rho q_v per level */
   double *lsfProf;
   int lsfN;
+  /* decomposed directions: their halo columns hold the neighbouring slabs' cells */
+  int peerX, peerY;
 };
 
 #define IX(o, i, j, k) (((size_t)(i) * (size_t)(o)->nyh + (size_t)(j)) * (size_t)(o)->nzh + (size_t)(k))
@@ -186,16 +188,28 @@ static void apply_bcs(ora_domain *o, double *f, int kind, int momfld, const doub
         else f[IX(o, i, j, k)] = f[IX(o, i, j, kMax - 1)];
       }
     }
-  for (j = 0; j < Nyh; j++)
-    for (k = 0; k < o->nzh; k++) {
-      for (i = 0; i < iMin; i++) f[IX(o, i, j, k)] = f[IX(o, iMax - 3 + i, j, k)];
-      for (i = iMax; i < iMax + 3; i++) f[IX(o, i, j, k)] = f[IX(o, i - iMax + 3, j, k)];
-    }
-  for (i = 0; i < Nxh; i++)
-    for (k = 0; k < o->nzh; k++) {
-      for (j = 0; j < jMin; j++) f[IX(o, i, j, k)] = f[IX(o, i, jMax - 3 + j, k)];
-      for (j = jMax; j < jMax + 3; j++) f[IX(o, i, j, k)] = f[IX(o, i, j - jMax + 3, k)];
-    }
+  if (!o->peerX)
+    for (j = 0; j < Nyh; j++)
+      for (k = 0; k < o->nzh; k++) {
+        for (i = 0; i < iMin; i++) f[IX(o, i, j, k)] = f[IX(o, iMax - 3 + i, j, k)];
+        for (i = iMax; i < iMax + 3; i++) f[IX(o, i, j, k)] = f[IX(o, i - iMax + 3, j, k)];
+      }
+  if (!o->peerY)
+    for (i = 0; i < Nxh; i++)
+      for (k = 0; k < o->nzh; k++) {
+        for (j = 0; j < jMin; j++) f[IX(o, i, j, k)] = f[IX(o, i, jMax - 3 + j, k)];
+        for (j = jMax; j < jMax + 3; j++) f[IX(o, i, j, k)] = f[IX(o, i, j - jMax + 3, k)];
+      }
+}
+
+/* A slab of a decomposed domain (fempi.c:98-160 rank grid): the caller writes the x (y) halo
+   columns from the neighbouring slabs before every stage (the exchange of
+   cuda_hydroCoreDevice.cu:276-314); the boundary pass then keeps them and applies only the
+   vertical rules on them. */
+int ora_set_decomposition(ora_domain *o, int peerX, int peerY) {
+  o->peerX = peerX != 0;
+  o->peerY = peerY != 0;
+  return FE_OK;
 }
 
 /* ------------------------------------------------------------------ advection */

@@ -26,6 +26,9 @@ int ora_set_state_f64(ora_domain *o, const double *hydroFlds, const double *sgst
 int ora_set_surface(ora_domain *o, const float *z0m, const float *z0t, const float *htFlux, const float *tskin,
                     const float *fricVel, const float *qFlux, const float *qskin);
 int ora_set_clock(ora_domain *o, double simTime, int simTime_it);
+/* Slab of a decomposed domain: x (y) halo columns are written by the caller before each
+ * stage instead of being periodic images. */
+int ora_set_decomposition(ora_domain *o, int peerX, int peerY);
 /* Tendency of RK stage `stage` (0..2) from the current state (updates the stateful
  * surface-layer arrays on the last stage exactly as the device path does). */
 int ora_build_frhs(ora_domain *o, int stage);

@@ -54,6 +54,7 @@ def _load():
         "ora_set_state_f64": (ip, [vp, dp, dp, dp]),
         "ora_set_surface": (ip, [vp, fp, fp, fp, fp, fp, fp, fp]),
         "ora_set_clock": (ip, [vp, ctypes.c_double, ip]),
+        "ora_set_decomposition": (ip, [vp, ip, ip]),
         "ora_build_frhs": (ip, [vp, ip]),
         "ora_rk_stage": (ip, [vp, ip]),
         "ora_step": (ip, [vp, ip]),
@@ -117,6 +118,19 @@ class Oracle:
         L.ora_set_state(self.h, self._p(inp["hydroFlds"]), self._p(inp.get("sgstke")), self._p(inp.get("moist")))
         L.ora_set_clock(self.h, simTime, simTime_it)
         self._keep.clear()
+
+    def set_decomposition(self, peer_x: bool, peer_y: bool) -> None:
+        """Keep the caller-written x / y halo columns (a slab of a decomposed domain)."""
+        self.lib.ora_set_decomposition(self.h, int(peer_x), int(peer_y))
+
+    def set_state_f64(self, hydro, sgstke=None, moist=None) -> None:
+        d = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        H, E, M = d(hydro), d(sgstke) if self.ntke else None, d(moist) if self.nmoist else None
+        p = lambda a: None if a is None else a.ctypes.data_as(c_double_p)
+        self.lib.ora_set_state_f64(self.h, p(H), p(E), p(M))
+
+    def set_clock(self, simTime: float, simTime_it: int) -> None:
+        self.lib.ora_set_clock(self.h, simTime, simTime_it)
 
     def step(self, n: int = 1) -> None:
         self.lib.ora_step(self.h, n)

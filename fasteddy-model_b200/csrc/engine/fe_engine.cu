@@ -625,7 +625,7 @@ static void launch_sgs_march_tj(const fe_domain* d, cudaStream_t s, const float*
   const int ni = d->sgsNi;
   const dim3 g((P.Nz + fe::SG_K - 1) / fe::SG_K, (P.Ny + TJ - 1) / TJ, (P.Nx + ni - 1) / ni);
   fe::k_sgs_march<TKE, NQ, TJ><<<g, dim3(fe::SG_K, TJ), fe::SgsTile<TJ>::SMEM_BYTES, s>>>(P, d->Q, st, stage, ni,
-                                                                                         store ? 1 : 0);
+                                                                                         store ? 1 : 0, d->mlp ? 1 : 0);
 }
 template <bool TKE, int NQ>
 static void launch_sgs_march_nq(const fe_domain* d, cudaStream_t s, const float* st, int stage, bool store) {
@@ -669,7 +669,7 @@ static cudaError_t sgs_march_attrs() {
 // Whether the last-stage physics runs as the fused kernel: the march stage kernel, SGS closure
 // on, no learned closure (whose stresses replace the closure's between the two kernels).
 static bool fused_sgs(const fe_domain* d) {
-  return d->sgsRows > 0 && d->kind == FE_KERNEL_MARCH && d->P.turb && !d->mlp;
+  return d->sgsRows > 0 && d->kind == FE_KERNEL_MARCH && d->P.turb;
 }
 
 // Everything a physics stage needs before its stage kernel, on state st: the SGS kernel and
@@ -680,14 +680,16 @@ static bool fused_sgs(const fe_domain* d) {
 static int launch_physics(const fe_domain* d, cudaStream_t s, const float* st, int stage, bool store = false) {
   const Phys& P = d->P;
   if (fused_sgs(d)) {
-    // the surface layer first: the fused kernel reads its first-level stresses
+    // the surface layer first: the fused kernel reads its first-level stresses; with the learned
+    // closure, the network's stresses of the ring (inputs from the state) before the fused kernel
     if (P.surf > 0) fe::k_surface<<<dim3((P.Ny + 1 + 127) / 128, P.Nx + 1), 128, 0, s>>>(P, d->Q, st, stage);
+    if (d->mlp) fe_learn_enqueue_tau(d->mlp, P, d->Q, st, s, true);
     launch_sgs_march(d, s, st, stage, store);
-    return P.surf > 0 ? 2 : 1;
+    return (P.surf > 0 ? 2 : 1) + (d->mlp ? 1 : 0);
   }
   int l = launch_turb(d, s, st, stage);
   if (d->mlp && P.turb) {
-    fe_learn_enqueue_tau(d->mlp, P, d->Q, st, s);
+    fe_learn_enqueue_tau(d->mlp, P, d->Q, st, s, false);
     l++;
   }
   if (d->kind == FE_KERNEL_MARCH && P.turb) {
@@ -806,7 +808,7 @@ static int launches_per_step(const fe_domain* d) {
   const Phys& P = d->P;
   int l = 4 + (split_last_stage(d) ? 1 : 0) + (P.lsfSub ? 2 : 0);
   if (P.turb || P.surf > 0) {
-    const int phys = fused_sgs(d) ? 1 + (P.surf > 0)
+    const int phys = fused_sgs(d) ? 1 + (P.surf > 0) + (d->mlp ? 1 : 0)
                                   : 2 + (P.surf > 0) + ((d->mlp && P.turb) ? 1 : 0) +
                                         ((d->kind == FE_KERNEL_MARCH && P.turb) ? 1 : 0);
     l += (P.oneRK ? 1 : 3) * phys;
@@ -1215,7 +1217,7 @@ extern "C" int fe_sgs_sample(fe_domain* d, long long every, float* X, float* tau
   float* A = d->st[0];
   d->launches += launch_turb(d, d->stream, A, 2);
   if (d->mlp) {
-    CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream));
+    CU(fe_learn_enqueue_tau(d->mlp, P, d->Q, A, d->stream, false));
     d->launches++;
   }
   float *dX = nullptr, *dT = nullptr, *dR = nullptr;

@@ -93,10 +93,11 @@ int launch_grad(fe_mlp* m, long long first, long long count) {
 int* fe_learn_err_flag(const fe_mlp* m) { return m ? m->err : nullptr; }
 int fe_learn_device(const fe_mlp* m) { return m ? m->device : -1; }
 
-cudaError_t fe_learn_enqueue_tau(const fe_mlp* m, const fe::Phys& P, const fe::Ptrs& Q, const float* st, cudaStream_t s) {
+cudaError_t fe_learn_enqueue_tau(const fe_mlp* m, const fe::Phys& P, const fe::Ptrs& Q, const float* st, cudaStream_t s,
+                                 bool fromState) {
   const long long cells = (long long)(P.Nx + 2) * (P.Ny + 2) * (P.Nz + 1);
   const long long tiles = (cells + fe::MLP_M - 1) / fe::MLP_M;
-  if (Q.feat)
+  if (Q.feat && !fromState)
     fe::k_mlp_infer<2><<<grid_for(m, tiles, 5), 128, fe::MlpInferSmem::BYTES, s>>>(P, Q, st, m->params, m->norm, nullptr,
                                                                                       nullptr, 0, m->err);
   else

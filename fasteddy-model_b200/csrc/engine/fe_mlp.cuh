@@ -205,11 +205,15 @@ __device__ __forceinline__ float tanh_hw(float x) {
 }
 // tanh of two hidden units for inference: the pre-activations rounded to BF16 (the precision of
 // the activation tile they end up in) and the hardware tanh.approx.bf16x2, two values per
-// special-function instruction; the result is the packed BF16 pair of the tile
+// special-function instruction; the result is the packed BF16 pair of the tile. The rounding
+// is integer arithmetic (add half a BF16 ulp to the FP32 bits, keep the high halves: round to
+// nearest, ties away from zero in magnitude) so that the special-function pipe, which the tanh
+// saturates, does not also carry a conversion per pair.
 __device__ __forceinline__ uint32_t tanh2_bf16(float a, float b) {
-  const __nv_bfloat162 p = __floats2bfloat162_rn(a, b);
+  const uint32_t ua = __float_as_uint(a) + 0x8000u, ub = __float_as_uint(b) + 0x8000u;
+  const uint32_t p = __byte_perm(ua, ub, 0x7632);  // a's high half low, b's high half high
   uint32_t r;
-  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(r) : "r"(*reinterpret_cast<const uint32_t*>(&p)));
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(r) : "r"(p));
   return r;
 }
 
@@ -218,11 +222,15 @@ __device__ __forceinline__ uint32_t tanh2_bf16(float a, float b) {
 template <bool PAIRED>
 __device__ __forceinline__ void epi_tanh(uint32_t tacc, const float* bias, char* out, int r) {
 #pragma unroll
-  for (int g = 0; g < 4; g++) {
-    float v[16];
-    tmem_ld16(tacc + g * 16, v);
+  for (int g = 0; g < 4; g += 2) {
+    float v2[32];
+    tmem_ld16(tacc + g * 16, v2);
+    tmem_ld16(tacc + g * 16 + 16, v2 + 16);
     tmem_wait_ld();
-    const float* b = bias + g * 16;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const float* v = v2 + 16 * h;
+    const float* b = bias + (g + h) * 16;
     if (PAIRED) {
       uint4 lo, hi;
       lo.x = tanh2_bf16(v[0] + b[0], v[1] + b[1]);
@@ -233,14 +241,16 @@ __device__ __forceinline__ void epi_tanh(uint32_t tacc, const float* bias, char*
       hi.y = tanh2_bf16(v[10] + b[10], v[11] + b[11]);
       hi.z = tanh2_bf16(v[12] + b[12], v[13] + b[13]);
       hi.w = tanh2_bf16(v[14] + b[14], v[15] + b[15]);
-      st_chunk_u(out, r, 2 * g, 64, lo);
-      st_chunk_u(out, r, 2 * g + 1, 64, hi);
+      st_chunk_u(out, r, 2 * (g + h), 64, lo);
+      st_chunk_u(out, r, 2 * (g + h) + 1, 64, hi);
     } else {
+      float t[16];
 #pragma unroll
-      for (int q = 0; q < 16; q++) v[q] = tanh_hw(v[q] + b[q]);
-      st_chunk(out, r, 2 * g, 64, v);
-      st_chunk(out, r, 2 * g + 1, 64, v + 8);
+      for (int q = 0; q < 16; q++) t[q] = tanh_hw(v[q] + b[q]);
+      st_chunk(out, r, 2 * (g + h), 64, t);
+      st_chunk(out, r, 2 * (g + h) + 1, 64, t + 8);
     }
+  }
   }
 }
 

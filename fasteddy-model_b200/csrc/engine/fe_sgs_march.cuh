@@ -19,8 +19,10 @@
 //
 // and writes only the 7 SGS tendency fields the last stage's march kernel reads (and, when asked,
 // the stresses and fluxes themselves, for callers that copy them back). The first-level stresses
-// of the surface columns come from the surface-layer kernel, launched before this one. Results
-// equal the two-kernel form (k_turb_t + k_turb_ring + k_sgs_tend) bit for bit.
+// of the surface columns come from the surface-layer kernel, launched before this one. With the
+// learned closure, the 9 stresses of every ring point come from the network's output (written by
+// the inference kernel, launched before this one), the other closure outputs from the closure.
+// Results equal the two-kernel form (k_turb_t + k_turb_ring [+ inference] + k_sgs_tend) bit for bit.
 #pragma once
 #include "fe_kernels.cuh"
 
@@ -188,12 +190,14 @@ __device__ __forceinline__ void sgs_length_scales(const Phys& P, const Ptrs& Q, 
 
 // The closure's outputs of plane i for rows j0-1..j0+TJ, levels k0-1..k0+32 into `ph` [NPH][PHN]
 // (zero outside the ring and below kMin); the first-level stresses of the surface columns from
-// the surface-layer kernel's output. With `store`, the per-point kernels' scratch fields too.
+// the surface-layer kernel's output; with `learned`, all 9 stresses from Q.tau (the network's,
+// the surface columns' first-level ones left there by the surface layer). With `store`, the
+// per-point kernels' scratch fields too.
 template <int TJ>
 __device__ __forceinline__ void sgs_physics_plane(const Phys& P, const Ptrs& Q, int i, int j0, int k0, int tid,
                                                   const float* pm, const float* p0, const float* pp,
                                                   const float* lsT, const float* seT, const float* mt, float* ph,
-                                                  bool store) {
+                                                  bool store, bool learned) {
   using T = SgsTile<TJ>;
   const long long n = P.n;
   for (int q = tid; q < T::PHN; q += T::NT) {
@@ -209,17 +213,20 @@ __device__ __forceinline__ void sgs_physics_plane(const Phys& P, const Ptrs& Q, 
       turb_point_m(P, pr, k, tke ? lsT[l] : 0.0f, tke ? lsT[l - 1] : 0.0f, tke ? seT[l - 1] : 0.0f,
                    tke ? seT[l] : -1.0f, sgs_metrics_at<TJ>(mt, l), o);
       const bool surfCell = P.surf > 0 && k == P.kMin && i >= P.iMin && j >= P.jMin;
-      if (surfCell) {
+      if (learned) {
+#pragma unroll
+        for (int t = 0; t < 9; t++) o.tau[t] = Q.tau[t * n + c];
+      } else if (surfCell) {
         o.tau[2] = Q.tau[2 * n + c];
         o.tau[3] = Q.tau[3 * n + c];
         o.tau[8] = Q.tau[8 * n + c];
-        if (P.moist && P.moistSGS > 0) o.mtau[2] = Q.mtau[2 * n + c];
       }
+      if (surfCell && P.moist && P.moistSGS > 0) o.mtau[2] = Q.mtau[2 * n + c];
       if (store) {
         float* Tt = Q.tau;
 #pragma unroll
         for (int t = 0; t < 9; t++)
-          if (!(surfCell && (t == 2 || t == 3 || t == 8))) Tt[t * n + c] = o.tau[t];
+          if (!learned && !(surfCell && (t == 2 || t == 3 || t == 8))) Tt[t * n + c] = o.tau[t];
         if (P.tke) {
           Q.ls[c] = o.ls;
 #pragma unroll
@@ -254,7 +261,7 @@ __device__ __forceinline__ void sgs_physics_plane(const Phys& P, const Ptrs& Q, 
 // arithmetic, term by term), on the large-scale forcing steps with the forcing folded in.
 template <bool TKE, int NQ, int TJ>
 __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
-    k_sgs_march(Phys P, Ptrs Q, const float* __restrict__ st, int stage, int ni, int store) {
+    k_sgs_march(Phys P, Ptrs Q, const float* __restrict__ st, int stage, int ni, int store, int learned) {
   using T = SgsTile<TJ>;
   extern __shared__ __align__(16) float sm[];
   float* const prim = sm;                          // [3][NPF][PRN]
@@ -313,7 +320,7 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
   sgs_fetch_plane<TJ>(P, st, i0 + 2, j0, k0, tid, ahead);
   sgs_fetch_metrics<TJ>(P, Q, i0 + 1, j0, k0, tid, mahead);
   sgs_physics_plane<TJ>(P, Q, i0, j0, k0, tid, plane(i0 - 1), plane(i0), plane(i0 + 1), lsT, seT, mtT, cur,
-                        store != 0);
+                        store != 0, learned != 0);
 
   // ---------------------------------------------------------------- march
   for (int i = i0; i < i1; i++) {
@@ -336,7 +343,7 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
     sgs_length_scales<TJ>(P, Q, i + 1, j0, k0, tid, plane(i), plane(i + 1), plane(i + 2), lsT, seT, mtT);
     __syncthreads();
     sgs_physics_plane<TJ>(P, Q, i + 1, j0, k0, tid, plane(i), plane(i + 1), plane(i + 2), lsT, seT, mtT, nxt,
-                          store != 0);
+                          store != 0, learned != 0);
     __syncthreads();
 
     if (active) {

@@ -13,7 +13,8 @@ Two modes:
   exact=False  FP64 arithmetic, but every tensor-core operand rounded to BF16 (round to
                nearest even) exactly where the device rounds it: the standardised inputs, the
                weights, the hidden activations (for predictions also the pre-activations,
-               the argument of the inference kernel's BF16 tanh), and the backward signals dZ. This is the
+               the argument of the inference kernel's BF16 tanh, with ties rounded away from
+               zero as that kernel does), and the backward signals dZ. This is the
                reference the device gradients and predictions are checked against.
 """
 from __future__ import annotations
@@ -36,6 +37,15 @@ def bf16(x: np.ndarray) -> np.ndarray:
     x32 = np.ascontiguousarray(x, dtype=np.float32)
     u = x32.view(np.uint32).astype(np.uint64)
     u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def bf16_ta(x: np.ndarray) -> np.ndarray:
+    """Round float32 values to bfloat16 (nearest, ties away from zero in magnitude: the inference
+    kernel's integer rounding of the tanh argument); returned as float64."""
+    x32 = np.ascontiguousarray(x, dtype=np.float32)
+    u = x32.view(np.uint32).astype(np.uint64)
+    u = (u + 0x8000) & 0xFFFF0000
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
@@ -66,7 +76,7 @@ def forward(p: np.ndarray, X: np.ndarray, norm: dict, exact: bool = False, infer
     does not (FP32 tanh)."""
     w = unpack(p)
     r = (lambda a: a) if exact else bf16
-    ra = r if inference else (lambda a: a)
+    ra = (lambda a: a) if (exact or not inference) else bf16_ta
     x0 = r(standardise(X, norm))
     h1 = r(np.tanh(ra(x0 @ r(w["W1"]).T + w["b1"])))
     h2 = r(np.tanh(ra(h1 @ r(w["W2"]).T + w["b2"])))

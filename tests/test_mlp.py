@@ -49,6 +49,12 @@ def test_bf16_rounding_matches_torch():
     x = np.concatenate([x, ties])
     ref = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy().astype(np.float64)
     np.testing.assert_array_equal(mo.bf16(x), ref)
+    # the inference kernel's rounding of the tanh argument: the same away from ties, ties away from zero
+    ta = mo.bf16_ta(x)
+    tie = np.zeros(x.shape, bool)
+    tie[-1000:] = True
+    np.testing.assert_array_equal(ta[~tie], ref[~tie])
+    assert np.all(np.abs(ta[tie]) > np.abs(x[tie]))
 
 
 def test_oracle_gradient_matches_finite_differences():
@@ -187,6 +193,47 @@ def test_learned_stresses_feed_the_time_step(fe):
     d.advance(16)
     assert d.nonfinite() == 0
     d.close()
+    m.close()
+    host.cleanup()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["cbl_dry", "cbl_moist_hill"])
+def test_learned_closure_in_the_fused_sgs_kernel_equals_the_chain(fe, case):
+    """With a network set, the fused last-stage SGS kernel (inference from the state first, the
+    network's stresses read by the fused kernel) and the kernel chain (closure kernel writing
+    the inputs, inference, tendency kernel) give the same tendencies, stresses and states bit for
+    bit (ragged tiles)."""
+    kw = dict(hill_halfwidth=90.0, hill_height=20.0, qv=(24.0, 8.0, 300.0)) if case == "cbl_moist_hill" else {}
+    host = fe.cases.setup_host(case, 37, 13, 45, **kw)
+    inp, cfg = host.inputs(), host.config()
+    d0 = fe.Domain(cfg)
+    d0.set_inputs(inp)
+    d0.advance(2)
+    samp = d0.sgs_sample()
+    d0.close()
+    m = fe.Mlp(seed=5)
+    m.set_data(samp["X"], samp["tau"] / samp["rho"][:, None])
+    m.train(50, 2048, 3e-3)
+    a, b = fe.Domain(cfg), fe.Domain(cfg)
+    for dom in (a, b):
+        dom.set_inputs(inp)
+        dom.set_sgs_mlp(m)
+    b.set_sgs_kernel(0)
+    fa, fb = a.build_frhs(2), b.build_frhs(2)
+    for key in ("hydroFrhs", "sgstkeFrhs", "moistFrhs", "taus"):
+        if fa.get(key) is not None:
+            np.testing.assert_array_equal(fa[key][..., 3:-3, 3:-3, 3:-3], fb[key][..., 3:-3, 3:-3, 3:-3], err_msg=key)
+    a.advance(10)
+    b.advance(10)
+    sa, sb = a.get_state(), b.get_state()
+    for key in ("hydroFlds", "sgstke", "moist"):
+        if sa.get(key) is not None:
+            np.testing.assert_array_equal(sa[key], sb[key], err_msg=key)
+    assert a.nonfinite() == 0
+    for dom in (a, b):
+        dom.set_sgs_mlp(None)
+        dom.close()
     m.close()
     host.cleanup()
 

@@ -408,8 +408,9 @@ def run_ours(args, rank: int, world: int, local: int) -> dict | None:
 
 # ---------------------------------------------------------------- batched ensemble
 def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
-    """64 uneven neutral-ABL members advanced together: every step of every member is one node
-    of one captured CUDA graph (members on parallel branches), launched once per 8 steps."""
+    """64 uneven neutral-ABL members advanced together in one captured CUDA graph per 8 steps:
+    each step is one work-list launch per kernel over the tiles of all members (the members'
+    parameters in device tables), or, with --ensemble-branches, one graph branch per member."""
     import numpy as np
     import torch
 
@@ -432,12 +433,13 @@ def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
     t_tune = time.perf_counter() - t_tune
     cells = sum(nx * ny * nz for nx, ny, nz, _, _ in specs)
     ens = fe.Ensemble(doms)
+    ens.set_batched(not args.ensemble_branches)
     ens.advance(graph_warmup(args.warmup))
     stream = torch.cuda.ExternalStream(ens.stream(), device=device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     steps = 8 * max(1, math.ceil(args.steps / 8))
-    launches0 = sum(d.launch_count() for d in doms)
+    launches0 = ens.launch_count()
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
@@ -448,7 +450,9 @@ def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
     torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
-    launches = sum(d.launch_count() for d in doms) - launches0
+    launches = ens.launch_count() - launches0
+    form = "work list: one launch per kernel of a step over the tiles of all members" if ens.batched() else \
+        "one CUDA-graph branch per member"
     max_ms = max_over_ranks(ms, device)
     value = whole_job_rate(cells, steps, max_ms / 1e3, world)
     # stage kernels of every member, timed alone: algorithmic bytes over summed launch times
@@ -495,7 +499,7 @@ def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
                                "U_g 5..15 m/s, z0 0.01..0.5 m (seeded), dx=dy=20 m, dz=10 m",
                    "members": len(specs), "cells": cells, "parallelism": f"replicas{world}",
                    "l2": f"state of all members {4 * 6 * cells / 1e9:.1f} GB >> 126 MB L2, no flush needed",
-                   "autotuned_shapes": kinds, "autotune_s": round(t_tune, 1)},
+                   "autotuned_shapes": kinds, "autotune_s": round(t_tune, 1), "launch_form": form},
         "e2e": {"value": whole_job_rate(cells, steps, e2e_s, world), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
                 "path": "engine API: fe_set_state of every member, one ensemble advance, fe_get_state "
@@ -510,6 +514,31 @@ def run_ensemble(args, rank: int, world: int, local: int) -> dict | None:
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_case(fe, "abl_neutral", 80)
     return line
+
+
+# ---------------------------------------------------------------- the other configurations
+def other_configs(args, local: int) -> dict:
+    """The batched ensemble and the 1024x1024x256 domain (plain and learned closure), measured in
+    the same one-GPU process after the headline case, each with its own device-timed rate and its
+    end-to-end rate; their full lines come from --case ensemble64 / --case dry_hill_1024."""
+    out = {}
+    sub = argparse.Namespace(**vars(args))
+    sub.no_cpu_baseline = True
+    sub.case, sub.steps, sub.warmup = ENSEMBLE_CASE, 16, max(3, args.warmup)
+    e = run_ensemble(sub, 0, 1, local)
+    out[ENSEMBLE_CASE] = {"workload": e["config"]["workload"], "value": e["value"], "ms_per_step": e["ms_per_step"],
+                          "steps": e["steps"], "e2e": e["e2e"]["value"], "gpu_launches": e["gpu_launches"],
+                          "nonfinite_cells": e["nonfinite_cells"]}
+    sub.case, sub.steps, sub.warmup, sub.no_learned = "dry_hill_1024", 5, 3, False
+    r = run_ours(sub, 0, 1, local)
+    big = {"workload": r["config"]["workload"], "value": r["value"], "ms_per_step": r["ms_per_step"],
+           "steps": r["steps"], "e2e": r["e2e"]["value"], "roofline_frac": r["roofline"]["frac"],
+           "nonfinite_cells": r["nonfinite_cells"]}
+    if "learned_sgs" in r:
+        big["learned_ms_per_step"] = r["learned_sgs"]["ms_per_step"]
+        big["learned_value"] = r["learned_sgs"]["value"]
+    out["dry_hill_1024"] = big
+    return out
 
 
 # ---------------------------------------------------------------- reference arm
@@ -572,6 +601,11 @@ def main(argv=None) -> int:
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-SGS form")
+    ap.add_argument("--ensemble-branches", action="store_true",
+                    help="ensemble: one CUDA-graph branch per member instead of the work-list launches")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="headline case only (by default a one-GPU run of it also measures the ensemble and "
+                         "the 1024x1024x256 domain)")
     args = ap.parse_args(argv)
     rank, world, local = dist_env()
     if world > 1:
@@ -592,6 +626,8 @@ def main(argv=None) -> int:
             line = run_ensemble(args, rank, world, local)
         else:
             line = run_ours(args, rank, world, local)
+            if line is not None and world == 1 and args.case == DEFAULT_CASE and not args.no_extra:
+                line["other_configs"] = other_configs(args, local)
     finally:
         if world > 1:
             import torch.distributed as dist

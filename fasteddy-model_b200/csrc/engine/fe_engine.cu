@@ -34,6 +34,7 @@
 #include "fe_sgs.cuh"
 #include "fe_config_phys.cuh"
 #include "fe_comm.h"
+#include "fe_batch.h"
 
 using fe::Phys;
 using fe::Ptrs;
@@ -100,6 +101,16 @@ struct fe_ensemble {
   cudaGraphExec_t graph = nullptr;
   int graphSteps = 0;
   bool coupled = false;  // slabs of one decomposed domain: every stage of all waits for the last
+  // work-list form: one launch per kernel of a step over the tiles of every member
+  bool wantBatched = true;
+  bool batched = false;               // the graph and the eager steps use the work-list launches
+  void* batchMem = nullptr;           // the member tables on the device
+  fe::MarchMember* bMarch[3] = {nullptr, nullptr, nullptr};
+  fe::SgsMember* bSgs[3] = {nullptr, nullptr, nullptr};
+  fe::SurfMember* bSurf[3] = {nullptr, nullptr, nullptr};
+  fe::ClockMember* bClock = nullptr;
+  int bMarchBlocks = 0, bSgsBlocks = 0, bSurfBlocks = 0;
+  long long launches = 0;             // the work-list launches (the members count their own otherwise)
 };
 
 extern "C" const char* fe_last_error(void) { return g_err.c_str(); }
@@ -298,6 +309,7 @@ extern "C" int fe_create(const fe_config* cfg, int device, fe_domain** out) {
   rc = march_attrs();
   if (rc == FE_OK) {
     cudaError_t ea = sgs_march_attrs();
+    if (ea == cudaSuccess) ea = fe::batch_set_attrs();
     if (ea != cudaSuccess) rc = set_err(FE_ERR_CUDA, std::string("SGS kernel attributes: ") + cudaGetErrorString(ea));
   }
   if (rc == FE_OK) rc = dev_alloc(d, &d->arena, 3 * n * (P.nf + 1));
@@ -1314,7 +1326,130 @@ extern "C" int fe_ensemble_create(fe_domain** members, int n, fe_ensemble** out)
   return FE_OK;
 }
 
-// One graph holds kGraphSteps steps of every member, members as independent branches.
+// ------------------------------------------------------------------ work-list (batched) form
+// Members that all run the dry flavour with the fused SGS kernel (prognostic TKE, no moisture,
+// no subsidence means, no network, undecomposed) advance with one launch per kernel of a step:
+// each launch walks the tiles of every member (fe_batch.h). Each member keeps the march shape the
+// autotuner chose for it when that is the 8-row march tile, else its default shape; the results
+// equal the per-member launches bit for bit (march shapes and SGS tile rows do not change bits).
+static bool batchable(const fe_ensemble* e) {
+  if (!e->wantBatched || e->coupled || e->m.empty()) return false;
+  const Phys& P0 = e->m[0]->P;
+  for (const fe_domain* d : e->m) {
+    const Phys& P = d->P;
+    if (fe::march_flavor(P) != fe::FL_DRY || !P.turb || P.lsfSub || P.moist || d->mlp || d->comm || d->sgsRows == 0)
+      return false;
+    if (P.surf != P0.surf || P.oneRK != P0.oneRK) return false;
+    for (int t = 0; t < 9; t++)
+      if (P.nbr[t]) return false;
+  }
+  return true;
+}
+
+static int ens_build_batch(fe_ensemble* e) {
+  const int nm = (int)e->m.size();
+  std::vector<fe::MarchMember> mm[3];
+  std::vector<fe::SgsMember> sg[3];
+  std::vector<fe::SurfMember> sf[3];
+  std::vector<fe::ClockMember> ck;
+  int mB = 0, sB = 0, fB = 0;
+  for (fe_domain* d : e->m) {
+    const Phys& P = d->P;
+    const int ni = d->mtj == 8 ? d->mni : d->mniDefault;
+    const int mgx = (P.Nz + fe::MK - 1) / fe::MK, mgy = (P.Ny + 7) / 8, mgz = (P.Nx + ni - 1) / ni;
+    const int sni = d->sgsNi;
+    const int sgx = (P.Nz + fe::SG_K - 1) / fe::SG_K, sgy = (P.Ny + 7) / 8, sgz = (P.Nx + sni - 1) / sni;
+    const int gj = (P.Ny + 1 + 127) / 128;
+    float *A = d->st[0], *B = d->st[1], *C = d->st[2];
+    const float* stIn[3] = {A, B, C};
+    const float* base[3] = {A, A, A};
+    float* out[3] = {B, C, A};
+    const float* pin[3] = {d->pr[0], d->pr[1], d->pr[2]};
+    float* pout[3] = {d->pr[1], d->pr[2], d->pr[0]};
+    for (int st = 0; st < 3; st++) {
+      fe::MarchMember x;
+      std::memset(&x, 0, sizeof(x));
+      x.P = P;
+      x.Q = d->Q;
+      x.cur = stIn[st]; x.base = base[st]; x.nxt = out[st]; x.pcur = pin[st]; x.pnxt = pout[st];
+      x.ni = ni; x.gx = mgx; x.gy = mgy; x.first = mB;
+      mm[st].push_back(x);
+      fe::SgsMember y;
+      std::memset(&y, 0, sizeof(y));
+      y.P = P; y.Q = d->Q; y.st = stIn[st]; y.ni = sni; y.gx = sgx; y.gy = sgy; y.first = sB;
+      sg[st].push_back(y);
+      fe::SurfMember z;
+      std::memset(&z, 0, sizeof(z));
+      z.P = P; z.Q = d->Q; z.st = stIn[st]; z.gj = gj; z.first = fB;
+      sf[st].push_back(z);
+    }
+    ck.push_back({d->Q.clockIt, d->Q.clockTime, P.dt});
+    mB += mgx * mgy * mgz;
+    sB += sgx * sgy * sgz;
+    fB += gj * (P.Nx + 1);
+  }
+  const size_t szM = sizeof(fe::MarchMember) * nm, szS = sizeof(fe::SgsMember) * nm;
+  const size_t szF = sizeof(fe::SurfMember) * nm, szC = sizeof(fe::ClockMember) * nm;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t total = 3 * (up(szM) + up(szS) + up(szF)) + up(szC);
+  if (e->batchMem) cudaFree(e->batchMem);
+  e->batchMem = nullptr;
+  if (cudaMalloc(&e->batchMem, total) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(FE_ERR_NOMEM, "ensemble table allocation failed");
+  }
+  char* p = (char*)e->batchMem;
+  for (int st = 0; st < 3; st++) {
+    e->bMarch[st] = (fe::MarchMember*)p;
+    CU(cudaMemcpyAsync(p, mm[st].data(), szM, cudaMemcpyHostToDevice, e->stream));
+    p += up(szM);
+    e->bSgs[st] = (fe::SgsMember*)p;
+    CU(cudaMemcpyAsync(p, sg[st].data(), szS, cudaMemcpyHostToDevice, e->stream));
+    p += up(szS);
+    e->bSurf[st] = (fe::SurfMember*)p;
+    CU(cudaMemcpyAsync(p, sf[st].data(), szF, cudaMemcpyHostToDevice, e->stream));
+    p += up(szF);
+  }
+  e->bClock = (fe::ClockMember*)p;
+  CU(cudaMemcpyAsync(p, ck.data(), szC, cudaMemcpyHostToDevice, e->stream));
+  CU(cudaStreamSynchronize(e->stream));
+  e->bMarchBlocks = mB;
+  e->bSgsBlocks = sB;
+  e->bSurfBlocks = fB;
+  return FE_OK;
+}
+
+// Work-list launches of one step (the count ens_enqueue_batched_step enqueues).
+static int ens_batched_launches(const fe_ensemble* e) {
+  const fe_domain* d0 = e->m[0];
+  int l = 1;  // clocks
+  for (int stage = 0; stage < 3; stage++) l += 1 + (stage_has_physics(d0, stage) ? 1 + (d0->P.surf > 0 ? 1 : 0) : 0);
+  return l;
+}
+
+// One RK3 step of every member in work-list launches on stream s; returns the launches enqueued.
+static int ens_enqueue_batched_step(fe_ensemble* e, cudaStream_t s) {
+  const fe_domain* d0 = e->m[0];
+  const int nm = (int)e->m.size();
+  int l = 0;
+  for (int stage = 0; stage < 3; stage++) {
+    if (stage_has_physics(d0, stage)) {
+      if (d0->P.surf > 0) {
+        fe::batch_surface(e->bSurf[stage], nm, e->bSurfBlocks, stage, s);
+        l++;
+      }
+      fe::batch_sgs(e->bSgs[stage], nm, e->bSgsBlocks, stage, s);
+      l++;
+    }
+    fe::batch_march(fe::FL_DRY, stage, e->bMarch[stage], nm, e->bMarchBlocks, s);
+    l++;
+  }
+  fe::batch_clock(e->bClock, nm, s);
+  return l + 1;
+}
+
+// One graph holds kGraphSteps steps of every member, members as independent branches (or, in the
+// work-list form, kGraphSteps steps of work-list launches).
 static int ens_build_graph(fe_ensemble* e) {
   if (e->graph) cudaGraphExecDestroy(e->graph);
   e->graph = nullptr;
@@ -1326,7 +1461,9 @@ static int ens_build_graph(fe_ensemble* e) {
   CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   std::vector<long long> before;
   for (auto* d : e->m) before.push_back(d->launches);
-  if (e->coupled) {
+  if (e->batched) {
+    for (int s = 0; s < kGraphSteps; s++) ens_enqueue_batched_step(e, e->stream);
+  } else if (e->coupled) {
     // slabs of one domain: each stage of every slab, then the next stage (its halos are the
     // neighbours' commits)
     for (int s = 0; s < kGraphSteps; s++)
@@ -1371,15 +1508,37 @@ extern "C" int fe_ensemble_advance(fe_ensemble* e, int nsteps) {
     if (!d->haveState) return set_err(FE_ERR_STATE, "member state not set");
   CU(cudaSetDevice(e->m[0]->device));
   int left = nsteps;
+  if (!e->graph) {
+    // the form (and, for the work-list form, the member tables) is fixed when the graph is made
+    e->batched = batchable(e);
+    if (e->batched && !e->batchMem) {
+      int rc = ens_build_batch(e);
+      if (rc) return rc;
+    }
+  }
+  // earlier work on the members' own streams (their inputs, ...) comes first
+  {
+    cudaEvent_t prior;
+    CU(cudaEventCreateWithFlags(&prior, cudaEventDisableTiming));
+    for (auto* d : e->m) {
+      cudaEventRecord(prior, d->stream);
+      cudaStreamWaitEvent(e->stream, prior, 0);
+    }
+    cudaEventDestroy(prior);
+  }
   if (left >= kGraphSteps && !e->graph) {
     int rc = ens_build_graph(e);
     if (rc) return rc;
   }
   while (left >= kGraphSteps) {
     CU(cudaGraphLaunch(e->graph, e->stream));
-    for (auto* d : e->m) d->launches += (long long)kGraphSteps * launches_per_step(d);
+    if (e->batched) e->launches += (long long)kGraphSteps * ens_batched_launches(e);
+    else
+      for (auto* d : e->m) d->launches += (long long)kGraphSteps * launches_per_step(d);
     left -= kGraphSteps;
   }
+  if (e->batched)
+    for (; left > 0; left--) e->launches += ens_enqueue_batched_step(e, e->stream);
   if (left > 0) {
     cudaEvent_t fork;
     CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -1429,10 +1588,35 @@ extern "C" int fe_ensemble_sync(fe_ensemble* e) {
 
 extern "C" void* fe_ensemble_stream(fe_ensemble* e) { return e ? (void*)e->stream : nullptr; }
 
+extern "C" int fe_ensemble_set_batched(fe_ensemble* e, int on) {
+  if (!e) return set_err(FE_ERR_ARG, "NULL handle");
+  e->wantBatched = on != 0;
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  e->graph = nullptr;
+  e->graphSteps = 0;
+  if (e->batchMem) {
+    cudaStreamSynchronize(e->stream);
+    cudaFree(e->batchMem);
+  }
+  e->batchMem = nullptr;
+  e->batched = false;
+  return FE_OK;
+}
+
+extern "C" int fe_ensemble_is_batched(const fe_ensemble* e) { return e && e->batched ? 1 : 0; }
+
+extern "C" long long fe_ensemble_launch_count(const fe_ensemble* e) {
+  if (!e) return 0;
+  long long l = e->launches;
+  for (const fe_domain* d : e->m) l += d->launches;
+  return l;
+}
+
 extern "C" int fe_ensemble_destroy(fe_ensemble* e) {
   if (!e) return FE_OK;
   cudaStreamSynchronize(e->stream);
   if (e->graph) cudaGraphExecDestroy(e->graph);
+  cudaFree(e->batchMem);
   cudaStreamDestroy(e->stream);
   delete e;
   return FE_OK;

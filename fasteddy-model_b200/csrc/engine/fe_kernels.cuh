@@ -962,6 +962,56 @@ static __global__ void k_clock(Ptrs Q, float dt) {
   *Q.clockTime = *Q.clockTime + dt;
 }
 
+// One member of a batched surface-layer launch: blocks first .. first + gj*(Nx+1) - 1, gj blocks
+// of 128 columns along j per i.
+struct SurfMember {
+  Phys P;
+  Ptrs Q;
+  const float* st;
+  int gj, first;
+};
+
+// k_surface of several domains in one launch.
+static __global__ void __launch_bounds__(128) k_surface_list(const SurfMember* __restrict__ mem, int nmem, int stage) {
+  __shared__ SurfMember sm_m;
+  __shared__ int sm_idx;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nmem - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (mem[mid].first <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    sm_idx = lo;
+  }
+  __syncthreads();
+  {
+    const int* src = reinterpret_cast<const int*>(mem + sm_idx);
+    int* dst = reinterpret_cast<int*>(&sm_m);
+    for (int q = threadIdx.x; q < (int)(sizeof(SurfMember) / sizeof(int)); q += blockDim.x) dst[q] = src[q];
+  }
+  __syncthreads();
+  const SurfMember& m = sm_m;
+  const int local = (int)blockIdx.x - m.first;
+  const int j = m.P.jMin + (local % m.gj) * 128 + threadIdx.x;
+  const int i = m.P.iMin + local / m.gj;
+  if (j > m.P.jMax || i > m.P.iMax) return;
+  surface_column(m.P, m.Q, m.st, i, j, stage);
+}
+
+// The device clocks of several domains (one thread each).
+struct ClockMember {
+  int* it;
+  float* time;
+  float dt;
+};
+static __global__ void k_clock_list(const ClockMember* __restrict__ mem, int nmem) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nmem) return;
+  *mem[t].it = *mem[t].it + 1;
+  *mem[t].time = *mem[t].time + mem[t].dt;
+}
+
 static __global__ void k_nonfinite(Phys P, const float* __restrict__ st, unsigned long long* out) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned int cnt = 0;

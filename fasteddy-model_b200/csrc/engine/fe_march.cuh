@@ -247,10 +247,12 @@ __global__ void __launch_bounds__(256, 4) k_sgs_tend(Phys P, Ptrs Q, const float
 // MP: the saturation adjustment of the last stage. -1 decides per step from the device clock;
 // 0 and 1 are the two halves of a pair launched back to back, each returning at once unless the
 // step is its kind (0: no adjustment this step, compiled without the adjustment; 1: adjustment).
-template <int STAGE, int MODE, int TJ, int FL, int MP = -1>
-__global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
-    k_march(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base, float* __restrict__ nxt,
-            const float* __restrict__ pcur, float* __restrict__ pnxt, float* __restrict__ frhs, int ni) {
+// The body of one thread block: tile (bx, by, bz) of the domain P / Q (k tile, j tile, i chunk).
+template <int STAGE, int MODE, int TJ, int FL, int MP>
+__device__ __forceinline__ void march_body(const Phys& P, const Ptrs& Q, const float* __restrict__ cur,
+                                           const float* __restrict__ base, float* __restrict__ nxt,
+                                           const float* __restrict__ pcur, float* __restrict__ pnxt,
+                                           float* __restrict__ frhs, int ni, int bx, int by, int bz) {
   const int ntke = FL == FL_ANY ? P.ntke : 1;
   const int nmoist = FL == FL_ANY ? P.nmoist : ((FL == FL_MOIST || FL == FL_MOIST34) ? 2 : 0);
   const bool pgf = FL == FL_ANY ? (P.pgf != 0) : true;
@@ -267,8 +269,8 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
   extern __shared__ __align__(16) float sm[];
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * MK + tx;
-  const int k0 = P.kMin + blockIdx.x * MK, j0 = P.jMin + blockIdx.y * TJ;
-  const int i0 = P.iMin + blockIdx.z * ni;
+  const int k0 = P.kMin + bx * MK, j0 = P.jMin + by * TJ;
+  const int i0 = P.iMin + bz * ni;
   const int i1 = min(i0 + ni, P.iMax);
   const int k = k0 + tx, j = j0 + ty;
   const bool inArr = (k < P.nzh) && (j < P.nyh);     // the thread's column exists in memory
@@ -838,6 +840,54 @@ __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
     cp_async_wait_all();
     __syncthreads();
   }
+}
+
+template <int STAGE, int MODE, int TJ, int FL, int MP = -1>
+__global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
+    k_march(Phys P, Ptrs Q, const float* __restrict__ cur, const float* __restrict__ base, float* __restrict__ nxt,
+            const float* __restrict__ pcur, float* __restrict__ pnxt, float* __restrict__ frhs, int ni) {
+  march_body<STAGE, MODE, TJ, FL, MP>(P, Q, cur, base, nxt, pcur, pnxt, frhs, ni, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// One member of a batched launch: its domain, the buffers of the stage, its planes per block and
+// its share of the launch's thread blocks (blocks first .. first + gx*gy*gz - 1).
+struct MarchMember {
+  Phys P;
+  Ptrs Q;
+  const float *cur, *base, *pcur;
+  float *nxt, *pnxt;
+  int ni, gx, gy, first;
+};
+
+// The stage kernel of several domains in one launch (a work list of tiles across uneven members):
+// block b finds its member by the members' first blocks, copies that member's parameters into
+// shared memory and runs the member's tile.
+template <int STAGE, int TJ, int FL, int MP = -1>
+__global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
+    k_march_list(const MarchMember* __restrict__ mem, int nmem) {
+  __shared__ MarchMember sm_m;
+  __shared__ int sm_idx;
+  const int tid = threadIdx.y * MK + threadIdx.x;
+  if (tid == 0) {
+    int lo = 0, hi = nmem - 1;  // last member whose first block <= blockIdx.x
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (mem[mid].first <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    sm_idx = lo;
+  }
+  __syncthreads();
+  {
+    const int* src = reinterpret_cast<const int*>(mem + sm_idx);
+    int* dst = reinterpret_cast<int*>(&sm_m);
+    for (int q = tid; q < (int)(sizeof(MarchMember) / sizeof(int)); q += MK * TJ) dst[q] = src[q];
+  }
+  __syncthreads();
+  const MarchMember& m = sm_m;
+  const int local = (int)blockIdx.x - m.first;
+  const int bx = local % m.gx, by = (local / m.gx) % m.gy, bz = local / (m.gx * m.gy);
+  march_body<STAGE, MODE_COMMIT, TJ, FL, MP>(m.P, m.Q, m.cur, m.base, m.nxt, m.pcur, m.pnxt, nullptr, m.ni, bx, by, bz);
 }
 
 }  // namespace fe

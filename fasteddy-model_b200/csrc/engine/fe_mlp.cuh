@@ -355,14 +355,14 @@ __global__ void __launch_bounds__(128) k_mlp_infer(Phys P, Ptrs Q, const float* 
     const int i = cur.i, j = cur.j, k = cur.k;
     put_inputs(sm + S::X0, tid, cur.x, nm, isig, valid);
     sync_for_mma();
-    fetch(tile + gridDim.x, nxt);  // in flight while this tile's layers run
     bool ok = true;
-    // layer 1
+    // layer 1, then the next tile's inputs (loads and, from the state, their arithmetic) while it runs
     if (tid == 0) {
       tc_fence_after();
       umma_bf16(tbase + TC_DF, umma_sdesc(sm + S::X0, 128, 256), umma_sdesc(sm + S::W1, 128, 256), id64, 0);
       umma_commit(bar);
     }
+    fetch(tile + gridDim.x, nxt);
     ok = ok && mbar_wait(bar, phase);
     phase ^= 1;
     tc_fence_after();

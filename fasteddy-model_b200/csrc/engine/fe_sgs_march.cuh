@@ -259,9 +259,10 @@ __device__ __forceinline__ void sgs_physics_plane(const Phys& P, const Ptrs& Q, 
 
 // SGS tendencies of the last stage into the seven fields of Q.sgsF (fe_march.cuh k_sgs_tend's
 // arithmetic, term by term), on the large-scale forcing steps with the forcing folded in.
+// The body of one thread block: tile (bx, by, bz) of the domain P / Q.
 template <bool TKE, int NQ, int TJ>
-__global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
-    k_sgs_march(Phys P, Ptrs Q, const float* __restrict__ st, int stage, int ni, int store, int learned) {
+__device__ __forceinline__ void sgs_march_body(const Phys& P, const Ptrs& Q, const float* __restrict__ st, int stage,
+                                               int ni, int store, int learned, int bx, int by, int bz) {
   using T = SgsTile<TJ>;
   extern __shared__ __align__(16) float sm[];
   float* const prim = sm;                          // [3][NPF][PRN]
@@ -270,8 +271,8 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
   float* const seT = lsT + T::LSN;
   float* const mtT = seT + T::LSN;                 // [4][PHJ][LSK] metrics of the physics plane
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SG_K + tx;
-  const int k0 = P.kMin + blockIdx.x * SG_K, j0 = P.jMin + blockIdx.y * TJ;
-  const int i0 = P.iMin + blockIdx.z * ni;
+  const int k0 = P.kMin + bx * SG_K, j0 = P.jMin + by * TJ;
+  const int i0 = P.iMin + bz * ni;
   const int i1 = min(i0 + ni, P.iMax);
   const int j = j0 + ty, k = k0 + tx;
   const bool active = j < P.jMax && k < P.kMax;
@@ -424,6 +425,50 @@ __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
     cur = nxt;
     nxt = t;
   }
+}
+
+template <bool TKE, int NQ, int TJ>
+__global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
+    k_sgs_march(Phys P, Ptrs Q, const float* __restrict__ st, int stage, int ni, int store, int learned) {
+  sgs_march_body<TKE, NQ, TJ>(P, Q, st, stage, ni, store, learned, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// One member of a batched launch of the fused SGS kernel (see MarchMember).
+struct SgsMember {
+  Phys P;
+  Ptrs Q;
+  const float* st;
+  int ni, gx, gy, first;
+};
+
+// The fused SGS kernel of several domains in one launch: block b runs a tile of the member whose
+// block range holds b, with that member's parameters copied into shared memory.
+template <bool TKE, int NQ, int TJ>
+__global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
+    k_sgs_march_list(const SgsMember* __restrict__ mem, int nmem, int stage) {
+  __shared__ SgsMember sm_m;
+  __shared__ int sm_idx;
+  const int tid = threadIdx.y * SG_K + threadIdx.x;
+  if (tid == 0) {
+    int lo = 0, hi = nmem - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (mem[mid].first <= (int)blockIdx.x) lo = mid;
+      else hi = mid - 1;
+    }
+    sm_idx = lo;
+  }
+  __syncthreads();
+  {
+    const int* src = reinterpret_cast<const int*>(mem + sm_idx);
+    int* dst = reinterpret_cast<int*>(&sm_m);
+    for (int q = tid; q < (int)(sizeof(SgsMember) / sizeof(int)); q += SG_K * TJ) dst[q] = src[q];
+  }
+  __syncthreads();
+  const SgsMember& m = sm_m;
+  const int local = (int)blockIdx.x - m.first;
+  sgs_march_body<TKE, NQ, TJ>(m.P, m.Q, m.st, stage, m.ni, 0, 0, local % m.gx, (local / m.gx) % m.gy,
+                              local / (m.gx * m.gy));
 }
 
 }  // namespace fe

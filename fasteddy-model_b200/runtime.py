@@ -158,6 +158,9 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_ensemble_sync", ip, [vp]),
         ("fe_ensemble_stream", vp, [vp]),
         ("fe_ensemble_destroy", ip, [vp]),
+        ("fe_ensemble_set_batched", ip, [vp, ip]),
+        ("fe_ensemble_is_batched", ip, [vp]),
+        ("fe_ensemble_launch_count", ctypes.c_longlong, [vp]),
         ("fe_slab_group_create", ip, [ctypes.POINTER(vp), ip, ip, ctypes.POINTER(vp)]),
         ("fe_ipc_handle_bytes", ctypes.c_size_t, []),
         ("fe_arena_ipc_handle", ip, [vp, vp, ctypes.c_size_t]),
@@ -573,6 +576,17 @@ class Ensemble:
 
     def stream(self) -> int:
         return int(self.e.fe_ensemble_stream(self.h) or 0)
+
+    def set_batched(self, on: bool) -> None:
+        """Work-list launches over all members (when they allow it) or one graph branch per member."""
+        _check(self.e.fe_ensemble_set_batched(self.h, int(on)), "fe_ensemble_set_batched")
+
+    def batched(self) -> bool:
+        """Whether the advances so far used the work-list launches."""
+        return bool(self.e.fe_ensemble_is_batched(self.h))
+
+    def launch_count(self) -> int:
+        return int(self.e.fe_ensemble_launch_count(self.h))
 
     def close(self) -> None:
         if self.h:

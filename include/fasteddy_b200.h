@@ -227,12 +227,21 @@ int fe_time_stage_kernel(fe_domain *d, int reps, float *ms);
 long long fe_launch_count(const fe_domain *d);
 
 /* Ensembles: advance several domains (different sizes allowed, same device) with one
- * captured CUDA graph per step batch. */
+ * captured CUDA graph per step batch. When every member runs the dry flavour with the fused
+ * SGS kernel (prognostic TKE, HYB56, no moisture, no subsidence means, no network, not
+ * decomposed), a step is one launch per kernel over the tiles of all members (a work list of
+ * (member, tile) items with the members' parameters in device tables), else one graph branch per
+ * member; both give the members' own results bit for bit. The members' settings and tile shapes
+ * are read when the ensemble first advances. fe_ensemble_set_batched(e, 0) keeps the branches. */
 int fe_ensemble_create(fe_domain **members, int n, fe_ensemble **out);
 int fe_ensemble_advance(fe_ensemble *e, int nsteps);
 int fe_ensemble_sync(fe_ensemble *e);
 void *fe_ensemble_stream(fe_ensemble *e);
 int fe_ensemble_destroy(fe_ensemble *e);
+int fe_ensemble_set_batched(fe_ensemble *e, int on);
+int fe_ensemble_is_batched(const fe_ensemble *e);
+/* Kernel launches enqueued for the ensemble and its members since creation. */
+long long fe_ensemble_launch_count(const fe_ensemble *e);
 
 /* Domain decomposition over px x py slabs, FastEddy's numProcsX x numProcsY ranks
  * (fempi.c:98-160 rank grid: rx = r % px, ry = r / px; periodic neighbours fempi.c:226-245).

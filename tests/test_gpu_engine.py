@@ -440,8 +440,11 @@ def test_fp64_domain_means(fe):
     host.cleanup()
 
 
-def test_ensemble_of_uneven_domains_matches_members(fe):
-    shapes = [(16, 12, 10), (20, 16, 12), (12, 20, 14)]
+@pytest.mark.parametrize("batched", [True, False])
+def test_ensemble_of_uneven_domains_matches_members(fe, batched):
+    """Uneven neutral-ABL members advanced together -- as work-list launches over all members'
+    tiles, or as one graph branch per member -- equal the members advanced alone, bit for bit."""
+    shapes = [(16, 12, 10), (20, 16, 12), (12, 20, 14), (37, 13, 45)]
     hosts, inps, cfgs = [], [], []
     for i, (nx, ny, nz) in enumerate(shapes):
         h = fe.cases.setup_host("abl_neutral", nx, ny, nz, seed=100 + i, ug=5.0 + 2 * i)
@@ -453,8 +456,11 @@ def test_ensemble_of_uneven_domains_matches_members(fe):
         d = fe.Domain(cfg)
         d.set_inputs(inp)
         members.append(d)
+    members[1].set_stage_kernel("march", 8, 5)  # a member with its own march shape (same bits)
     ens = fe.Ensemble(members)
+    ens.set_batched(batched)
     ens.advance(11)  # one 8-step graph + 3 eager steps
+    assert ens.batched() == batched
     for cfg, inp, d in zip(cfgs, inps, members):
         solo = fe.Domain(cfg)
         solo.set_inputs(inp)

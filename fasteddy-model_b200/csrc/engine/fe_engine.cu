@@ -109,6 +109,7 @@ struct fe_ensemble {
   fe::SgsMember* bSgs[3] = {nullptr, nullptr, nullptr};
   fe::SurfMember* bSurf[3] = {nullptr, nullptr, nullptr};
   fe::ClockMember* bClock = nullptr;
+  int *bMapMarch = nullptr, *bMapSgs = nullptr, *bMapSurf = nullptr;  // member of each thread block
   int bMarchBlocks = 0, bSgsBlocks = 0, bSurfBlocks = 0;
   long long launches = 0;             // the work-list launches (the members count their own otherwise)
 };
@@ -1329,9 +1330,11 @@ extern "C" int fe_ensemble_create(fe_domain** members, int n, fe_ensemble** out)
 // ------------------------------------------------------------------ work-list (batched) form
 // Members that all run the dry flavour with the fused SGS kernel (prognostic TKE, no moisture,
 // no subsidence means, no network, undecomposed) advance with one launch per kernel of a step:
-// each launch walks the tiles of every member (fe_batch.h). Each member keeps the march shape the
-// autotuner chose for it when that is the 8-row march tile, else its default shape; the results
+// each launch walks the tiles of every member (fe_batch.h). Every block marches kListPlanes planes
+// (the launch holds all members' blocks, so long blocks keep the GPU full while their start-up --
+// the member lookup, the parameter copy and the first planes -- is paid less often); the results
 // equal the per-member launches bit for bit (march shapes and SGS tile rows do not change bits).
+static const int kListPlanes = 64;
 static bool batchable(const fe_ensemble* e) {
   if (!e->wantBatched || e->coupled || e->m.empty()) return false;
   const Phys& P0 = e->m[0]->P;
@@ -1352,12 +1355,13 @@ static int ens_build_batch(fe_ensemble* e) {
   std::vector<fe::SgsMember> sg[3];
   std::vector<fe::SurfMember> sf[3];
   std::vector<fe::ClockMember> ck;
+  std::vector<int> mapM, mapS, mapF;
   int mB = 0, sB = 0, fB = 0;
   for (fe_domain* d : e->m) {
     const Phys& P = d->P;
-    const int ni = d->mtj == 8 ? d->mni : d->mniDefault;
+    const int ni = kListPlanes;
     const int mgx = (P.Nz + fe::MK - 1) / fe::MK, mgy = (P.Ny + 7) / 8, mgz = (P.Nx + ni - 1) / ni;
-    const int sni = d->sgsNi;
+    const int sni = kListPlanes;
     const int sgx = (P.Nz + fe::SG_K - 1) / fe::SG_K, sgy = (P.Ny + 7) / 8, sgz = (P.Nx + sni - 1) / sni;
     const int gj = (P.Ny + 1 + 127) / 128;
     float *A = d->st[0], *B = d->st[1], *C = d->st[2];
@@ -1384,14 +1388,18 @@ static int ens_build_batch(fe_ensemble* e) {
       sf[st].push_back(z);
     }
     ck.push_back({d->Q.clockIt, d->Q.clockTime, P.dt});
+    const int mi = (int)ck.size() - 1;
     mB += mgx * mgy * mgz;
     sB += sgx * sgy * sgz;
     fB += gj * (P.Nx + 1);
+    mapM.resize(mB, mi);
+    mapS.resize(sB, mi);
+    mapF.resize(fB, mi);
   }
   const size_t szM = sizeof(fe::MarchMember) * nm, szS = sizeof(fe::SgsMember) * nm;
   const size_t szF = sizeof(fe::SurfMember) * nm, szC = sizeof(fe::ClockMember) * nm;
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-  const size_t total = 3 * (up(szM) + up(szS) + up(szF)) + up(szC);
+  const size_t total = 3 * (up(szM) + up(szS) + up(szF)) + up(szC) + up(4 * mB) + up(4 * sB) + up(4 * fB);
   if (e->batchMem) cudaFree(e->batchMem);
   e->batchMem = nullptr;
   if (cudaMalloc(&e->batchMem, total) != cudaSuccess) {
@@ -1412,6 +1420,15 @@ static int ens_build_batch(fe_ensemble* e) {
   }
   e->bClock = (fe::ClockMember*)p;
   CU(cudaMemcpyAsync(p, ck.data(), szC, cudaMemcpyHostToDevice, e->stream));
+  p += up(szC);
+  e->bMapMarch = (int*)p;
+  CU(cudaMemcpyAsync(p, mapM.data(), 4 * (size_t)mB, cudaMemcpyHostToDevice, e->stream));
+  p += up(4 * mB);
+  e->bMapSgs = (int*)p;
+  CU(cudaMemcpyAsync(p, mapS.data(), 4 * (size_t)sB, cudaMemcpyHostToDevice, e->stream));
+  p += up(4 * sB);
+  e->bMapSurf = (int*)p;
+  CU(cudaMemcpyAsync(p, mapF.data(), 4 * (size_t)fB, cudaMemcpyHostToDevice, e->stream));
   CU(cudaStreamSynchronize(e->stream));
   e->bMarchBlocks = mB;
   e->bSgsBlocks = sB;
@@ -1435,13 +1452,13 @@ static int ens_enqueue_batched_step(fe_ensemble* e, cudaStream_t s) {
   for (int stage = 0; stage < 3; stage++) {
     if (stage_has_physics(d0, stage)) {
       if (d0->P.surf > 0) {
-        fe::batch_surface(e->bSurf[stage], nm, e->bSurfBlocks, stage, s);
+        fe::batch_surface(e->bSurf[stage], e->bMapSurf, e->bSurfBlocks, stage, s);
         l++;
       }
-      fe::batch_sgs(e->bSgs[stage], nm, e->bSgsBlocks, stage, s);
+      fe::batch_sgs(e->bSgs[stage], e->bMapSgs, e->bSgsBlocks, stage, s);
       l++;
     }
-    fe::batch_march(fe::FL_DRY, stage, e->bMarch[stage], nm, e->bMarchBlocks, s);
+    fe::batch_march(fe::FL_DRY, stage, e->bMarch[stage], e->bMapMarch, e->bMarchBlocks, s);
     l++;
   }
   fe::batch_clock(e->bClock, nm, s);

@@ -972,18 +972,11 @@ struct SurfMember {
 };
 
 // k_surface of several domains in one launch.
-static __global__ void __launch_bounds__(128) k_surface_list(const SurfMember* __restrict__ mem, int nmem, int stage) {
+static __global__ void __launch_bounds__(128) k_surface_list(const SurfMember* __restrict__ mem, const int* __restrict__ bmap,
+                                                             int stage) {
   __shared__ SurfMember sm_m;
   __shared__ int sm_idx;
-  if (threadIdx.x == 0) {
-    int lo = 0, hi = nmem - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (mem[mid].first <= (int)blockIdx.x) lo = mid;
-      else hi = mid - 1;
-    }
-    sm_idx = lo;
-  }
+  if (threadIdx.x == 0) sm_idx = bmap[blockIdx.x];
   __syncthreads();
   {
     const int* src = reinterpret_cast<const int*>(mem + sm_idx);

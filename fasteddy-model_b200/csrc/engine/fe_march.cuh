@@ -860,23 +860,15 @@ struct MarchMember {
 };
 
 // The stage kernel of several domains in one launch (a work list of tiles across uneven members):
-// block b finds its member by the members' first blocks, copies that member's parameters into
-// shared memory and runs the member's tile.
+// block b reads its member from the block map, copies that member's parameters into shared memory
+// and runs the member's tile.
 template <int STAGE, int TJ, int FL, int MP = -1>
 __global__ void __launch_bounds__(MK * TJ, 512 / (MK * TJ))
-    k_march_list(const MarchMember* __restrict__ mem, int nmem) {
+    k_march_list(const MarchMember* __restrict__ mem, const int* __restrict__ bmap) {
   __shared__ MarchMember sm_m;
   __shared__ int sm_idx;
   const int tid = threadIdx.y * MK + threadIdx.x;
-  if (tid == 0) {
-    int lo = 0, hi = nmem - 1;  // last member whose first block <= blockIdx.x
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (mem[mid].first <= (int)blockIdx.x) lo = mid;
-      else hi = mid - 1;
-    }
-    sm_idx = lo;
-  }
+  if (tid == 0) sm_idx = bmap[blockIdx.x];
   __syncthreads();
   {
     const int* src = reinterpret_cast<const int*>(mem + sm_idx);

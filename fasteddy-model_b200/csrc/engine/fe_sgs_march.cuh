@@ -441,23 +441,15 @@ struct SgsMember {
   int ni, gx, gy, first;
 };
 
-// The fused SGS kernel of several domains in one launch: block b runs a tile of the member whose
-// block range holds b, with that member's parameters copied into shared memory.
+// The fused SGS kernel of several domains in one launch: block b runs a tile of the member the
+// block map names, with that member's parameters copied into shared memory.
 template <bool TKE, int NQ, int TJ>
 __global__ void __launch_bounds__(SG_K * TJ, TJ <= 8 ? 2 : 1)
-    k_sgs_march_list(const SgsMember* __restrict__ mem, int nmem, int stage) {
+    k_sgs_march_list(const SgsMember* __restrict__ mem, const int* __restrict__ bmap, int stage) {
   __shared__ SgsMember sm_m;
   __shared__ int sm_idx;
   const int tid = threadIdx.y * SG_K + threadIdx.x;
-  if (tid == 0) {
-    int lo = 0, hi = nmem - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (mem[mid].first <= (int)blockIdx.x) lo = mid;
-      else hi = mid - 1;
-    }
-    sm_idx = lo;
-  }
+  if (tid == 0) sm_idx = bmap[blockIdx.x];
   __syncthreads();
   {
     const int* src = reinterpret_cast<const int*>(mem + sm_idx);

@@ -1039,6 +1039,22 @@ extern "C" int fe_set_sgs_kernel(fe_domain* d, int rows) {
   return FE_OK;
 }
 
+extern "C" int fe_set_sgs_shape(fe_domain* d, int rows, int ni) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (ni < 1) return set_err(FE_ERR_ARG, "fused SGS kernel: planes per block must be >= 1");
+  int rc = fe_set_sgs_kernel(d, rows);
+  if (rc) return rc;
+  d->sgsNi = ni;
+  return FE_OK;
+}
+
+extern "C" int fe_get_sgs_shape(const fe_domain* d, int* rows, int* ni) {
+  if (!d) return set_err(FE_ERR_ARG, "NULL handle");
+  if (rows) *rows = d->sgsRows;
+  if (ni) *ni = d->sgsNi;
+  return FE_OK;
+}
+
 extern "C" int fe_get_stage_kernel(const fe_domain* d, int* kind, int* tj, int* ni) {
   if (!d) return set_err(FE_ERR_ARG, "NULL handle");
   if (kind) *kind = d->kind;
@@ -1106,6 +1122,35 @@ extern "C" int fe_autotune(fe_domain* d, int* tk, int* tj, int* ti) {
   d->kind = b.kind;
   if (b.kind == FE_KERNEL_MARCH) { d->mtj = b.a; d->mni = b.b; }
   else { d->tk = b.a; d->tj = b.b; d->ti = b.c; }
+  // the fused SGS kernel's tile rows and planes per block (it writes only its 7 tendency fields,
+  // which the next physics stage rewrites)
+  if (fused_sgs(d)) {
+    const int saveRows = d->sgsRows, saveNi = d->sgsNi;
+    float sbest = 1e30f;
+    int brow = saveRows, bni = saveNi;
+    cudaEvent_t s0, s1;
+    CU(cudaEventCreate(&s0));
+    CU(cudaEventCreate(&s1));
+    for (int rows : {8, 16})
+      for (int ni : {8, 16, 32, 64}) {
+        if (ni > std::max(8, d->P.Nx)) continue;
+        d->sgsRows = rows;
+        d->sgsNi = ni;
+        launch_sgs_march(d, d->stream, d->st[0], 2, false);
+        cudaEventRecord(s0, d->stream);
+        for (int r = 0; r < 3; r++) launch_sgs_march(d, d->stream, d->st[0], 2, false);
+        cudaEventRecord(s1, d->stream);
+        d->launches += 4;
+        if (cudaEventSynchronize(s1) != cudaSuccess) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s0, s1);
+        if (ms < sbest) { sbest = ms; brow = rows; bni = ni; }
+      }
+    cudaEventDestroy(s0);
+    cudaEventDestroy(s1);
+    d->sgsRows = brow;
+    d->sgsNi = bni;
+  }
   invalidate_graph(d);
   if (tk) *tk = d->tk;
   if (tj) *tj = d->tj;

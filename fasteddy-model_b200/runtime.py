@@ -147,6 +147,8 @@ def load(rebuild: bool = True) -> dict[str, ctypes.CDLL]:
         ("fe_set_tiling", ip, [vp, ip, ip, ip]),
         ("fe_set_stage_kernel", ip, [vp, ip, ip, ip]),
         ("fe_set_sgs_kernel", ip, [vp, ip]),
+        ("fe_set_sgs_shape", ip, [vp, ip, ip]),
+        ("fe_get_sgs_shape", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_get_stage_kernel", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_autotune", ip, [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]),
         ("fe_launch_count", ctypes.c_longlong, [vp]),
@@ -531,6 +533,15 @@ class Domain:
         """Last-stage SGS physics as one fused kernel with tiles of `rows` rows (8 or 16), or
         (rows = 0) as the separate kernels."""
         _check(self.e.fe_set_sgs_kernel(self.h, int(rows)), "fe_set_sgs_kernel")
+
+    def set_sgs_shape(self, rows: int, ni: int) -> None:
+        """The fused SGS kernel's tile rows (8 or 16; 0 = the separate kernels) and planes per block."""
+        _check(self.e.fe_set_sgs_shape(self.h, int(rows), int(ni)), "fe_set_sgs_shape")
+
+    def sgs_shape(self) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(self.e.fe_get_sgs_shape(self.h, ctypes.byref(a), ctypes.byref(b)), "fe_get_sgs_shape")
+        return a.value, b.value
 
     def stage_kernel(self) -> tuple[str, int, int]:
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

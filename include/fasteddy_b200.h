@@ -213,6 +213,10 @@ int fe_get_stage_kernel(const fe_domain *d, int *kind, int *tj, int *ni);
  * scratch fields (the form the learned closure and the per-cell stage kernel always use). Results
  * are equal bit for bit. */
 int fe_set_sgs_kernel(fe_domain *d, int rows);
+/* The fused SGS kernel's tile rows (0, 8 or 16) and planes per thread block; and both read back.
+ * fe_autotune times the fused SGS kernel's shapes too and keeps the fastest. */
+int fe_set_sgs_shape(fe_domain *d, int rows, int ni);
+int fe_get_sgs_shape(const fe_domain *d, int *rows, int *ni);
 /* Pick the stage-kernel form and launch shape by timing the candidates (the autotuner);
  * tk/tj/ti receive the cell-kernel tiling, fe_get_stage_kernel the chosen form. */
 int fe_autotune(fe_domain *d, int *tk, int *tj, int *ti);

@@ -257,7 +257,7 @@ def measure_learned(fe, dom, args, cells: int, stream, local: int) -> dict:
     return {
         "value": cells * args.steps / (ms * 1e-3), "unit": "cell-updates/s", "ms_per_step": ms / args.steps,
         "nonfinite_cells": nonfinite,
-        "closure": "BF16 MLP 15-64-64-64-9 (tcgen05) replacing the TKE closure's 9 stresses at each physics stage",
+        "closure": "BF16 MLP 11-64-64-64-9 (tcgen05) replacing the TKE closure's 9 stresses at each physics stage",
         "mlp_inference": {"cells_per_s": nsamp / (inf_ms * 1e-3), "tflops": inf_tf, "peak_tflops": peak,
                           "frac": inf_tf / peak, "peak_source": src, "flop_per_cell": MLP_FWD_FLOP,
                           "sample": f"{nsamp} cells, inputs/outputs FP32 in HBM"},

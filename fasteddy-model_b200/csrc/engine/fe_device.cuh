@@ -70,7 +70,7 @@ struct Ptrs {
   float *mtau;                 // 3 per moisture species
   float *cd, *ch, *cq, *fricVel, *htFlux, *tskin, *invOblen, *z0m, *z0t, *qFlux, *qskin;
   const float* delta;          // grid scale (dx dy dz D)^(1/3) per cell, or nullptr (evaluated inline)
-  float* feat;                 // inputs of the learned closure per ring cell (SGS_NIN fields), or nullptr
+  float* feat;                 // inputs of the learned closure per ring cell (11 fields), or nullptr
   float* sgsF;                 // SGS tendencies for the march kernel's physics stages (7 fields), or nullptr
   float* lsfProf;              // slab means of rho, rho u, rho v, rho theta, rho q_v (nzh levels each), or nullptr
   double* lsfPart;             // per-block FP64 partial sums of the slab means

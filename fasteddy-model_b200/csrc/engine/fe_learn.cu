@@ -31,7 +31,7 @@ struct fe_mlp {
   float* mom2 = nullptr;
   fe::MlpNorm* norm = nullptr;
   fe::MlpNorm hnorm;
-  float* X = nullptr;       // data set: n x SGS_NIN inputs, n x 9 targets (tau/rho)
+  float* X = nullptr;       // data set: n x 11 inputs, n x 9 targets (tau/rho)
   float* T = nullptr;
   int* order = nullptr;     // shuffled sample order
   long long n = 0;

@@ -1,6 +1,6 @@
 // fe_mlp.cuh -- the learned SGS closure on the 5th-generation tensor cores (sm_100a).
 //
-// Network: 15 -> 64 -> 64 -> 64 -> 9, tanh on the hidden layers (hardware tanh.approx: bf16x2 on
+// Network: 11 -> 64 -> 64 -> 64 -> 9, tanh on the hidden layers (hardware tanh.approx: bf16x2 on
 // the BF16-rounded pre-activations for inference, f32 for training; see epi_tanh); inputs standardised ((x - mu) times the
 // FP32 reciprocal of sig), outputs tau/rho = out_mu + out_sig * y. Every layer is one 128-row tile of tcgen05.mma
 // (kind::f16, BF16 A and B operands from shared memory, FP32 accumulators in tensor memory),
@@ -26,7 +26,7 @@
 namespace fe {
 
 constexpr int MLP_H = 64;    // hidden width
-constexpr int MLP_K0 = 16;   // padded input width (SGS_NIN = 15 used)
+constexpr int MLP_K0 = 16;   // padded input width (11 used)
 constexpr int MLP_N4 = 16;   // padded output width (9 used)
 constexpr int MLP_M = 128;   // cells per tile (MMA M)
 constexpr int MP_W1 = 0;

@@ -5,16 +5,13 @@
 // strain-rate elements: S11 = g11, S22 = g22, S33 = g33, S21 = (g21 + g12)/2,
 // S31 = (g31 + g13)/2, S32 = (g32 + g23)/2, each half in the reference's own arithmetic, so
 // the components sit at the stress point the closure writes (index c, lower faces/edges).
-// N^2 is the length-scale buoyancy frequency and the grid scale is (dx dy dz D)^(1/3). The last
-// four are what the closure's heat fluxes are made of: sqrt(e) (its eddy diffusivity's velocity
-// scale; 0 without prognostic TKE) and the staggered theta gradients T6, T7, T8 of
-// cuda_sgsTurbDevice.cu:60-197 at the same stress point.
+// N^2 is the length-scale buoyancy frequency and the grid scale is (dx dy dz D)^(1/3).
 #pragma once
 #include "fe_device.cuh"
 
 namespace fe {
 
-constexpr int SGS_NIN = 15;   // g11 g12 g13 g21 g22 g23 g31 g32 g33 N^2 Delta sqrt(e) T6 T7 T8
+constexpr int SGS_NIN = 11;   // g11 g12 g13 g21 g22 g23 g31 g32 g33 N^2 Delta
 constexpr int SGS_NOUT = 9;   // tau11 tau21 tau31 tau32 tau22 tau33 tauTH1 tauTH2 tauTH3 (hydroTauFlds order)
 
 // Every rounding is spelled out (__fmul_rn/__fadd_rn/__fsub_rn, no fused multiply-add): the
@@ -57,19 +54,13 @@ __device__ __forceinline__ void sgs_inputs_a(const Phys& P, const Ptrs& Q, const
   const float dthdz = (float)(0.5 * (double)add(add(gx, gy), gz));
   x[9] = __fmul_rn(__fdiv_rn(P.g, pr.th(0, 0, 0)), dthdz);
   x[10] = grid_scale(P, Q, c);
-  x[11] = P.tke ? sqrtf(fmaxf(pr.ev(0, 0, 0), 0.0f)) : 0.0f;
-  const float thc = pr.th(0, 0, 0), tha = pr.th(-1, 0, 0), thb = pr.th(0, -1, 0), thd = pr.th(0, 0, -1);
-  x[12] = d1(dXi, thc, tha);
-  x[13] = d1(dYi, thc, thb);
-  x[14] = add(add(d2(J1, dXi, thc, tha), d2(J2, dYi, thc, thb)), d2(J3, dZi, thc, thd));
 }
 
 // The inputs of cell c straight from the flux-form state.
 __device__ __forceinline__ void sgs_inputs(const Phys& P, const Ptrs& Q, const float* __restrict__ st, long long c,
                                            float* x) {
   const long long n = P.n;
-  const GlobalPrims pr{st, st + n, st + 2 * n, st + 3 * n, st + 4 * n, P.ntke ? st + 5 * n : nullptr, nullptr, n, c,
-                       P.si, P.sj};
+  const GlobalPrims pr{st, st + n, st + 2 * n, st + 3 * n, st + 4 * n, nullptr, nullptr, n, c, P.si, P.sj};
   sgs_inputs_a(P, Q, pr, c, x);
 }
 

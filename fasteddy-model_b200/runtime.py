@@ -16,7 +16,7 @@ from . import build as _build
 
 _LIBS: dict[str, ctypes.CDLL] = {}
 
-SGS_NIN = 15      # FE_SGS_NIN
+SGS_NIN = 11      # FE_SGS_NIN
 SGS_NOUT = 9      # FE_SGS_NOUT
 KERNEL_CELL = 0   # FE_KERNEL_CELL
 KERNEL_MARCH = 1  # FE_KERNEL_MARCH

@@ -295,16 +295,14 @@ int fe_checkpoint_load(fe_domain *d, const void *buf, size_t bytes);
  * (cuda_hydroCoreDevice.cu:759-768); the TKE closure stays the fallback (no network set).
  *
  * Inputs per stress point (FE_SGS_NIN): the 9 velocity-gradient halves of the closure's
- * staggered strain rates g11 g12 g13 g21 g22 g23 g31 g32 g33, the buoyancy frequency N^2, the
- * grid scale (dx dy dz D)^(1/3), sqrt(e) of the prognostic SGS TKE (0 without it) and the
- * staggered theta gradients of the closure's heat fluxes (its T6, T7, T8). Outputs
- * (FE_SGS_NOUT): tau/rho in the closure's field order tau11 tau21 tau31 tau32 tau22 tau33 tauTH1
- * tauTH2 tauTH3. Network 15 -> 64 -> 64 -> 64 -> 9 with tanh, BF16 weights/activations on the
- * tensor cores, FP32 accumulation; inputs standardised with (in_mu, in_sig), outputs
- * tau/rho = out_mu + out_sig * y.
- * Parameters (fe_mlp_param_count() FP32 values): W1[64][16] (column 15 unused), b1[64],
+ * staggered strain rates g11 g12 g13 g21 g22 g23 g31 g32 g33, the buoyancy frequency N^2 and
+ * the grid scale (dx dy dz D)^(1/3). Outputs (FE_SGS_NOUT): tau/rho in the closure's field
+ * order tau11 tau21 tau31 tau32 tau22 tau33 tauTH1 tauTH2 tauTH3. Network 11 -> 64 -> 64 ->
+ * 64 -> 9 with tanh, BF16 weights/activations on the tensor cores, FP32 accumulation;
+ * inputs standardised with (in_mu, in_sig), outputs tau/rho = out_mu + out_sig * y.
+ * Parameters (fe_mlp_param_count() FP32 values): W1[64][16] (columns 11..15 unused), b1[64],
  * W2[64][64], b2[64], W3[64][64], b3[64], W4[16][64] (rows 9..15 unused), b4[16]. */
-#define FE_SGS_NIN 15
+#define FE_SGS_NIN 11
 #define FE_SGS_NOUT 9
 typedef struct fe_mlp fe_mlp;
 long long fe_mlp_param_count(void);

@@ -3,7 +3,7 @@
 Only tests and bench.py's CPU baseline use this module; the product path runs the tensor-core
 kernels of fasteddy-model_b200/csrc/engine/fe_mlp.cuh and never calls into here.
 
-The network is the closure's: 15 -> 64 -> 64 -> 64 -> 9, tanh hidden layers, standardised
+The network is the closure's: 11 -> 64 -> 64 -> 64 -> 9, tanh hidden layers, standardised
 inputs, outputs tau/rho = out_mu + out_sig * y, loss = mean over samples and the 9 outputs of
 the squared standardised error. Parameter layout as fe_mlp_param_count() documents in
 include/fasteddy_b200.h (W1[64][16], b1, W2[64][64], b2, W3[64][64], b3, W4[16][64], b4[16]).
@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import numpy as np
 
-NIN, NOUT, H, K0, N4 = 15, 9, 64, 16, 16
+NIN, NOUT, H, K0, N4 = 11, 9, 64, 16, 16
 W1, B1 = 0, 64 * 16
 W2 = B1 + 64
 B2 = W2 + 64 * 64
@@ -141,17 +141,14 @@ def glorot(seed: int) -> np.ndarray:
 
 
 def closure_inputs(hydro: np.ndarray, J31: np.ndarray, J32: np.ndarray, J33: np.ndarray, D: np.ndarray,
-                   dX: float, dY: float, dZ: float, g: float, tke: np.ndarray | None = None,
-                   halo: int = 3) -> np.ndarray:
+                   dX: float, dY: float, dZ: float, g: float, halo: int = 3) -> np.ndarray:
     """FP64 closure inputs of every interior cell (rows in i, j, k order, k fastest).
 
     hydro is the flux-form state [rho, rho u, rho v, rho w, rho theta][i][j][k] with `halo` cells
     per side; J31/J32/J33/D the grid metrics on the same points. The 9 velocity-gradient halves
     are the staggered strain-rate terms of cuda_sgsTurbDevice.cu:60-197 at the stress point (the
     cell's lower faces and edges); N^2 = g/theta * dtheta/dz with the centred terrain-following
-    derivative of cuda_sgstkeDevice.cu:96-151; the grid scale is (dx dy dz D)^(1/3); then sqrt(e)
-    of the SGS TKE `tke` (flux form rho e; 0 when None) and the staggered theta gradients T6, T7,
-    T8 of the closure's heat fluxes (cuda_sgsTurbDevice.cu:60-197).
+    derivative of cuda_sgstkeDevice.cu:96-151; the grid scale is (dx dy dz D)^(1/3).
     """
     h = hydro.astype(np.float64)
     r = np.maximum(h[0], 1e-6)
@@ -176,7 +173,7 @@ def closure_inputs(hydro: np.ndarray, J31: np.ndarray, J32: np.ndarray, J33: np.
 
     C, Ai, Bj, Dk = (0, 0, 0), (-1, 0, 0), (0, -1, 0), (0, 0, -1)
     AB, AD, BD, ABD = (-1, -1, 0), (-1, 0, -1), (0, -1, -1), (-1, -1, -1)
-    x = np.empty((NIN, nx, ny, nz))
+    x = np.empty((11, nx, ny, nz))
     x[0] = dx(u, C, Ai)
     x[1] = 0.5 * (dy(u, C, Bj) + dy(u, Ai, AB))
     x[2] = (0.5 * J1 * (dx(u, C, Ai) + dx(u, Dk, AD))
@@ -194,8 +191,4 @@ def closure_inputs(hydro: np.ndarray, J31: np.ndarray, J32: np.ndarray, J33: np.
                    + J3 * dzi * (at(th, 0, 0, 1) - at(th, 0, 0, -1)))
     x[9] = g / at(th, 0, 0, 0) * dthdz
     x[10] = np.cbrt(float(dX) * float(dY) * float(dZ) * at(D.astype(np.float64), 0, 0, 0))
-    x[11] = 0.0 if tke is None else np.sqrt(np.maximum(at(tke.astype(np.float64) / r, 0, 0, 0), 0.0))
-    x[12] = dx(th, C, Ai)
-    x[13] = dy(th, C, Bj)
-    x[14] = J1 * dx(th, C, Ai) + J2 * dy(th, C, Bj) + J3 * dz(th, C, Dk)
-    return x.reshape(NIN, -1).T
+    return x.reshape(11, -1).T

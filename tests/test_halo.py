@@ -180,3 +180,90 @@ def test_slabs_with_per_stage_halo_exchange_equal_the_whole_domain(px, py):
     for k, v in diffs.items():
         if v is not None:
             assert v == 0.0, (k, v)
+
+
+def _distributed_slab_worker(rank, world, port, q):
+    """DistributedSlab's set-up and tear-down on a stand-in engine that records its calls."""
+    dist = _init(rank, world, port)
+    import ctypes
+    import importlib
+
+    fe = importlib.import_module("fasteddy-model_b200")
+    log = []
+
+    class Engine:
+        def fe_ipc_handle_bytes(self):
+            return 64
+
+        def fe_arena_ipc_handle(self, h, buf, n):
+            ctypes.memmove(buf, bytes([0xA0 + rank]) * 64, 64)
+            return 0
+
+        def fe_set_halo_peers(self, h, px, py, arr):
+            log.append(("peers", px, py, [None if arr[t] is None else ctypes.string_at(arr[t], 64) for t in range(9)]))
+            return 0
+
+        def fe_comm_unique_id_bytes(self):
+            return 128
+
+        def fe_comm_unique_id(self, buf, n):
+            ctypes.memmove(buf, b"U" * 128, 128)
+            return 0
+
+        def fe_comm_create(self, uid, n, r, dev, out):
+            log.append(("comm", uid.raw, n, r, dev))
+            out._obj.value = 7
+            return 0
+
+        def fe_set_halo_comm(self, h, c):
+            log.append(("set_comm", None if c is None else c.value))
+            return 0
+
+        def fe_clear_halo_peers(self, h):
+            log.append(("clear_peers",))
+            return 0
+
+        def fe_comm_destroy(self, c):
+            log.append(("destroy_comm", c.value))
+            return 0
+
+    class Domain:
+        def __init__(self, cfg, device):
+            self.h, self.e = ctypes.c_void_p(1), Engine()
+            log.append(("domain", cfg.Nx, cfg.Ny, device))
+
+        def set_inputs(self, inp, simTime, simTime_it):
+            log.append(("inputs", inp["hydroFlds"].shape))
+
+        def sync(self):
+            log.append(("sync",))
+
+        def close(self):
+            log.append(("close",))
+            self.h = ctypes.c_void_p()
+
+    fe.halo.Domain = Domain
+    host = fe.cases.setup_host("cbl_dry", 16, 12, 8)
+    slab = fe.halo.DistributedSlab(host.config(), host.inputs(), 2, 1, device=rank)
+    slab.close()
+    host.cleanup()
+    q.put((rank, log))
+    dist.destroy_process_group()
+
+
+def test_distributed_slab_set_up_and_tear_down_over_gloo():
+    """Two ranks, 2 x 1 slabs: each makes an 8 x 12 slab, gets the other rank's arena handle for
+    its x neighbours (itself for y), the communicator of rank 0's unique id with its own rank and
+    device, its slab of the inputs; on close, the peers are unmapped and the communicator
+    released before the slab."""
+    res = _spawn(_distributed_slab_worker, 2)
+    for rank, log in res:
+        other = bytes([0xA0 + 1 - rank]) * 64
+        kinds = [e[0] for e in log]
+        assert kinds == ["domain", "peers", "comm", "set_comm", "inputs", "sync", "clear_peers", "set_comm",
+                         "destroy_comm", "close"]
+        assert log[0] == ("domain", 8, 12, rank)
+        assert log[1] == ("peers", 2, 1, [other, other, other, None, None, None, other, other, other])
+        assert log[2] == ("comm", b"U" * 128, 2, rank, rank)
+        assert log[3] == ("set_comm", 7) and log[7] == ("set_comm", None) and log[8] == ("destroy_comm", 7)
+        assert log[4] == ("inputs", (5, 14, 18, 14))

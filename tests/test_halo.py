@@ -142,14 +142,17 @@ def _oracle_slab_worker(rank, world, port, q, px, py, nsteps):
     o = Oracle(fe.halo.slab_config(cfg, px, py))
     o.set_decomposition(px > 1, py > 1)
     o.set_inputs(fe.halo.split_inputs(inp, px, py, rank))
-    axis, n = (1, cfg.Nx // px) if px > 1 else (2, cfg.Ny // py)
+    # x first (own rows), then y over the whole x range, halos included: the corners arrive with it
+    # (with two slabs per direction both neighbours along a direction are the same rank)
+    dirs = ([(1, cfg.Nx // px, rank ^ 1)] if px > 1 else []) + ([(2, cfg.Ny // py, rank ^ px)] if py > 1 else [])
     t, it = np.float32(0.0), 0
     for _ in range(nsteps):
         for stage in range(3):
             s = o.get_state()
             for key in ("hydroFlds", "sgstke", "moist"):
                 if s[key] is not None:
-                    _exchange(dist, s[key], axis, n, 1 - rank)
+                    for axis, n, other in dirs:
+                        _exchange(dist, s[key], axis, n, other)
             o.set_state_f64(s["hydroFlds"], s["sgstke"], s["moist"])
             o.rk_stage(stage)
         t, it = np.float32(t + np.float32(cfg.dt)), it + 1  # the clock rule of ora_step
@@ -171,11 +174,12 @@ def _oracle_slab_worker(rank, world, port, q, px, py, nsteps):
     host.cleanup()
 
 
-@pytest.mark.parametrize("px,py", [(2, 1), (1, 2)])
+@pytest.mark.parametrize("px,py", [(2, 1), (1, 2), (2, 2)])
 def test_slabs_with_per_stage_halo_exchange_equal_the_whole_domain(px, py):
-    """Moist CBL over a hill, 16 x 12 x 8, 3 RK3 steps: two oracle slabs exchanging their
-    halos over gloo before each stage give the single-domain state exactly."""
-    res = _spawn(_oracle_slab_worker, 2, px, py, 3)
+    """Moist CBL over a hill, 16 x 12 x 8, 3 RK3 steps: oracle slabs (two, or four with corner
+    neighbours) exchanging their halos over gloo before each stage give the single-domain state
+    exactly."""
+    res = _spawn(_oracle_slab_worker, px * py, px, py, 3)
     diffs = res[0][1]
     for k, v in diffs.items():
         if v is not None:

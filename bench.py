@@ -668,7 +668,10 @@ def main(argv=None) -> int:
         else:
             line = run_ours(args, rank, world, local)
             if line is not None and world == 1 and args.case == DEFAULT_CASE and not args.no_extra:
-                line["other_configs"] = other_configs(args, local)
+                try:
+                    line["other_configs"] = other_configs(args, local)
+                except Exception as exc:  # the headline line stands without them
+                    line["other_configs"] = {"error": f"{type(exc).__name__}: {str(exc).splitlines()[0][:200]}"}
     finally:
         if world > 1:
             import torch.distributed as dist
